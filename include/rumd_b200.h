@@ -1,0 +1,201 @@
+/*
+ * rumd_b200.h -- C ABI of the B200-native RUMD time-step engine.
+ *
+ * One engine holds any number of independent MD systems ("replicas": a plain
+ * Sample is an engine with one replica) resident in HBM on one GPU, and
+ * advances all of them with the same fused kernels:
+ *   neighbour-list rebuild (cell-key stable sort + sorted 5x5x5 cell scan),
+ *   shifted-force / shifted-potential Lennard-Jones forces, energy and virial,
+ *   Nose-Hoover leap-frog NVT update, FP64 reductions.
+ *
+ * Conventions
+ *   - Every function returns B2MD_OK (0) or a B2MD_ERR_* code; the message of
+ *     the last failure on the calling thread is b2md_last_error().  No C++
+ *     exception crosses this boundary.
+ *   - Particle arrays passed in or out are HOST arrays in the ORIGINAL
+ *     particle order (RUMD's convention: host data is never sorted,
+ *     src/ParticleData.cu:333-393), float32 with 4 components per particle:
+ *       positions  [x, y, z, type bit-cast to float]  (ParticleData.h:41)
+ *       velocities [vx, vy, vz, 1/m]                 (ParticleData.h:42)
+ *       forces     [fx, fy, fz, u_i]  u_i already halved (PairPotential.cu:371)
+ *       virials    [w_mol, s_xz, s_xy, w_i]  w_i = sum_j d^2 s (ParticleData.h:44)
+ *       stresses   [s_xx, s_yy, s_zz, s_yz]           (ParticleData.h:46)
+ *     Images are int32 [imx, imy, imz] per particle.
+ *   - Parameter tables use RUMD's layout: float params[T][T][12] with
+ *     p0 = Rcut (absolute), p1 = A12, p2 = A6, p10 = s(Rcut)*Rcut,
+ *     p11 = u(Rcut) (PairPotential.cu:82-125, PairPotential.h:149-207).
+ */
+#ifndef RUMD_B200_H
+#define RUMD_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define B2MD_API __attribute__((visibility("default")))
+#else
+#define B2MD_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2MD_OK 0
+#define B2MD_ERR_ARG 1       /* invalid argument */
+#define B2MD_ERR_CUDA 2      /* CUDA runtime error (message has the detail) */
+#define B2MD_ERR_NOMEM 3     /* device memory or engine capacity exhausted */
+#define B2MD_ERR_STATE 4     /* call not valid in the current state */
+#define B2MD_ERR_OVERFLOW 5  /* neighbour list could not be made large enough */
+
+#define B2MD_CUTOFF_NS 0
+#define B2MD_CUTOFF_SP 1
+#define B2MD_CUTOFF_SF 2
+
+/* fields for b2md_replica_get / b2md_replica_set */
+#define B2MD_FIELD_POS 0
+#define B2MD_FIELD_VEL 1
+#define B2MD_FIELD_FORCE 2
+#define B2MD_FIELD_VIRIAL 3
+#define B2MD_FIELD_IMAGES 4
+#define B2MD_FIELD_STRESS 5
+
+/* indices of b2md_replica_stats output (doubles) */
+#define B2MD_STAT_PE 0          /* sum_i u_i of the last force evaluation      */
+#define B2MD_STAT_VIRIAL 1      /* sum_i w_i / 6                               */
+#define B2MD_STAT_KE 2          /* leap-frog KE(t) of the last integrated step */
+#define B2MD_STAT_XI 3          /* Nose-Hoover thermostat state                 */
+#define B2MD_STAT_KE2 4         /* sum m v^2 (t + h/2) of the last step         */
+#define B2MD_STAT_STEPS 5       /* steps integrated since the replica was added */
+#define B2MD_STAT_REBUILDS 6    /* neighbour-list rebuilds                      */
+#define B2MD_STAT_STEPS_LEFT 7  /* steps still queued for b2md_run_queued       */
+#define B2MD_STAT_OVERFLOW 8    /* 1 if the list overflowed and is waiting      */
+#define B2MD_STAT_TARGET_T 9    /* current target temperature                   */
+#define B2MD_STAT_MAX_NBRS 10   /* list capacity per particle                   */
+#define B2MD_STAT_ACTUAL_MAX_NBRS 11 /* largest neighbour count of the last build */
+#define B2MD_NSTAT 12
+
+typedef struct b2md_engine b2md_engine;
+
+/* One MD system.  Mirrors the state a RUMD Sample + Pot_LJ_12_6 +
+ * IntegratorNVT hold (Sample.h:33-90, PairPotential.h:33-128,
+ * IntegratorNVT.h:14-92). */
+typedef struct {
+  int n;                    /* number of particles (>= 2)                          */
+  int ntypes;               /* number of particle types (1..8)                     */
+  float box[3];             /* rectangular periodic box lengths                    */
+  const float* params;      /* ntypes*ntypes*12 floats, RUMD layout                */
+  int cutoff_method;        /* B2MD_CUTOFF_*                                       */
+  float skin;               /* neighbour-list skin (NeighborList::SetSkin)         */
+  float dt;                 /* time step                                           */
+  double target_T;          /* thermostat target temperature                       */
+  double tau;               /* thermostat relaxation time (omega^2 = 4 pi^2/tau^2) */
+  double dT_per_step;       /* SetTemperatureChangePerTimeStep                     */
+  double xi;                /* initial thermostat state                            */
+  unsigned thermostat_mask; /* bit t set: type t is thermostatted (0 = NVE)        */
+  int reset_interval;       /* zero total momentum every k steps (0 = never)       */
+  int max_nbrs;             /* list capacity per particle (0 = density estimate)   */
+  int energy_interval;      /* log (pe, W, KE, xi) every k steps (0 = off)         */
+  int energy_capacity;      /* number of log entries kept                          */
+} b2md_replica_desc;
+
+/* Engine lifetime.  Replaces the allocation that RUMD spreads over
+ * Sample::SetNumberOfParticles (Sample.cu:208-249),
+ * NeighborList::AllocateNeighborList (NeighborList.cu:275-295) and
+ * IntegratorNVT::AllocateIntegratorState (IntegratorNVT.cu:106-126).
+ * Capacities bound what b2md_replica_add may admit (0 = grow on demand).
+ * pb = particles per block, tp = threads per particle (Sample(pb, tp)). */
+B2MD_API int b2md_engine_create(int device, long long max_particles, int max_replicas,
+                       long long max_list_entries, int pb, int tp, b2md_engine** out);
+B2MD_API int b2md_engine_destroy(b2md_engine* e);
+/* Sample::SetPB_TP (Sample.h:96).  tp in {1,2,4,8}; pb a multiple of 32;
+ * pb*tp <= 512. */
+B2MD_API int b2md_engine_set_launch(b2md_engine* e, int pb, int tp);
+/* Device bytes currently allocated by the engine. */
+B2MD_API int b2md_engine_memory(b2md_engine* e, long long* bytes);
+/* Chooses CUDA-graph conditional rebuild nodes (1, default) or unconditional
+ * early-exit rebuild kernels (0) for b2md_run. */
+B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
+
+/* Admission of one system (Sample::ReadConf + SetPotential + SetIntegrator,
+ * Simulation.py:29-31,157-214).  vel4/im3 may be NULL (zero). */
+B2MD_API int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* pos4,
+                     const float* vel4, const int* im3, int* id_out);
+B2MD_API int b2md_replica_remove(b2md_engine* e, int id);
+/* Copies a field out in original order (ParticleData::Copy*FromDevice,
+ * ParticleData.cu:383-470).  out: n*4 floats, or n*3 ints for images. */
+B2MD_API int b2md_replica_get(b2md_engine* e, int id, int field, void* out);
+/* Replaces positions, velocities or images (ParticleData::CopyPosToDevice
+ * with reset_sorting, ParticleData.cu:333-355).  Setting positions forces a
+ * neighbour-list rebuild before the next force evaluation. */
+B2MD_API int b2md_replica_set(b2md_engine* e, int id, int field, const void* in);
+/* Pair parameter table / cut-off method / skin (PairPotential::SetParams +
+ * CopyParamsToGPU, PairPotential.cu:82-125; SetNbListSkin). */
+B2MD_API int b2md_replica_set_potential(b2md_engine* e, int id, int ntypes, const float* params,
+                               int cutoff_method, float skin);
+/* Integrator settings (IntegratorNVT::SetTimeStep, SetTargetTemperature,
+ * SetRelaxationTime, SetThermostatState, SetThermostatOn*,
+ * SetTemperatureChangePerTimeStep; IntegratorNVT.cu:132-190). */
+B2MD_API int b2md_replica_set_integrator(b2md_engine* e, int id, float dt, double target_T,
+                                double tau, double dT_per_step, unsigned thermostat_mask);
+B2MD_API int b2md_replica_set_xi(b2md_engine* e, int id, double xi);
+B2MD_API int b2md_replica_set_reset_interval(b2md_engine* e, int id, int reset_interval);
+/* NeighborList::SetNB_Method (NeighborList.cu:226-245): -1 "default" (cell
+ * sort when the 5x5x5 scan covers rc+skin, else all pairs), 0 "sort", 1 "n2". */
+B2MD_API int b2md_replica_set_nb_method(b2md_engine* e, int id, int method);
+/* FP64 scalars of the replica, B2MD_NSTAT doubles (Sample::GetPotentialEnergy,
+ * GetVirial, IntegratorNVT::GetKineticEnergy/GetThermostatState). */
+B2MD_API int b2md_replica_stats(b2md_engine* e, int id, double* out);
+/* Energy log: up to cap entries of (step, pe, W, KE, xi); returns count. */
+B2MD_API int b2md_replica_energy_log(b2md_engine* e, int id, double* out, int cap, int* count);
+/* Stress tensor sum (Sample::GetStress, Sample.cu:393-444): 6 doubles
+ * (xx, yy, zz, yz, xz, xy), requires a force evaluation with stress. */
+B2MD_API int b2md_replica_stress(b2md_engine* e, int id, int include_kinetic, double* out6);
+
+/* Sample::CalcF (Sample.cu:329-351) for every replica: neighbour-list update
+ * (NeighborList::UpdateNBlist, NeighborList.cu:583-690) then pair forces
+ * (Calcf_NBL_tp*, PairPotential.cu:330-515). */
+B2MD_API int b2md_calc_f(b2md_engine* e, int stress);
+/* IntegratorNVT::Integrate (IntegratorNVT.cu:64-92) for every replica. */
+B2MD_API int b2md_integrate(b2md_engine* e);
+/* IntegratorNVT::SetMomentumToZero (IntegratorNVT.cu:176-183). */
+B2MD_API int b2md_zero_momentum(b2md_engine* e);
+/* Simulation.Run(nsteps) (Simulation.py:538-622) for every replica, in
+ * lock step: momentum reset every reset_interval steps, CalcF, Integrate,
+ * then a final CalcF.  Runs as CUDA graphs of fused kernels with the rebuild
+ * decided on the device; list overflow is repaired on the host (capacity
+ * doubled, NeighborList.cu:657-676) and the run resumed. */
+B2MD_API int b2md_run(b2md_engine* e, long long nsteps);
+/* Batched/served form: each replica advances its own queued step count
+ * (b2md_replica_queue_steps) in the same launches; returns when all queues
+ * are empty or after max_steps launches-worth of steps (0 = until empty). */
+B2MD_API int b2md_replica_queue_steps(b2md_engine* e, int id, long long nsteps);
+B2MD_API int b2md_run_queued(b2md_engine* e, long long max_steps, long long* steps_run);
+
+/* Parity hooks.  Neighbour list of replica id in ORIGINAL particle ids:
+ * counts[n], nbl[n][max_nbrs] row-major (entries in list order). */
+B2MD_API int b2md_nbl_export(b2md_engine* e, int id, unsigned* counts, unsigned* nbl, int max_nbrs);
+/* d_unsorted_index (ParticleData.h:56): original id of each sorted slot. */
+B2MD_API int b2md_sort_export(b2md_engine* e, int id, unsigned* unsorted_index);
+/* Cell key grid used by the rebuild: nc[3]. */
+B2MD_API int b2md_cell_grid(b2md_engine* e, int id, int* nc3);
+
+B2MD_API int b2md_sync(b2md_engine* e);
+/* The engine's CUDA stream (cudaStream_t) for callers that interleave work. */
+B2MD_API void* b2md_stream(b2md_engine* e);
+B2MD_API const char* b2md_last_error(void);
+B2MD_API const char* b2md_version(void);
+
+/* Evaluates, on the device, the squared minimum-image distance of npairs
+ * pairs both as the reference source expression (compiled with nvcc's default
+ * multiply-add contraction) and as this engine's explicit form; used by the
+ * parity tests to pin the neighbour-list arithmetic.  Inputs and outputs are
+ * host arrays: a4/b4 npairs*4 floats, box 3 floats, out 2*npairs floats. */
+B2MD_API int b2md_probe_dist2(const float* a4, const float* b4, const float* box, int npairs, float* out);
+/* Same for the cell coordinate (int)(nc * (x / L + 0.5f)) of n coordinates:
+ * out 2*n ints (reference expression, explicit form). */
+B2MD_API int b2md_probe_cell(const float* x, int n, float box, int nc, int* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RUMD_B200_H */

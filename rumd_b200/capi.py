@@ -1,0 +1,305 @@
+"""ctypes binding of the C ABI in include/rumd_b200.h.
+
+This is the thinnest host layer over the native engine: it loads the in-tree
+``librumd_b200.so`` and fails loudly when it is missing -- there is no CPU or
+PyTorch fallback.  ``Engine`` below is a convenience wrapper with numpy I/O;
+the RUMD class surface (Sample, Pot_LJ_12_6, IntegratorNVT) is in
+``rumd_b200.rumd`` on top of the C++ classes.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librumd_b200.so")
+
+B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_OVERFLOW = range(6)
+CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
+FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
+STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",
+              "target_T", "max_nbrs", "actual_max_nbrs"]
+NSTAT = len(STAT_NAMES)
+NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
+
+EXPORTS = [
+    "b2md_engine_create", "b2md_engine_destroy", "b2md_engine_set_launch", "b2md_engine_memory",
+    "b2md_engine_set_graph_mode", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
+    "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_set_integrator",
+    "b2md_replica_set_xi", "b2md_replica_set_reset_interval", "b2md_replica_set_nb_method",
+    "b2md_replica_stats", "b2md_replica_energy_log", "b2md_replica_stress", "b2md_calc_f",
+    "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_replica_queue_steps",
+    "b2md_run_queued", "b2md_nbl_export", "b2md_sort_export", "b2md_cell_grid", "b2md_sync",
+    "b2md_stream", "b2md_last_error", "b2md_version", "b2md_probe_dist2", "b2md_probe_cell",
+]
+
+
+class ReplicaDesc(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_int), ("ntypes", ctypes.c_int), ("box", ctypes.c_float * 3),
+        ("params", ctypes.POINTER(ctypes.c_float)), ("cutoff_method", ctypes.c_int),
+        ("skin", ctypes.c_float), ("dt", ctypes.c_float), ("target_T", ctypes.c_double),
+        ("tau", ctypes.c_double), ("dT_per_step", ctypes.c_double), ("xi", ctypes.c_double),
+        ("thermostat_mask", ctypes.c_uint), ("reset_interval", ctypes.c_int),
+        ("max_nbrs", ctypes.c_int), ("energy_interval", ctypes.c_int),
+        ("energy_capacity", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Loads librumd_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m rumd_b200.build` (no CPU fallback exists)")
+        L = ctypes.CDLL(LIB_PATH)
+        P, i, ll, f, d, u = (ctypes.c_void_p, ctypes.c_int, ctypes.c_longlong, ctypes.c_float,
+                             ctypes.c_double, ctypes.c_uint)
+        sig = {
+            "b2md_engine_create": [i, ll, i, ll, i, i, ctypes.POINTER(P)],
+            "b2md_engine_destroy": [P],
+            "b2md_engine_set_launch": [P, i, i],
+            "b2md_engine_memory": [P, ctypes.POINTER(ll)],
+            "b2md_engine_set_graph_mode": [P, i],
+            "b2md_replica_add": [P, ctypes.POINTER(ReplicaDesc), P, P, P, ctypes.POINTER(i)],
+            "b2md_replica_remove": [P, i],
+            "b2md_replica_get": [P, i, i, P],
+            "b2md_replica_set": [P, i, i, P],
+            "b2md_replica_set_potential": [P, i, i, P, i, f],
+            "b2md_replica_set_integrator": [P, i, f, d, d, d, u],
+            "b2md_replica_set_xi": [P, i, d],
+            "b2md_replica_set_reset_interval": [P, i, i],
+            "b2md_replica_set_nb_method": [P, i, i],
+            "b2md_replica_stats": [P, i, P],
+            "b2md_replica_energy_log": [P, i, P, i, ctypes.POINTER(i)],
+            "b2md_replica_stress": [P, i, i, P],
+            "b2md_calc_f": [P, i],
+            "b2md_integrate": [P],
+            "b2md_zero_momentum": [P],
+            "b2md_run": [P, ll],
+            "b2md_replica_queue_steps": [P, i, ll],
+            "b2md_run_queued": [P, ll, ctypes.POINTER(ll)],
+            "b2md_nbl_export": [P, i, P, P, i],
+            "b2md_sort_export": [P, i, P],
+            "b2md_cell_grid": [P, i, P],
+            "b2md_sync": [P],
+            "b2md_probe_dist2": [P, P, P, i, P],
+            "b2md_probe_cell": [P, i, f, i, P],
+        }
+        for name, args in sig.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.b2md_stream.argtypes = [P]
+        L.b2md_stream.restype = P
+        L.b2md_last_error.restype = ctypes.c_char_p
+        L.b2md_version.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+class B2MDError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[b2md error {code}] {msg}")
+        self.code = code
+
+
+def check(rc):
+    if rc != B2MD_OK:
+        msg = lib().b2md_last_error().decode(errors="replace")
+        if rc == B2MD_ERR_ARG:
+            raise ValueError(msg)
+        raise B2MDError(rc, msg)
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def pack_pos4(pos, types):
+    """float32 [n,4]: xyz and the type bit-cast into the fourth lane."""
+    pos = np.asarray(pos)
+    n = len(pos)
+    out = np.zeros((n, 4), np.float32)
+    out[:, :3] = pos[:, :3]
+    out[:, 3] = np.asarray(types, np.int32).view(np.float32)
+    return out
+
+
+def pack_vel4(vel, masses_per_particle):
+    vel = np.asarray(vel)
+    out = np.zeros((len(vel), 4), np.float32)
+    out[:, :3] = vel[:, :3]
+    out[:, 3] = 1.0 / np.asarray(masses_per_particle, np.float32)
+    return out
+
+
+class Engine:
+    """Owns one b2md_engine: any number of resident MD systems on one GPU."""
+
+    def __init__(self, device=0, max_particles=0, max_replicas=1, max_list_entries=0, pb=64, tp=4):
+        h = ctypes.c_void_p()
+        check(lib().b2md_engine_create(device, max_particles, max_replicas, max_list_entries, pb, tp,
+                                       ctypes.byref(h)))
+        self._h = h
+        self.pb, self.tp = pb, tp
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().b2md_engine_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_launch(self, pb, tp):
+        check(lib().b2md_engine_set_launch(self._h, pb, tp))
+        self.pb, self.tp = pb, tp
+
+    def set_graph_mode(self, conditional):
+        check(lib().b2md_engine_set_graph_mode(self._h, int(bool(conditional))))
+
+    def memory(self):
+        b = ctypes.c_longlong()
+        check(lib().b2md_engine_memory(self._h, ctypes.byref(b)))
+        return b.value
+
+    def add(self, pos4, box, params, ntypes, cutoff="SF", skin=0.3, dt=0.005, T=1.0, tau=0.2,
+            vel4=None, im3=None, thermostat=True, xi=0.0, reset_interval=100, max_nbrs=0,
+            dT_per_step=0.0, energy_interval=0, energy_capacity=0, thermostat_mask=None):
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        n = len(pos4)
+        params = np.ascontiguousarray(params, np.float32)
+        d = ReplicaDesc()
+        d.n, d.ntypes = n, ntypes
+        for k in range(3):
+            d.box[k] = float(box[k])
+        d.params = params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        d.cutoff_method = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
+        d.skin, d.dt = skin, dt
+        d.target_T, d.tau, d.dT_per_step, d.xi = T, tau, dT_per_step, xi
+        if thermostat_mask is None:
+            thermostat_mask = 0xFFFFFFFF if thermostat else 0
+        d.thermostat_mask = thermostat_mask
+        d.reset_interval = reset_interval
+        d.max_nbrs = max_nbrs
+        d.energy_interval, d.energy_capacity = energy_interval, energy_capacity
+        v = None if vel4 is None else np.ascontiguousarray(vel4, np.float32)
+        im = None if im3 is None else np.ascontiguousarray(im3, np.int32)
+        rid = ctypes.c_int()
+        check(lib().b2md_replica_add(self._h, ctypes.byref(d), _ptr(pos4), _ptr(v), _ptr(im), ctypes.byref(rid)))
+        return rid.value
+
+    def remove(self, rid):
+        check(lib().b2md_replica_remove(self._h, rid))
+
+    def get(self, rid, field, n):
+        if field == "images":
+            out = np.zeros((n, 3), np.int32)
+        else:
+            out = np.zeros((n, 4), np.float32)
+        check(lib().b2md_replica_get(self._h, rid, FIELD[field], _ptr(out)))
+        return out
+
+    def set(self, rid, field, arr):
+        dt = np.int32 if field == "images" else np.float32
+        arr = np.ascontiguousarray(arr, dt)
+        check(lib().b2md_replica_set(self._h, rid, FIELD[field], _ptr(arr)))
+
+    def set_potential(self, rid, ntypes, params, cutoff, skin):
+        params = np.ascontiguousarray(params, np.float32)
+        c = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
+        check(lib().b2md_replica_set_potential(self._h, rid, ntypes, _ptr(params), c, skin))
+
+    def set_integrator(self, rid, dt, T, tau, dT_per_step=0.0, thermostat_mask=0xFFFFFFFF):
+        check(lib().b2md_replica_set_integrator(self._h, rid, dt, T, tau, dT_per_step, thermostat_mask))
+
+    def set_xi(self, rid, xi):
+        check(lib().b2md_replica_set_xi(self._h, rid, xi))
+
+    def set_reset_interval(self, rid, k):
+        check(lib().b2md_replica_set_reset_interval(self._h, rid, k))
+
+    def set_nb_method(self, rid, method):
+        check(lib().b2md_replica_set_nb_method(self._h, rid, NB_METHOD[method]))
+
+    def stats(self, rid):
+        out = np.zeros(NSTAT)
+        check(lib().b2md_replica_stats(self._h, rid, _ptr(out)))
+        return dict(zip(STAT_NAMES, out.tolist()))
+
+    def energy_log(self, rid, cap=1 << 20):
+        out = np.zeros((cap, 5))
+        cnt = ctypes.c_int()
+        check(lib().b2md_replica_energy_log(self._h, rid, _ptr(out), cap, ctypes.byref(cnt)))
+        return out[: cnt.value]
+
+    def stress(self, rid, include_kinetic=False):
+        out = np.zeros(6)
+        check(lib().b2md_replica_stress(self._h, rid, int(include_kinetic), _ptr(out)))
+        return out
+
+    def calc_f(self, stress=False):
+        check(lib().b2md_calc_f(self._h, int(stress)))
+
+    def integrate(self):
+        check(lib().b2md_integrate(self._h))
+
+    def zero_momentum(self):
+        check(lib().b2md_zero_momentum(self._h))
+
+    def run(self, nsteps):
+        check(lib().b2md_run(self._h, int(nsteps)))
+
+    def queue(self, rid, nsteps):
+        check(lib().b2md_replica_queue_steps(self._h, rid, int(nsteps)))
+
+    def run_queued(self, max_steps=0):
+        n = ctypes.c_longlong()
+        check(lib().b2md_run_queued(self._h, int(max_steps), ctypes.byref(n)))
+        return n.value
+
+    def nbl(self, rid, n, max_nbrs):
+        counts = np.zeros(n, np.uint32)
+        nbl = np.zeros((n, max_nbrs), np.uint32)
+        check(lib().b2md_nbl_export(self._h, rid, _ptr(counts), _ptr(nbl), max_nbrs))
+        return counts, nbl
+
+    def sort_index(self, rid, n):
+        out = np.zeros(n, np.uint32)
+        check(lib().b2md_sort_export(self._h, rid, _ptr(out)))
+        return out
+
+    def cell_grid(self, rid):
+        out = np.zeros(3, np.int32)
+        check(lib().b2md_cell_grid(self._h, rid, _ptr(out)))
+        return out
+
+    def sync(self):
+        check(lib().b2md_sync(self._h))
+
+
+def probe_dist2(a4, b4, box):
+    a4 = np.ascontiguousarray(a4, np.float32)
+    b4 = np.ascontiguousarray(b4, np.float32)
+    box = np.ascontiguousarray(box, np.float32)
+    out = np.zeros((len(a4), 2), np.float32)
+    check(lib().b2md_probe_dist2(_ptr(a4), _ptr(b4), _ptr(box), len(a4), _ptr(out)))
+    return out
+
+
+def probe_cell(x, box, nc):
+    x = np.ascontiguousarray(x, np.float32)
+    out = np.zeros((len(x), 2), np.int32)
+    check(lib().b2md_probe_cell(_ptr(x), len(x), float(box), int(nc), _ptr(out)))
+    return out

@@ -1,0 +1,1221 @@
+// Host side of the B200 RUMD engine: pools in HBM, replica admission, CUDA
+// graphs with device-decided neighbour-list rebuilds, and the C ABI declared
+// in include/rumd_b200.h.
+#include "../../include/rumd_b200.h"
+#include "kernels.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+using namespace b2md;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+struct CudaErr {
+  cudaError_t e;
+  const char* what;
+  int line;
+};
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) throw CudaErr{e_, #call, __LINE__};     \
+  } while (0)
+
+struct ApiErr {
+  int code;
+  std::string msg;
+};
+
+[[noreturn]] void api_fail(int code, const std::string& m) { throw ApiErr{code, m}; }
+
+// First-fit allocator of [0, cap) ranges, alignment in units.
+struct RangeAlloc {
+  long long cap = 0;
+  std::map<long long, long long> free_;  // offset -> size
+  void init(long long c) { cap = c; free_.clear(); if (c > 0) free_[0] = c; }
+  void grow(long long c) {
+    if (c <= cap) return;
+    long long old = cap;
+    cap = c;
+    auto it = free_.end();
+    if (!free_.empty()) {
+      --it;
+      if (it->first + it->second == old) { it->second += c - old; return; }
+    }
+    free_[old] = c - old;
+  }
+  long long alloc(long long n, long long align) {
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      long long off = (it->first + align - 1) / align * align;
+      long long pad = off - it->first;
+      if (pad + n <= it->second) {
+        long long start = it->first, size = it->second;
+        free_.erase(it);
+        if (pad > 0) free_[start] = pad;
+        if (size - pad - n > 0) free_[off + n] = size - pad - n;
+        return off;
+      }
+    }
+    return -1;
+  }
+  void release(long long off, long long n) {
+    if (n <= 0) return;
+    auto it = free_.emplace(off, n).first;
+    auto nx = std::next(it);
+    if (nx != free_.end() && it->first + it->second == nx->first) { it->second += nx->second; free_.erase(nx); }
+    if (it != free_.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) { pv->second += it->second; free_.erase(it); }
+    }
+  }
+  long long used_end() const {
+    if (free_.empty()) return cap;
+    auto it = std::prev(free_.end());
+    return it->first + it->second == cap ? it->first : cap;
+  }
+};
+
+struct HostRep {
+  bool active = false;
+  int n = 0, np = 0;           // particles, padded
+  long long p0 = -1;
+  long long nbl0 = -1, nbl_len = 0;
+  long long cell0 = -1;
+  int ncell = 0;
+  long long par0 = -1;
+  int npar = 0;
+  long long elog0 = -1;
+  int ecap = 0;
+  RepDev d{};
+  float rcmax = 0.f, skin = 0.f;
+  std::vector<float> params;   // RUMD layout
+  int nb_method_req = -1;      // -1 default
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  long long n = 0;
+};
+
+}  // namespace
+
+struct b2md_engine {
+  int device = 0;
+  cudaStream_t stream = nullptr, cap_stream = nullptr;
+  int pb = 64, tp = 4;
+  int cond_mode = 1;
+  // pools
+  long long pcap = 0, ecap = 0, ccap = 0, qcap = 0, zcap = 0;
+  int rcap = 0;
+  RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
+  float4* r[2] = {nullptr, nullptr};
+  float4* v[2] = {nullptr, nullptr};
+  int4* im[2] = {nullptr, nullptr};
+  unsigned* uidx[2] = {nullptr, nullptr};
+  float4 *f = nullptr, *w = nullptr, *sts = nullptr, *last_r = nullptr;
+  unsigned *nn = nullptr, *order = nullptr;
+  int *key = nullptr, *slot = nullptr;
+  unsigned* nbl = nullptr;
+  int *cnt = nullptr, *cstart = nullptr;
+  float* par = nullptr;
+  double* elog = nullptr;
+  RepDev* rep = nullptr;
+  RepState* st = nullptr;
+  unsigned* rctr = nullptr;
+  // tiles
+  int ntiles = 0, tcap = 0, ngroups = 0, gcap = 0;
+  int *tile_rep = nullptr, *tile_first = nullptr, *ctot = nullptr, *cpref = nullptr;
+  double *tpart = nullptr, *gpart = nullptr;
+  unsigned* gctr = nullptr;
+  unsigned* fctr = nullptr;
+  int* any_rebuild = nullptr;
+  std::vector<HostRep> reps;
+  // graphs
+  bool graphs_valid = false;
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // [0]: 1 step, [1]: kChunk steps
+  cudaGraph_t graph[2] = {nullptr, nullptr};
+  long long bytes = 0;
+};
+
+namespace {
+
+constexpr int kChunk = 32;
+
+template <class T>
+void dev_grow(b2md_engine* e, T*& p, long long old_n, long long new_n, bool zero_new) {
+  T* np = nullptr;
+  CK(cudaMalloc(&np, (size_t)std::max<long long>(new_n, 1) * sizeof(T)));
+  e->bytes += (new_n - old_n) * (long long)sizeof(T);
+  if (p && old_n > 0) CK(cudaMemcpyAsync(np, p, (size_t)old_n * sizeof(T), cudaMemcpyDeviceToDevice, e->stream));
+  if (zero_new && new_n > old_n)
+    CK(cudaMemsetAsync(np + old_n, 0, (size_t)(new_n - old_n) * sizeof(T), e->stream));
+  if (p) {
+    CK(cudaStreamSynchronize(e->stream));
+    CK(cudaFree(p));
+  }
+  p = np;
+}
+
+void invalidate_graphs(b2md_engine* e) {
+  for (int k = 0; k < 2; ++k) {
+    if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
+    if (e->graph[k]) cudaGraphDestroy(e->graph[k]);
+    e->gexec[k] = nullptr;
+    e->graph[k] = nullptr;
+  }
+  e->graphs_valid = false;
+}
+
+void grow_particles(b2md_engine* e, long long need) {
+  if (need <= e->pcap) return;
+  long long nc = std::max(need, e->pcap * 2);
+  nc = (nc + 31) / 32 * 32;
+  for (int k = 0; k < 2; ++k) {
+    dev_grow(e, e->r[k], e->pcap, nc, true);
+    dev_grow(e, e->v[k], e->pcap, nc, true);
+    dev_grow(e, e->im[k], e->pcap, nc, true);
+    dev_grow(e, e->uidx[k], e->pcap, nc, true);
+  }
+  dev_grow(e, e->f, e->pcap, nc, true);
+  dev_grow(e, e->w, e->pcap, nc, true);
+  dev_grow(e, e->sts, e->pcap, nc, true);
+  dev_grow(e, e->last_r, e->pcap, nc, true);
+  dev_grow(e, e->nn, e->pcap, nc, true);
+  dev_grow(e, e->order, e->pcap, nc, true);
+  dev_grow(e, e->key, e->pcap, nc, true);
+  dev_grow(e, e->slot, e->pcap, nc, true);
+  e->palloc.grow(nc);
+  e->pcap = nc;
+  invalidate_graphs(e);
+}
+
+void grow_list(b2md_engine* e, long long need) {
+  if (need <= e->ecap) return;
+  long long nc = std::max(need, e->ecap + e->ecap / 2);
+  dev_grow(e, e->nbl, e->ecap, nc, false);
+  e->ealloc.grow(nc);
+  e->ecap = nc;
+  invalidate_graphs(e);
+}
+
+void grow_cells(b2md_engine* e, long long need) {
+  if (need <= e->ccap) return;
+  long long nc = std::max(need, e->ccap * 2);
+  dev_grow(e, e->cnt, e->ccap, nc, true);
+  dev_grow(e, e->cstart, e->ccap, nc, true);
+  e->calloc.grow(nc);
+  e->ccap = nc;
+  invalidate_graphs(e);
+}
+
+void grow_params(b2md_engine* e, long long need) {
+  if (need <= e->qcap) return;
+  long long nc = std::max(need, std::max<long long>(e->qcap * 2, 1024));
+  dev_grow(e, e->par, e->qcap, nc, true);
+  e->qalloc.grow(nc);
+  e->qcap = nc;
+  invalidate_graphs(e);
+}
+
+void grow_elog(b2md_engine* e, long long need) {
+  if (need <= e->zcap) return;
+  long long nc = std::max(need, e->zcap * 2);
+  dev_grow(e, e->elog, e->zcap * 5, nc * 5, true);
+  e->zalloc.grow(nc);
+  e->zcap = nc;
+  invalidate_graphs(e);
+}
+
+void grow_reps(b2md_engine* e, int need) {
+  if (need <= e->rcap) return;
+  int nc = std::max(need, std::max(e->rcap * 2, 8));
+  dev_grow(e, e->rep, e->rcap, nc, true);
+  dev_grow(e, e->st, e->rcap, nc, true);
+  dev_grow(e, e->rctr, e->rcap, nc, true);
+  e->rcap = nc;
+  invalidate_graphs(e);
+}
+
+EngArgs make_args(b2md_engine* e) {
+  EngArgs a;
+  for (int k = 0; k < 2; ++k) { a.r[k] = e->r[k]; a.v[k] = e->v[k]; a.im[k] = e->im[k]; a.uidx[k] = e->uidx[k]; }
+  a.f = e->f; a.w = e->w; a.sts = e->sts; a.last_r = e->last_r; a.nn = e->nn; a.nbl = e->nbl;
+  a.key = e->key; a.slot = e->slot; a.order = e->order; a.cnt = e->cnt; a.cstart = e->cstart;
+  a.ctot = e->ctot; a.cpref = e->cpref; a.par = e->par; a.rep = e->rep; a.st = e->st;
+  a.tile_rep = e->tile_rep; a.tile_first = e->tile_first; a.tpart = e->tpart; a.gpart = e->gpart;
+  a.gctr = e->gctr; a.rctr = e->rctr; a.fctr = e->fctr; a.any_rebuild = e->any_rebuild; a.elog = e->elog;
+  a.ntiles = e->ntiles;
+  a.nrep = (int)e->reps.size();
+  return a;
+}
+
+// Re-lays out tiles and reduction groups over the active replicas and uploads
+// the replica table.
+void relayout(b2md_engine* e) {
+  int T = 0, G = 0;
+  for (auto& h : e->reps) {
+    if (!h.active) { h.d.tile0 = T; h.d.ntiles = 0; h.d.group0 = G; h.d.ngroups = 0; h.d.active = 0; continue; }
+    h.d.tile0 = T;
+    h.d.ntiles = (h.n + e->pb - 1) / e->pb;
+    h.d.group0 = G;
+    h.d.ngroups = (h.d.ntiles + kGroup - 1) / kGroup;
+    T += h.d.ntiles;
+    G += h.d.ngroups;
+  }
+  if (T > e->tcap) {
+    int nc = std::max(T, e->tcap * 2);
+    dev_grow(e, e->tile_rep, e->tcap, nc, true);
+    dev_grow(e, e->tile_first, e->tcap, nc, true);
+    dev_grow(e, e->ctot, e->tcap, nc, true);
+    dev_grow(e, e->cpref, e->tcap, nc, true);
+    dev_grow(e, e->tpart, (long long)e->tcap * kNPart, (long long)nc * kNPart, true);
+    e->tcap = nc;
+  }
+  if (G > e->gcap) {
+    int nc = std::max(G, e->gcap * 2);
+    dev_grow(e, e->gpart, (long long)e->gcap * kNPart, (long long)nc * kNPart, true);
+    dev_grow(e, e->gctr, e->gcap, nc, true);
+    e->gcap = nc;
+  }
+  std::vector<int> trep(T), tfirst(T);
+  for (size_t r = 0; r < e->reps.size(); ++r) {
+    const HostRep& h = e->reps[r];
+    for (int t = 0; t < h.d.ntiles; ++t) {
+      trep[h.d.tile0 + t] = (int)r;
+      tfirst[h.d.tile0 + t] = t * e->pb;
+    }
+  }
+  if (T > 0) {
+    CK(cudaMemcpyAsync(e->tile_rep, trep.data(), T * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->tile_first, tfirst.data(), T * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  }
+  std::vector<RepDev> table(e->reps.size());
+  for (size_t r = 0; r < e->reps.size(); ++r) table[r] = e->reps[r].d;
+  if (!table.empty())
+    CK(cudaMemcpyAsync(e->rep, table.data(), table.size() * sizeof(RepDev), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  e->ntiles = T;
+  e->ngroups = G;
+  invalidate_graphs(e);
+}
+
+void upload_rep(b2md_engine* e, int id) {
+  const HostRep& h = e->reps[id];
+  CK(cudaMemcpyAsync(e->rep + id, &h.d, sizeof(RepDev), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+}
+
+HostRep& get_rep(b2md_engine* e, int id) {
+  if (!e) api_fail(B2MD_ERR_ARG, "null engine");
+  if (id < 0 || id >= (int)e->reps.size() || !e->reps[id].active) api_fail(B2MD_ERR_ARG, "no replica with this id");
+  return e->reps[id];
+}
+
+RepState read_state(b2md_engine* e, int id) {
+  RepState s;
+  CK(cudaMemcpyAsync(&s, e->st + id, sizeof(RepState), cudaMemcpyDeviceToHost, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+  return s;
+}
+
+std::vector<RepState> read_states(b2md_engine* e) {
+  std::vector<RepState> s(e->reps.size());
+  if (!s.empty()) {
+    CK(cudaMemcpyAsync(s.data(), e->st, s.size() * sizeof(RepState), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  }
+  return s;
+}
+
+template <class T>
+void write_field(b2md_engine* e, int id, size_t off, const T& val) {
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(e->st + id) + off, &val, sizeof(T), cudaMemcpyHostToDevice, e->stream));
+  CK(cudaStreamSynchronize(e->stream));
+}
+#define WRITE_STATE(e, id, field, val) write_field(e, id, offsetof(RepState, field), (decltype(RepState::field))(val))
+
+// Packs a RUMD parameter table into the engine's per-pair rows and derives
+// the cell grid (NeighborList.cu:717-732).
+void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, float skin) {
+  if (ntypes < 1 || ntypes > kMaxTypes) api_fail(B2MD_ERR_ARG, "ntypes must be 1..8");
+  if (cutoff < 0 || cutoff > 2) api_fail(B2MD_ERR_ARG, "cutoff method must be NS, SP or SF");
+  if (!(skin >= 0.f)) api_fail(B2MD_ERR_ARG, "skin must be >= 0");
+  h.params.assign(params, params + ntypes * ntypes * kNumParam);
+  h.d.ntypes = ntypes;
+  h.d.cutoff = cutoff;
+  h.skin = skin;
+  h.rcmax = 0.f;
+  for (int k = 0; k < ntypes * ntypes; ++k) h.rcmax = std::max(h.rcmax, params[k * kNumParam]);
+  if (!(h.rcmax > 0.f)) api_fail(B2MD_ERR_ARG, "all cut-offs are zero");
+  h.d.skin2_4 = (float)(0.25 * skin * skin);
+  int ncheck[3];
+  for (int d = 0; d < 3; ++d) {
+    float q = 2 * h.d.L[d] / (h.rcmax + skin);
+    ncheck[d] = (int)floor(q);
+    h.d.nc[d] = ncheck[d] < 5 ? 5 : ncheck[d];
+  }
+  bool grid_complete = ncheck[0] >= 5 && ncheck[1] >= 5 && ncheck[2] >= 5;
+  if (h.nb_method_req == NB_CELLS) h.d.nb_method = NB_CELLS;
+  else if (h.nb_method_req == NB_N2) h.d.nb_method = NB_N2;
+  else h.d.nb_method = grid_complete ? NB_CELLS : NB_N2;
+}
+
+std::vector<float> pack_params(const HostRep& h) {
+  int T = h.d.ntypes;
+  std::vector<float> out(T * T * kParStride, 0.f);
+  for (int k = 0; k < T * T; ++k) {
+    const float* p = &h.params[k * kNumParam];
+    float* q = &out[k * kParStride];
+    float rc = p[0];
+    q[0] = rc * rc;
+    q[1] = p[1];
+    q[2] = p[2];
+    q[3] = p[kNumParam - 2];
+    q[4] = p[kNumParam - 1];
+    q[5] = rc;
+    float cs = rc + h.skin;  // calculateNBL_*: (params + skin)^2 in float
+    q[6] = cs * cs;
+    q[7] = 0.f;
+  }
+  return out;
+}
+
+int estimate_max_nbrs(const HostRep& h) {
+  double V = (double)h.d.L[0] * h.d.L[1] * h.d.L[2];
+  double rs = (double)h.rcmax + h.skin;
+  double est = 1.5 * (4.0 / 3.0) * M_PI * rs * rs * rs * h.n / V;
+  int m = (int)std::ceil(est);
+  m = std::max(m, 32);
+  m = std::min(m, std::max(h.n - 1, 1));
+  return m;
+}
+
+void place_cells(b2md_engine* e, HostRep& h) {
+  int ncell = h.d.nc[0] * h.d.nc[1] * h.d.nc[2];
+  if (h.cell0 >= 0 && h.ncell == ncell) return;
+  if (h.cell0 >= 0) e->calloc.release(h.cell0, h.ncell);
+  long long off = e->calloc.alloc(ncell, 1);
+  if (off < 0) {
+    grow_cells(e, e->ccap + ncell);
+    off = e->calloc.alloc(ncell, 1);
+  }
+  h.cell0 = off;
+  h.ncell = ncell;
+  h.d.cell0 = (int)off;
+  h.d.ncell = ncell;
+}
+
+void place_params(b2md_engine* e, HostRep& h) {
+  std::vector<float> packed = pack_params(h);
+  int np = (int)packed.size();
+  if (h.par0 < 0 || h.npar != np) {
+    if (h.par0 >= 0) e->qalloc.release(h.par0, h.npar);
+    long long off = e->qalloc.alloc(np, 8);
+    if (off < 0) {
+      grow_params(e, e->qcap + np + 8);
+      off = e->qalloc.alloc(np, 8);
+    }
+    h.par0 = off;
+    h.npar = np;
+    h.d.par0 = (int)off;
+  }
+  CK(cudaMemcpyAsync(e->par + h.par0, packed.data(), np * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+}
+
+void place_list(b2md_engine* e, HostRep& h, int max_nbrs) {
+  long long len = (long long)max_nbrs * h.np;
+  if (h.nbl0 >= 0) e->ealloc.release(h.nbl0, h.nbl_len);
+  long long off = e->ealloc.alloc(len, 32);
+  if (off < 0) {
+    grow_list(e, e->ealloc.used_end() + len + 32);
+    off = e->ealloc.alloc(len, 32);
+    if (off < 0) api_fail(B2MD_ERR_NOMEM, "neighbour-list pool exhausted");
+  }
+  h.nbl0 = off;
+  h.nbl_len = len;
+  h.d.nbl0 = off;
+  h.d.max_nbrs = max_nbrs;
+  h.d.nbl_stride = h.np;
+}
+
+// ---- launches ----
+void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
+  const int T = e->ntiles;
+  const int R = (int)e->reps.size();
+  if (T == 0) return;
+  int maxt = 1;
+  for (auto& h : e->reps) if (h.active) maxt = std::max(maxt, h.d.ntypes);
+  k_rb_begin<<<(R + 127) / 128, 128, 0, s>>>(a);
+  k_rb_clear<<<T, e->pb, 0, s>>>(a);
+  k_rb_count<<<T, e->pb, 0, s>>>(a);
+  k_rb_scan_local<<<T, e->pb, 0, s>>>(a);
+  k_rb_scan_tiles<<<R, 256, 0, s>>>(a);
+  k_rb_scatter<<<T, e->pb, 0, s>>>(a);
+  k_rb_fix<<<T, e->pb, 0, s>>>(a);
+  k_rb_permute<<<T, e->pb, 0, s>>>(a);
+  k_rb_build<<<T, e->pb, maxt * maxt * sizeof(float), s>>>(a);
+}
+
+int max_types(b2md_engine* e) {
+  int m = 1;
+  for (auto& h : e->reps) if (h.active) m = std::max(m, h.d.ntypes);
+  return m;
+}
+
+typedef void (*ForceFn)(EngArgs, int, cudaGraphConditionalHandle);
+
+ForceFn force_fn(int tp, bool fused, bool stress) {
+#define SEL(TPV)                                               \
+  if (tp == TPV) {                                             \
+    if (fused) return k_force<TPV, true, false>;               \
+    return stress ? k_force<TPV, false, true> : k_force<TPV, false, false>; \
+  }
+  SEL(1) SEL(2) SEL(4) SEL(8)
+#undef SEL
+  return nullptr;
+}
+
+void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
+  if (e->ntiles == 0) return;
+  int mt = max_types(e);
+  size_t smem = (size_t)mt * mt * kParStride * sizeof(float);
+  ForceFn fn = force_fn(e->tp, fused, stress);
+  fn<<<e->ntiles, e->pb * e->tp, smem, s>>>(a, 0, cudaGraphConditionalHandle{});
+}
+
+void check_launch() { CK(cudaGetLastError()); }
+
+// Builds the step graphs: [gate] -> K x { IF(rebuild) {rebuild kernels} ; fused step }.
+void build_graph(b2md_engine* e, int which, int K) {
+  EngArgs a = make_args(e);
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  const int mt = max_types(e);
+  const size_t smem = (size_t)mt * mt * kParStride * sizeof(float);
+  ForceFn fstep = force_fn(e->tp, true, false);
+  if (e->cond_mode) {
+    std::vector<cudaGraphConditionalHandle> hs(K);
+    for (int k = 0; k < K; ++k) CK(cudaGraphConditionalHandleCreate(&hs[k], g, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t prev;
+    {
+      cudaKernelNodeParams kp = {};
+      void* args[] = {&a, &hs[0]};
+      kp.func = (void*)k_gate;
+      kp.gridDim = dim3(1);
+      kp.blockDim = dim3(256);
+      kp.kernelParams = args;
+      CK(cudaGraphAddKernelNode(&prev, g, nullptr, 0, &kp));
+    }
+    for (int k = 0; k < K; ++k) {
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = hs[k];
+      cp.conditional.type = cudaGraphCondTypeIf;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cnode;
+      CK(cudaGraphAddNode(&cnode, g, &prev, 1, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      CK(cudaStreamBeginCaptureToGraph(e->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      launch_rebuild(e, e->cap_stream, a);
+      cudaGraph_t captured;
+      CK(cudaStreamEndCapture(e->cap_stream, &captured));
+      int has_next = (k + 1 < K) ? 1 : 0;
+      cudaGraphConditionalHandle hn = has_next ? hs[k + 1] : cudaGraphConditionalHandle{};
+      cudaKernelNodeParams kp = {};
+      void* args[] = {&a, &has_next, &hn};
+      kp.func = (void*)fstep;
+      kp.gridDim = dim3(e->ntiles);
+      kp.blockDim = dim3(e->pb * e->tp);
+      kp.sharedMemBytes = (unsigned)smem;
+      kp.kernelParams = args;
+      cudaGraphNode_t knode;
+      CK(cudaGraphAddKernelNode(&knode, g, &cnode, 1, &kp));
+      prev = knode;
+    }
+  } else {
+    cudaGraph_t captured;
+    CK(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < K; ++k) {
+      launch_rebuild(e, e->cap_stream, a);
+      fstep<<<e->ntiles, e->pb * e->tp, smem, e->cap_stream>>>(a, 0, cudaGraphConditionalHandle{});
+    }
+    CK(cudaStreamEndCapture(e->cap_stream, &captured));
+    CK(cudaGraphDestroy(g));
+    g = captured;
+  }
+  cudaGraphExec_t ex;
+  CK(cudaGraphInstantiate(&ex, g, 0));
+  e->graph[which] = g;
+  e->gexec[which] = ex;
+}
+
+void ensure_graphs(b2md_engine* e) {
+  if (e->graphs_valid) return;
+  invalidate_graphs(e);
+  build_graph(e, 0, 1);
+  build_graph(e, 1, kChunk);
+  e->graphs_valid = true;
+}
+
+// Overflowed lists: double the capacity (NeighborList.cu:657-676) and flag a rebuild.
+bool repair_overflow(b2md_engine* e) {
+  std::vector<RepState> s = read_states(e);
+  bool any = false;
+  for (size_t r = 0; r < e->reps.size(); ++r) {
+    HostRep& h = e->reps[r];
+    if (!h.active || !s[r].overflow) continue;
+    int want = std::max(h.d.max_nbrs * 2, s[r].actual_max_nbrs + 8);
+    want = std::min(want, std::max(h.n - 1, 1));
+    if (want <= h.d.max_nbrs) api_fail(B2MD_ERR_OVERFLOW, "neighbour list cannot grow further");
+    place_list(e, h, want);
+    upload_rep(e, (int)r);
+    WRITE_STATE(e, (int)r, overflow, 0);
+    WRITE_STATE(e, (int)r, rebuild, 1);
+    any = true;
+  }
+  if (any) invalidate_graphs(e);
+  return any;
+}
+
+void calc_f(b2md_engine* e, bool stress) {
+  for (int attempt = 0; attempt < 8; ++attempt) {
+    EngArgs a = make_args(e);
+    launch_rebuild(e, e->stream, a);
+    launch_force(e, e->stream, a, false, stress);
+    check_launch();
+    if (!repair_overflow(e)) return;
+  }
+  api_fail(B2MD_ERR_OVERFLOW, "neighbour list overflow persists");
+}
+
+long long max_steps_left(b2md_engine* e) {
+  std::vector<RepState> s = read_states(e);
+  long long m = 0;
+  for (size_t r = 0; r < e->reps.size(); ++r)
+    if (e->reps[r].active && !s[r].overflow) m = std::max(m, s[r].steps_left);
+  return m;
+}
+
+// Runs up to `limit` steps of the queued work with the step graphs.
+long long run_steps(b2md_engine* e, long long limit) {
+  long long done = 0;
+  for (int guard = 0; guard < 64; ++guard) {
+    long long todo = std::min(max_steps_left(e), limit - done);
+    if (todo <= 0) break;
+    ensure_graphs(e);
+    long long big = todo / kChunk, small = todo % kChunk;
+    for (long long k = 0; k < big; ++k) CK(cudaGraphLaunch(e->gexec[1], e->stream));
+    for (long long k = 0; k < small; ++k) CK(cudaGraphLaunch(e->gexec[0], e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    done += todo;
+    if (!repair_overflow(e)) {
+      // replicas that were frozen by an overflow keep their queue; others are done
+      if (max_steps_left(e) == 0) break;
+    }
+    done = std::min(done, limit);
+  }
+  return done;
+}
+
+template <class F>
+int guarded(F&& fn) {
+  try {
+    fn();
+    return B2MD_OK;
+  } catch (const ApiErr& x) {
+    g_err = x.msg;
+    return x.code;
+  } catch (const CudaErr& x) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "CUDA error %s (%s) at engine.cu:%d: %s", cudaGetErrorName(x.e),
+             cudaGetErrorString(x.e), x.line, x.what);
+    g_err = buf;
+    cudaGetLastError();
+    return x.e == cudaErrorMemoryAllocation ? B2MD_ERR_NOMEM : B2MD_ERR_CUDA;
+  } catch (const std::bad_alloc&) {
+    g_err = "host allocation failed";
+    return B2MD_ERR_NOMEM;
+  }
+}
+
+void launch_momentum(b2md_engine* e) {
+  if (e->ntiles == 0) return;
+  EngArgs a = make_args(e);
+  k_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+  check_launch();
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+extern "C" {
+
+const char* b2md_last_error(void) { return g_err.c_str(); }
+const char* b2md_version(void) { return "rumd_b200 0.1 (sm_100a)"; }
+
+int b2md_engine_create(int device, long long max_particles, int max_replicas, long long max_list_entries,
+                       int pb, int tp, b2md_engine** out) {
+  if (!out) return fail(B2MD_ERR_ARG, "out is null");
+  *out = nullptr;
+  if (tp != 1 && tp != 2 && tp != 4 && tp != 8) return fail(B2MD_ERR_ARG, "tp must be 1, 2, 4 or 8");
+  if (pb < 32 || pb % 32 || pb * tp > kMaxBlock) return fail(B2MD_ERR_ARG, "pb must be a multiple of 32 with pb*tp <= 512");
+  b2md_engine* e = new b2md_engine();
+  int rc = guarded([&] {
+    CK(cudaSetDevice(device));
+    e->device = device;
+    CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&e->cap_stream, cudaStreamNonBlocking));
+    e->pb = pb;
+    e->tp = tp;
+    e->palloc.init(0);
+    e->ealloc.init(0);
+    e->calloc.init(0);
+    e->qalloc.init(0);
+    e->zalloc.init(0);
+    grow_particles(e, std::max<long long>(max_particles, 32));
+    grow_list(e, std::max<long long>(max_list_entries, 1024));
+    grow_cells(e, 1024);
+    grow_params(e, 1024);
+    grow_elog(e, 16);
+    grow_reps(e, std::max(max_replicas, 1));
+    CK(cudaMalloc(&e->fctr, sizeof(unsigned)));
+    CK(cudaMalloc(&e->any_rebuild, sizeof(int)));
+    CK(cudaMemsetAsync(e->fctr, 0, sizeof(unsigned), e->stream));
+    CK(cudaMemsetAsync(e->any_rebuild, 0, sizeof(int), e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  });
+  if (rc != B2MD_OK) {
+    b2md_engine_destroy(e);
+    return rc;
+  }
+  *out = e;
+  return B2MD_OK;
+}
+
+int b2md_engine_destroy(b2md_engine* e) {
+  if (!e) return B2MD_OK;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamSynchronize(e->stream);
+  invalidate_graphs(e);
+  void* ptrs[] = {e->r[0], e->r[1], e->v[0], e->v[1], e->im[0], e->im[1], e->uidx[0], e->uidx[1], e->f, e->w,
+                  e->sts, e->last_r, e->nn, e->order, e->key, e->slot, e->nbl, e->cnt, e->cstart, e->par, e->elog,
+                  e->rep, e->st, e->rctr, e->tile_rep, e->tile_first, e->ctot, e->cpref, e->tpart, e->gpart,
+                  e->gctr, e->fctr, e->any_rebuild};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
+  delete e;
+  return B2MD_OK;
+}
+
+int b2md_engine_set_launch(b2md_engine* e, int pb, int tp) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  if (tp != 1 && tp != 2 && tp != 4 && tp != 8) return fail(B2MD_ERR_ARG, "tp must be 1, 2, 4 or 8");
+  if (pb < 32 || pb % 32 || pb * tp > kMaxBlock) return fail(B2MD_ERR_ARG, "pb must be a multiple of 32 with pb*tp <= 512");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    e->pb = pb;
+    e->tp = tp;
+    relayout(e);
+  });
+}
+
+int b2md_engine_memory(b2md_engine* e, long long* bytes) {
+  if (!e || !bytes) return fail(B2MD_ERR_ARG, "null argument");
+  *bytes = e->bytes;
+  return B2MD_OK;
+}
+
+int b2md_engine_set_graph_mode(b2md_engine* e, int conditional) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  e->cond_mode = conditional ? 1 : 0;
+  invalidate_graphs(e);
+  return B2MD_OK;
+}
+
+int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* pos4, const float* vel4,
+                     const int* im3, int* id_out) {
+  if (!e || !d || !pos4 || !id_out) return fail(B2MD_ERR_ARG, "null argument");
+  if (d->n < 2) return fail(B2MD_ERR_ARG, "need at least 2 particles");
+  for (int k = 0; k < 3; ++k)
+    if (!(d->box[k] > 0.f)) return fail(B2MD_ERR_ARG, "box lengths must be positive");
+  if (!d->params) return fail(B2MD_ERR_ARG, "params is null");
+  if (!(d->dt > 0.f)) return fail(B2MD_ERR_ARG, "dt must be positive");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    int id = -1;
+    for (size_t r = 0; r < e->reps.size(); ++r)
+      if (!e->reps[r].active) { id = (int)r; break; }
+    if (id < 0) {
+      id = (int)e->reps.size();
+      grow_reps(e, id + 1);
+      e->reps.emplace_back();
+    }
+    HostRep h;
+    h.n = d->n;
+    h.np = (d->n + 31) / 32 * 32;
+    h.d.n = d->n;
+    for (int k = 0; k < 3; ++k) {
+      h.d.L[k] = d->box[k];
+      h.d.invL[k] = 1.f / d->box[k];
+    }
+    set_potential(h, d->ntypes, d->params, d->cutoff_method, d->skin);
+    // types must be in range
+    for (int i = 0; i < d->n; ++i) {
+      int t;
+      std::memcpy(&t, &pos4[4 * i + 3], 4);
+      if (t < 0 || t >= d->ntypes) api_fail(B2MD_ERR_ARG, "particle type out of range");
+    }
+    h.d.dt = d->dt;
+    h.d.omega2 = (float)(4. * M_PI * M_PI / (d->tau * d->tau));
+    h.d.thermo_mask = d->thermostat_mask;
+    h.d.reset_interval = d->reset_interval;
+    h.d.dof = 3.0 * d->n - 3.0;
+    h.d.energy_interval = d->energy_interval;
+    h.d.active = 1;
+    // particle segment
+    long long p0 = e->palloc.alloc(h.np, 32);
+    if (p0 < 0) {
+      grow_particles(e, e->palloc.used_end() + h.np + 32);
+      p0 = e->palloc.alloc(h.np, 32);
+      if (p0 < 0) api_fail(B2MD_ERR_NOMEM, "particle pool exhausted");
+    }
+    h.p0 = p0;
+    h.d.p0 = (int)p0;
+    place_cells(e, h);
+    place_params(e, h);
+    place_list(e, h, d->max_nbrs > 0 ? d->max_nbrs : estimate_max_nbrs(h));
+    if (d->energy_interval > 0 && d->energy_capacity > 0) {
+      long long z = e->zalloc.alloc(d->energy_capacity, 1);
+      if (z < 0) {
+        grow_elog(e, e->zalloc.used_end() + d->energy_capacity);
+        z = e->zalloc.alloc(d->energy_capacity, 1);
+      }
+      h.elog0 = z;
+      h.ecap = d->energy_capacity;
+      h.d.elog0 = z;
+      h.d.energy_cap = d->energy_capacity;
+    } else {
+      h.d.energy_interval = 0;
+      h.d.energy_cap = 0;
+    }
+    h.active = true;
+    // upload particle data (slot order = original order until the first sort)
+    std::vector<int4> imv(h.n);
+    std::vector<unsigned> ids(h.n);
+    std::vector<float4> vv(h.n);
+    for (int i = 0; i < h.n; ++i) {
+      imv[i] = im3 ? make_int4(im3[3 * i], im3[3 * i + 1], im3[3 * i + 2], 0) : make_int4(0, 0, 0, 0);
+      ids[i] = (unsigned)i;
+      vv[i] = vel4 ? make_float4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], vel4[4 * i + 3])
+                   : make_float4(0.f, 0.f, 0.f, 1.f);
+      if (!(vv[i].w > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass (vel4[.,3]) must be positive");
+    }
+    CK(cudaMemcpyAsync(e->r[0] + p0, pos4, h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->last_r + p0, pos4, h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->v[0] + p0, vv.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->im[0] + p0, imv.data(), h.n * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->uidx[0] + p0, ids.data(), h.n * sizeof(unsigned), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemsetAsync(e->f + p0, 0, h.np * sizeof(float4), e->stream));
+    CK(cudaMemsetAsync(e->w + p0, 0, h.np * sizeof(float4), e->stream));
+    CK(cudaMemsetAsync(e->sts + p0, 0, h.np * sizeof(float4), e->stream));
+    CK(cudaMemsetAsync(e->nn + p0, 0, h.np * sizeof(unsigned), e->stream));
+    RepState s;
+    std::memset(&s, 0, sizeof(s));
+    s.xi = d->xi;
+    s.T = d->target_T;
+    s.dT = d->dT_per_step;
+    s.rebuild = 1;
+    CK(cudaMemcpyAsync(e->st + id, &s, sizeof(RepState), cudaMemcpyHostToDevice, e->stream));
+    e->reps[id] = h;
+    relayout(e);
+    launch_momentum(e);
+    CK(cudaStreamSynchronize(e->stream));
+    *id_out = id;
+  });
+}
+
+int b2md_replica_remove(b2md_engine* e, int id) {
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    e->palloc.release(h.p0, h.np);
+    e->ealloc.release(h.nbl0, h.nbl_len);
+    e->calloc.release(h.cell0, h.ncell);
+    e->qalloc.release(h.par0, h.npar);
+    if (h.elog0 >= 0) e->zalloc.release(h.elog0, h.ecap);
+    h = HostRep();
+    relayout(e);
+  });
+}
+
+int b2md_replica_get(b2md_engine* e, int id, int field, void* out) {
+  if (!out) return fail(B2MD_ERR_ARG, "out is null");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    std::vector<unsigned> ids(h.n);
+    CK(cudaMemcpyAsync(ids.data(), e->uidx[s.abuf] + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    if (field == B2MD_FIELD_IMAGES) {
+      std::vector<int4> tmp(h.n);
+      CK(cudaMemcpyAsync(tmp.data(), e->im[s.abuf] + h.p0, h.n * sizeof(int4), cudaMemcpyDeviceToHost, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      int* o = static_cast<int*>(out);
+      for (int k = 0; k < h.n; ++k) {
+        unsigned i = ids[k];
+        o[3 * i] = tmp[k].x; o[3 * i + 1] = tmp[k].y; o[3 * i + 2] = tmp[k].z;
+      }
+      return;
+    }
+    const float4* src = nullptr;
+    switch (field) {
+      case B2MD_FIELD_POS: src = e->r[s.rbuf]; break;
+      case B2MD_FIELD_VEL: src = e->v[s.abuf]; break;
+      case B2MD_FIELD_FORCE: src = e->f; break;
+      case B2MD_FIELD_VIRIAL: src = e->w; break;
+      case B2MD_FIELD_STRESS: src = e->sts; break;
+      default: api_fail(B2MD_ERR_ARG, "unknown field");
+    }
+    std::vector<float4> tmp(h.n);
+    CK(cudaMemcpyAsync(tmp.data(), src + h.p0, h.n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    float4* o = static_cast<float4*>(out);
+    for (int k = 0; k < h.n; ++k) o[ids[k]] = tmp[k];
+  });
+}
+
+int b2md_replica_set(b2md_engine* e, int id, int field, const void* in) {
+  if (!in) return fail(B2MD_ERR_ARG, "in is null");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    std::vector<unsigned> ids(h.n);
+    CK(cudaMemcpyAsync(ids.data(), e->uidx[s.abuf] + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    if (field == B2MD_FIELD_IMAGES) {
+      const int* src = static_cast<const int*>(in);
+      std::vector<int4> tmp(h.n);
+      for (int k = 0; k < h.n; ++k) {
+        unsigned i = ids[k];
+        tmp[k] = make_int4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0);
+      }
+      CK(cudaMemcpyAsync(e->im[s.abuf] + h.p0, tmp.data(), h.n * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      return;
+    }
+    const float4* src = static_cast<const float4*>(in);
+    std::vector<float4> tmp(h.n);
+    for (int k = 0; k < h.n; ++k) tmp[k] = src[ids[k]];
+    if (field == B2MD_FIELD_POS) {
+      for (int k = 0; k < h.n; ++k) {
+        int t;
+        std::memcpy(&t, &tmp[k].w, 4);
+        if (t < 0 || t >= h.d.ntypes) api_fail(B2MD_ERR_ARG, "particle type out of range");
+      }
+      CK(cudaMemcpyAsync(e->r[s.rbuf] + h.p0, tmp.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      WRITE_STATE(e, id, rebuild, 1);
+    } else if (field == B2MD_FIELD_VEL) {
+      for (int k = 0; k < h.n; ++k)
+        if (!(tmp[k].w > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass must be positive");
+      CK(cudaMemcpyAsync(e->v[s.abuf] + h.p0, tmp.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
+      launch_momentum(e);
+      CK(cudaStreamSynchronize(e->stream));
+    } else {
+      api_fail(B2MD_ERR_ARG, "field cannot be set");
+    }
+  });
+}
+
+int b2md_replica_set_potential(b2md_engine* e, int id, int ntypes, const float* params, int cutoff_method,
+                               float skin) {
+  if (!params) return fail(B2MD_ERR_ARG, "params is null");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    if (ntypes != h.d.ntypes) api_fail(B2MD_ERR_ARG, "number of types cannot change");
+    set_potential(h, ntypes, params, cutoff_method, skin);
+    place_cells(e, h);
+    place_params(e, h);
+    int want = estimate_max_nbrs(h);
+    if (want > h.d.max_nbrs) place_list(e, h, want);
+    upload_rep(e, id);
+    WRITE_STATE(e, id, rebuild, 1);
+    invalidate_graphs(e);
+  });
+}
+
+int b2md_replica_set_integrator(b2md_engine* e, int id, float dt, double target_T, double tau, double dT_per_step,
+                                unsigned thermostat_mask) {
+  if (!(dt > 0.f)) return fail(B2MD_ERR_ARG, "dt must be positive");
+  if (!(tau > 0.0)) return fail(B2MD_ERR_ARG, "tau must be positive");
+  if (target_T < 0.0) return fail(B2MD_ERR_ARG, "targetTemperature is negative");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    h.d.dt = dt;
+    h.d.omega2 = (float)(4. * M_PI * M_PI / (tau * tau));
+    h.d.thermo_mask = thermostat_mask;
+    upload_rep(e, id);
+    WRITE_STATE(e, id, T, target_T);
+    WRITE_STATE(e, id, dT, dT_per_step);
+  });
+}
+
+int b2md_replica_set_xi(b2md_engine* e, int id, double xi) {
+  return guarded([&] {
+    get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    WRITE_STATE(e, id, xi, xi);
+  });
+}
+
+int b2md_replica_set_reset_interval(b2md_engine* e, int id, int reset_interval) {
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    h.d.reset_interval = std::max(reset_interval, 0);
+    upload_rep(e, id);
+  });
+}
+
+int b2md_replica_set_nb_method(b2md_engine* e, int id, int method) {
+  if (method < -1 || method > 1) return fail(B2MD_ERR_ARG, "method must be -1 (default), 0 (sort) or 1 (n2)");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    h.nb_method_req = method;
+    std::vector<float> params = h.params;
+    set_potential(h, h.d.ntypes, params.data(), h.d.cutoff, h.skin);
+    upload_rep(e, id);
+    WRITE_STATE(e, id, rebuild, 1);
+    invalidate_graphs(e);
+  });
+}
+
+int b2md_replica_stats(b2md_engine* e, int id, double* out) {
+  if (!out) return fail(B2MD_ERR_ARG, "out is null");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    out[B2MD_STAT_PE] = s.pe;
+    out[B2MD_STAT_VIRIAL] = s.vir;
+    out[B2MD_STAT_KE] = s.ke_t;
+    out[B2MD_STAT_XI] = s.xi;
+    out[B2MD_STAT_KE2] = s.ke2;
+    out[B2MD_STAT_STEPS] = (double)s.steps;
+    out[B2MD_STAT_REBUILDS] = s.nrebuilds;
+    out[B2MD_STAT_STEPS_LEFT] = (double)s.steps_left;
+    out[B2MD_STAT_OVERFLOW] = s.overflow;
+    out[B2MD_STAT_TARGET_T] = s.T;
+    out[B2MD_STAT_MAX_NBRS] = h.d.max_nbrs;
+    out[B2MD_STAT_ACTUAL_MAX_NBRS] = s.actual_max_nbrs;
+  });
+}
+
+int b2md_replica_energy_log(b2md_engine* e, int id, double* out, int cap, int* count) {
+  if (!out || !count) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    int have = std::min(s.nlog, h.ecap);
+    int first = s.nlog - have;
+    std::vector<double> buf((size_t)h.ecap * 5);
+    if (h.ecap > 0) {
+      CK(cudaMemcpyAsync(buf.data(), e->elog + h.elog0 * 5, buf.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                         e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+    }
+    int nout = std::min(have, cap);
+    for (int k = 0; k < nout; ++k) {
+      int slot = (first + k) % std::max(h.ecap, 1);
+      for (int c = 0; c < 5; ++c) out[5 * k + c] = buf[(size_t)slot * 5 + c];
+    }
+    *count = nout;
+  });
+}
+
+int b2md_replica_stress(b2md_engine* e, int id, int include_kinetic, double* out6) {
+  if (!out6) return fail(B2MD_ERR_ARG, "out is null");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    std::vector<float4> sts(h.n), w(h.n), v(h.n);
+    RepState s = read_state(e, id);
+    CK(cudaMemcpyAsync(sts.data(), e->sts + h.p0, h.n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(w.data(), e->w + h.p0, h.n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(v.data(), e->v[s.abuf] + h.p0, h.n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    // Sample::GetStress (Sample.cu:393-444)
+    double st[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < h.n; ++i) {
+      st[0] += sts[i].x; st[1] += sts[i].y; st[2] += sts[i].z; st[3] += sts[i].w;
+      st[4] += w[i].y; st[5] += w[i].z;
+      if (include_kinetic) {
+        float mass2 = 2.f / v[i].w;
+        st[0] -= mass2 * v[i].x * v[i].x; st[1] -= mass2 * v[i].y * v[i].y; st[2] -= mass2 * v[i].z * v[i].z;
+        st[3] -= mass2 * v[i].y * v[i].z; st[4] -= mass2 * v[i].x * v[i].z; st[5] -= mass2 * v[i].x * v[i].y;
+      }
+    }
+    double V = (double)h.d.L[0] * h.d.L[1] * h.d.L[2];
+    for (int k = 0; k < 6; ++k) out6[k] = 0.5 * st[k] / V;
+  });
+}
+
+int b2md_calc_f(b2md_engine* e, int stress) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    calc_f(e, stress != 0);
+    CK(cudaStreamSynchronize(e->stream));
+  });
+}
+
+int b2md_integrate(b2md_engine* e) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    if (e->ntiles == 0) return;
+    EngArgs a = make_args(e);
+    k_integrate<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    check_launch();
+  });
+}
+
+int b2md_zero_momentum(b2md_engine* e) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    if (e->ntiles == 0) return;
+    EngArgs a = make_args(e);
+    k_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    k_apply_zero_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    k_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    check_launch();
+  });
+}
+
+int b2md_run(b2md_engine* e, long long nsteps) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  if (nsteps < 0) return fail(B2MD_ERR_ARG, "nsteps must be >= 0");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    if (e->ntiles == 0) return;
+    EngArgs a = make_args(e);
+    int R = (int)e->reps.size();
+    k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
+    launch_momentum(e);
+    check_launch();
+    if (nsteps > 0) run_steps(e, nsteps);
+    calc_f(e, false);
+    CK(cudaStreamSynchronize(e->stream));
+  });
+}
+
+int b2md_replica_queue_steps(b2md_engine* e, int id, long long nsteps) {
+  if (nsteps < 0) return fail(B2MD_ERR_ARG, "nsteps must be >= 0");
+  return guarded([&] {
+    get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    WRITE_STATE(e, id, steps_left, s.steps_left + nsteps);
+  });
+}
+
+int b2md_run_queued(b2md_engine* e, long long max_steps, long long* steps_run) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    long long lim = max_steps > 0 ? max_steps : (1LL << 62);
+    long long n = e->ntiles ? run_steps(e, lim) : 0;
+    if (steps_run) *steps_run = n;
+  });
+}
+
+int b2md_nbl_export(b2md_engine* e, int id, unsigned* counts, unsigned* nbl, int max_nbrs) {
+  if (!counts || !nbl) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    std::vector<unsigned> ids(h.n), nn(h.n), lst((size_t)h.d.max_nbrs * h.np);
+    CK(cudaMemcpyAsync(ids.data(), e->uidx[s.abuf] + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(nn.data(), e->nn + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaMemcpyAsync(lst.data(), e->nbl + h.nbl0, lst.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    for (int sl = 0; sl < h.n; ++sl) {
+      unsigned i = ids[sl];
+      unsigned c = std::min<unsigned>(nn[sl], (unsigned)max_nbrs);
+      counts[i] = nn[sl];
+      for (unsigned k = 0; k < c; ++k) nbl[(size_t)i * max_nbrs + k] = ids[lst[(size_t)k * h.np + sl]];
+    }
+  });
+}
+
+int b2md_sort_export(b2md_engine* e, int id, unsigned* unsorted_index) {
+  if (!unsorted_index) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    CK(cudaMemcpyAsync(unsorted_index, e->uidx[s.abuf] + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                       e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+  });
+}
+
+int b2md_cell_grid(b2md_engine* e, int id, int* nc3) {
+  if (!nc3) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    for (int k = 0; k < 3; ++k) nc3[k] = h.d.nc[k];
+    if (h.d.nb_method != NB_CELLS) nc3[0] = nc3[1] = nc3[2] = 0;
+  });
+}
+
+int b2md_sync(b2md_engine* e) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+  });
+}
+
+void* b2md_stream(b2md_engine* e) { return e ? (void*)e->stream : nullptr; }
+
+}  // extern "C"

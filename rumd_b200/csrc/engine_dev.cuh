@@ -1,0 +1,105 @@
+// Device-side data layout and kernels of the B200 RUMD engine.
+//
+// Layout in HBM (one engine = many replicas; a plain Sample is one replica):
+//   particle pools, indexed p0 + local slot (slot = position in cell-sorted order)
+//     r[2]    float4  x, y, z, type bits   (ping-pong: step k reads r[rbuf], writes r[rbuf^1])
+//     v[2]    float4  vx, vy, vz, 1/m      (ping-pong with abuf: swapped only by the sort)
+//     im[2]   int4    images               (abuf)
+//     uidx[2] uint    original particle id (abuf)  == d_unsorted_index (ParticleData.h:56)
+//     f, w, sts float4 as RUMD (ParticleData.h:41-46); last_r float4; nn uint
+//   list pool: nbl[nbl0 + k*stride + slot]  (column-major per replica, like RUMD's
+//     nbl[k*nvp + i], NeighborList.cu:1293, so a warp's k-th entries are one sector run)
+//   cell pools: cnt[cell0 + c], start[cell0 + c] (chunk-local exclusive prefix)
+//   per-tile / per-group FP64 partial sums for deterministic two-level reductions.
+//
+// A "tile" is pb consecutive slots of one replica; one CUDA block processes one
+// tile (pb particles x tp threads per particle).  Tiles never straddle replicas,
+// so a replica's arithmetic is the same alone and in any batch.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace b2md {
+
+constexpr int kMaxTypes = 8;
+constexpr int kParStride = 8;   // packed floats per type pair
+constexpr int kNumParam = 12;   // RUMD NumParam (rumd_base.h)
+constexpr int kNPart = 8;       // FP64 partial sums per tile
+constexpr int kGroup = 32;      // tiles per reduction group
+constexpr int kMaxBlock = 512;  // pb*tp limit (launch bounds)
+
+enum { P_PE = 0, P_W, P_KE2, P_KET, P_PX, P_PY, P_PZ, P_M };
+enum { CUT_NS = 0, CUT_SP = 1, CUT_SF = 2 };
+enum { NB_CELLS = 0, NB_N2 = 1 };
+
+// Packed pair row: rc^2, A12, A6, p10 = s(rc)*rc, p11 = u(rc), rc, (rc+skin)^2, 0
+struct RepDev {
+  int n, p0, tile0, ntiles;
+  int group0, ngroups;
+  int ntypes, par0;
+  int cell0, ncell;
+  int nc[3];
+  int nb_method;
+  int max_nbrs, nbl_stride;
+  long long nbl0;
+  float L[3], invL[3];
+  float skin2_4;
+  float dt, omega2;
+  int cutoff;
+  unsigned thermo_mask;
+  int reset_interval;
+  int energy_interval, energy_cap;
+  long long elog0;
+  double dof;
+  int active;
+  int pad_;
+};
+
+struct RepState {
+  double xi, T, dT;
+  double ke2, ke_t, pe, vir;
+  double P[3], M;
+  long long steps;       // total integrated steps
+  long long steps_left;  // queued steps
+  long long run_step;    // step index inside the current run (momentum-reset schedule)
+  int rbuf, abuf;
+  int rebuild, exceed;
+  int overflow, nrebuilds;
+  int actual_max_nbrs, nlog;
+};
+
+struct EngArgs {
+  float4* r[2];
+  float4* v[2];
+  int4* im[2];
+  unsigned* uidx[2];
+  float4* f;
+  float4* w;
+  float4* sts;
+  float4* last_r;
+  unsigned* nn;
+  unsigned* nbl;
+  int* key;
+  int* slot;
+  unsigned* order;
+  int* cnt;
+  int* cstart;
+  int* ctot;    // per tile: cell-chunk total (scan)
+  int* cpref;   // per tile: exclusive prefix of chunk totals within the replica
+  const float* par;
+  const RepDev* rep;
+  RepState* st;
+  const int* tile_rep;
+  const int* tile_first;
+  double* tpart;
+  double* gpart;
+  unsigned* gctr;
+  unsigned* rctr;
+  unsigned* fctr;
+  int* any_rebuild;
+  double* elog;
+  int ntiles;
+  int nrep;
+};
+
+}  // namespace b2md

@@ -1,0 +1,698 @@
+// Kernels of the B200 RUMD engine (sm_100a).  See engine_dev.cuh for layout.
+//
+// Arithmetic contract
+//   * Neighbour-list decisions (cell keys, d^2 < (rc+skin)^2, displacement
+//     trigger) use the exact FP32 operation sequence of the reference source
+//     (SimulationBox.h:111-125, NeighborList.cu:1106-1140, 1282-1285) with the
+//     multiply-add contractions that nvcc applies to it written out as
+//     __fmaf_rn, so list sets and the sort permutation are bit-exact.
+//   * Pair forces are FP32 (PairPotential.h:161-168, 1198-1244); 1/d^2 is a
+//     correctly rounded reciprocal, the shifted-force 1/r term uses rsqrtf.
+//   * Reductions (pe, virial, kinetic energy, momentum) are FP64 with a fixed
+//     summation tree, so results do not depend on scheduling or on which other
+//     replicas share the launch; the thermostat state is FP64.
+#pragma once
+#include "engine_dev.cuh"
+#include "pbc_math.cuh"
+
+namespace b2md {
+
+__device__ __forceinline__ double warp_sum_d(double x) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// Block sum of kNPart doubles per thread -> s_out[kNPart] (valid after return,
+// fixed tree: warp butterfly then warps in index order).
+__device__ __forceinline__ void block_sum8(double (&v)[kNPart], double* s_warp, double* s_out) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int k = 0; k < kNPart; ++k) {
+    double x = warp_sum_d(v[k]);
+    if (lane == 0) s_warp[wid * kNPart + k] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNPart) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += s_warp[w * kNPart + threadIdx.x];
+    s_out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// Ordered strided sum of count rows of kNPart doubles (deterministic).
+__device__ __forceinline__ void block_rows_sum(const double* base, int count, double* s_scr, double* s_out) {
+  const int nslot = blockDim.x / kNPart;
+  const int k = threadIdx.x % kNPart, slot = threadIdx.x / kNPart;
+  double acc = 0.0;
+  if (slot < nslot)
+    for (int t = slot; t < count; t += nslot) acc += __ldcg(base + (size_t)t * kNPart + k);
+  s_scr[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x < kNPart) {
+    double s = 0.0;
+    for (int q = 0; q < nslot; ++q) s += s_scr[q * kNPart + threadIdx.x];
+    s_out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// Two-level deterministic replica reduction.  Every block of the replica
+// calls it with its block totals in s_blk; returns true in exactly one block
+// (the last to finish) with the replica totals in s_tot.
+__device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int lt,
+                               const double* s_blk, double* s_scr, double* s_tot) {
+  __shared__ int s_last;
+  const int g = lt / kGroup;
+  const int gfirst = g * kGroup;
+  const int gsize = min(kGroup, R.ntiles - gfirst);
+  if (threadIdx.x < kNPart) {
+    a.tpart[(size_t)(R.tile0 + lt) * kNPart + threadIdx.x] = s_blk[threadIdx.x];
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned c = atomicAdd(&a.gctr[R.group0 + g], 1u);
+    s_last = (c == (unsigned)(gsize - 1));
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  block_rows_sum(a.tpart + (size_t)(R.tile0 + gfirst) * kNPart, gsize, s_scr, s_tot);
+  if (threadIdx.x < kNPart) {
+    a.gpart[(size_t)(R.group0 + g) * kNPart + threadIdx.x] = s_tot[threadIdx.x];
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a.gctr[R.group0 + g] = 0u;
+    unsigned c = atomicAdd(&a.rctr[rep], 1u);
+    s_last = (c == (unsigned)(R.ngroups - 1));
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  __threadfence();
+  block_rows_sum(a.gpart + (size_t)R.group0 * kNPart, R.ngroups, s_scr, s_tot);
+  if (threadIdx.x == 0) a.rctr[rep] = 0u;
+  return true;
+}
+
+// Last block of the whole grid: publishes "any replica needs a rebuild" to
+// the next conditional graph node (or nothing when launched eagerly).
+__device__ __forceinline__ void grid_final(const EngArgs& a, int has_cond, cudaGraphConditionalHandle h) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned c = atomicAdd(a.fctr, 1u);
+    if (c == gridDim.x - 1) {
+      __threadfence();
+      int any = atomicExch(a.any_rebuild, 0);
+      *a.fctr = 0u;
+      if (has_cond) cudaGraphSetConditional(h, any ? 1u : 0u);
+    }
+  }
+}
+
+// Nose-Hoover leap-frog for one particle (integrateNVTAlgorithm,
+// IntegratorNVT.cu:364-418); accumulates FP64 kinetic sums.
+__device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float3 vshift, bool do_reset,
+                                              float4 r, float4 f, float4& v, int4& im, float4& rn,
+                                              double (&acc)[kNPart], bool& exceed, float4 lr) {
+  const int ti = __float_as_int(r.w);
+  const bool thermo = (R.thermo_mask >> ti) & 1u;
+  if (do_reset) { v.x -= vshift.x; v.y -= vshift.y; v.z -= vshift.z; }
+  const float xs = thermo ? xi_f : 0.f;
+  const float factor = 0.5f * xs * R.dt;
+  const float plus = 1.f / (1.f + factor);
+  const float minus = 1.f - factor;
+  const float dt = R.dt;
+  const double vb = (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
+  float vx = plus * __fmaf_rn(minus, v.x, __fmul_rn(__fmul_rn(v.w, f.x), dt));
+  float vy = plus * __fmaf_rn(minus, v.y, __fmul_rn(__fmul_rn(v.w, f.y), dt));
+  float vz = plus * __fmaf_rn(minus, v.z, __fmul_rn(__fmul_rn(v.w, f.z), dt));
+  float x = __fmaf_rn(vx, dt, r.x), y = __fmaf_rn(vy, dt, r.y), z = __fmaf_rn(vz, dt, r.z);
+  float kx = rintf(__fmul_rn(x, R.invL[0])), ky = rintf(__fmul_rn(y, R.invL[1])), kz = rintf(__fmul_rn(z, R.invL[2]));
+  x = __fmaf_rn(-R.L[0], kx, x); y = __fmaf_rn(-R.L[1], ky, y); z = __fmaf_rn(-R.L[2], kz, z);
+  im.x += (int)kx; im.y += (int)ky; im.z += (int)kz;
+  v.x = vx; v.y = vy; v.z = vz;
+  rn = make_float4(x, y, z, r.w);
+  const double m = 1.0 / (double)v.w;
+  const double vf = (double)vx * vx + (double)vy * vy + (double)vz * vz;
+  acc[P_KET] += 0.25 * m * (vb + vf);
+  if (thermo) acc[P_KE2] += m * vf;
+  acc[P_PX] += m * vx; acc[P_PY] += m * vy; acc[P_PZ] += m * vz;
+  acc[P_M] += m;
+  // displacement since the last build (displacement_since_nb_build, NeighborList.cu:970-997)
+  float d2 = dist2_ref(mi_comp(x - lr.x, R.L[0], R.invL[0]), mi_comp(y - lr.y, R.L[1], R.invL[1]),
+                       mi_comp(z - lr.z, R.L[2], R.invL[2]));
+  exceed = d2 > R.skin2_4;
+}
+
+// Replica bookkeeping after an integration step (last block only).
+__device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState* S, const double* tot,
+                            bool with_forces) {
+  if (threadIdx.x != 0) return;
+  if (R.thermo_mask) {
+    double dev = tot[P_KE2] / (R.dof * S->T) - 1.0;
+    if (dev > 10.0) dev = 10.0;  // updateNVTThermostatState (IntegratorNVT.cu:426-437)
+    S->xi += (double)R.dt * (double)R.omega2 * dev;
+    S->T += S->dT;
+  }
+  S->ke2 = tot[P_KE2];
+  S->ke_t = tot[P_KET];
+  if (with_forces) { S->pe = tot[P_PE]; S->vir = tot[P_W] / 6.0; }
+  S->P[0] = tot[P_PX]; S->P[1] = tot[P_PY]; S->P[2] = tot[P_PZ]; S->M = tot[P_M];
+  S->rbuf ^= 1;
+  S->steps += 1;
+  S->run_step += 1;
+  if (S->steps_left > 0) S->steps_left -= 1;
+  int ex = atomicExch(&S->exceed, 0);
+  S->rebuild = ex > 0;
+  if (ex > 0) atomicAdd(a.any_rebuild, 1);
+  if (R.energy_interval > 0 && (S->steps % R.energy_interval) == 0 && R.energy_cap > 0) {
+    int k = S->nlog % R.energy_cap;
+    double* e = a.elog + (size_t)(R.elog0 + k) * 5;
+    e[0] = (double)S->steps; e[1] = S->pe; e[2] = S->vir; e[3] = S->ke_t; e[4] = S->xi;
+    S->nlog += 1;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pair force (+ fused integration).  FUSED = one MD step: forces from r[rbuf],
+// integrate, write r[rbuf^1].  Otherwise Sample::CalcF only.
+// ---------------------------------------------------------------------------
+template <int TP, bool FUSED, bool STRESS>
+__global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cudaGraphConditionalHandle h) {
+  extern __shared__ float s_par[];
+  __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
+  __shared__ double s_scr[kMaxBlock];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  const int tile = blockIdx.x;
+  const int rep = a.tile_rep[tile];
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  const bool skip = (S->overflow != 0) || (FUSED && S->steps_left <= 0) || !R.active;
+  if (!skip) {
+    const int nt = R.ntypes;
+    for (int k = threadIdx.x; k < nt * nt * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
+    __syncthreads();
+    const int lp = threadIdx.x / TP, lane_t = threadIdx.x % TP;
+    const int i = a.tile_first[tile] + lp;
+    const bool valid = i < R.n;
+    const int rb = S->rbuf;
+    const float4* __restrict__ rc = a.r[rb] + R.p0;
+    const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
+    const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+    const int cutoff = R.cutoff;
+    float4 ri = valid ? rc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int ti = valid ? __float_as_int(ri.w) : 0;
+    const float* prow = s_par + ti * nt * kParStride;
+    float fx = 0.f, fy = 0.f, fz = 0.f, uu = 0.f, ww = 0.f;
+    float sxx = 0.f, syy = 0.f, szz = 0.f, syz = 0.f, sxz = 0.f, sxy = 0.f;
+    const unsigned nn = valid ? a.nn[R.p0 + i] : 0u;
+    const unsigned* __restrict__ col = a.nbl + R.nbl0 + i;
+    const size_t stride = (size_t)R.nbl_stride;
+#pragma unroll 4
+    for (unsigned k = lane_t; k < nn; k += TP) {
+      const unsigned j = __ldg(col + k * stride);
+      const float4 rj = __ldg(rc + j);
+      const float dx = mi_comp(ri.x - rj.x, Lx, iLx);
+      const float dy = mi_comp(ri.y - rj.y, Ly, iLy);
+      const float dz = mi_comp(ri.z - rj.z, Lz, iLz);
+      const float d2 = dist2_ref(dx, dy, dz);
+      const float* pp = prow + __float_as_int(rj.w) * kParStride;
+      const float4 q = *reinterpret_cast<const float4*>(pp);
+      if (d2 < q.x) {
+        const float i2 = __frcp_rn(d2);
+        const float i6 = i2 * i2 * i2;
+        const float t = q.y * i6;
+        float s = i6 * i2 * __fmaf_rn(12.f, t, 6.f * q.z);
+        float u = i6 * (t + q.z);
+        if (cutoff == CUT_SF) {
+          const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);
+          const float ir = rsqrtf(d2);
+          s = __fmaf_rn(-q.w, ir, s);
+          u += __fmaf_rn(q.w, __fmaf_rn(d2, ir, -q2.y), -q2.x);
+        } else if (cutoff == CUT_SP) {
+          u -= pp[4];
+        }
+        fx = __fmaf_rn(dx, s, fx);
+        fy = __fmaf_rn(dy, s, fy);
+        fz = __fmaf_rn(dz, s, fz);
+        ww = __fmaf_rn(d2, s, ww);
+        uu += u;
+        if (STRESS) {
+          sxx -= dx * dx * s; syy -= dy * dy * s; szz -= dz * dz * s;
+          syz -= dy * dz * s; sxz -= dx * dz * s; sxy -= dx * dy * s;
+        }
+      }
+    }
+    if (TP > 1) {
+#pragma unroll
+      for (int o = TP / 2; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+        uu += __shfl_xor_sync(0xffffffffu, uu, o);
+        ww += __shfl_xor_sync(0xffffffffu, ww, o);
+        if (STRESS) {
+          sxx += __shfl_xor_sync(0xffffffffu, sxx, o);
+          syy += __shfl_xor_sync(0xffffffffu, syy, o);
+          szz += __shfl_xor_sync(0xffffffffu, szz, o);
+          syz += __shfl_xor_sync(0xffffffffu, syz, o);
+          sxz += __shfl_xor_sync(0xffffffffu, sxz, o);
+          sxy += __shfl_xor_sync(0xffffffffu, sxy, o);
+        }
+      }
+    }
+    double acc[kNPart];
+#pragma unroll
+    for (int k = 0; k < kNPart; ++k) acc[k] = 0.0;
+    bool exceed = false;
+    if (valid && lane_t == 0) {
+      const float4 fo = make_float4(fx, fy, fz, 0.5f * uu);
+      const size_t gi = (size_t)R.p0 + i;
+      a.f[gi] = fo;
+      a.w[gi] = make_float4(0.f, sxz, sxy, ww);
+      if (STRESS) a.sts[gi] = make_float4(sxx, syy, szz, syz);
+      acc[P_PE] = (double)fo.w;
+      acc[P_W] = (double)ww;
+      if (FUSED) {
+        const int ab = S->abuf;
+        float4 v = a.v[ab][gi];
+        int4 im = a.im[ab][gi];
+        const bool do_reset = R.reset_interval > 0 && (S->run_step % R.reset_interval) == 0;
+        float3 vs = make_float3(0.f, 0.f, 0.f);
+        if (do_reset && S->M > 0.0)
+          vs = make_float3((float)(S->P[0] / S->M), (float)(S->P[1] / S->M), (float)(S->P[2] / S->M));
+        float4 rn;
+        integrate_one(R, (float)S->xi, vs, do_reset, ri, fo, v, im, rn, acc, exceed, a.last_r[gi]);
+        a.v[ab][gi] = v;
+        a.im[ab][gi] = im;
+        a.r[rb ^ 1][gi] = rn;
+      }
+    }
+    if (FUSED) {
+      const int ex = __syncthreads_or(exceed);
+      if (ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
+    }
+    block_sum8(acc, s_warp, s_blk);
+    if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
+      if (FUSED) {
+        finish_step(a, rep, R, S, s_tot, true);
+      } else if (threadIdx.x == 0) {
+        S->pe = s_tot[P_PE];
+        S->vir = s_tot[P_W] / 6.0;
+      }
+    }
+  }
+  grid_final(a, has_cond, h);
+}
+
+// IntegratorNVT::Integrate alone (forces already in f).  One thread per particle.
+__global__ void __launch_bounds__(kMaxBlock) k_integrate(EngArgs a) {
+  __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
+  __shared__ double s_scr[kMaxBlock];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  const int tile = blockIdx.x;
+  const int rep = a.tile_rep[tile];
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  if (S->overflow || !R.active) return;
+  const int i = a.tile_first[tile] + threadIdx.x;
+  double acc[kNPart];
+#pragma unroll
+  for (int k = 0; k < kNPart; ++k) acc[k] = 0.0;
+  bool exceed = false;
+  const int rb = S->rbuf, ab = S->abuf;
+  if (i < R.n) {
+    const size_t gi = (size_t)R.p0 + i;
+    float4 r = a.r[rb][gi], f = a.f[gi], v = a.v[ab][gi];
+    int4 im = a.im[ab][gi];
+    float4 rn;
+    integrate_one(R, (float)S->xi, make_float3(0.f, 0.f, 0.f), false, r, f, v, im, rn, acc, exceed, a.last_r[gi]);
+    acc[P_PE] = 0.0; acc[P_W] = 0.0;
+    a.v[ab][gi] = v; a.im[ab][gi] = im; a.r[rb ^ 1][gi] = rn;
+  }
+  const int ex = __syncthreads_or(exceed);
+  if (ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
+  block_sum8(acc, s_warp, s_blk);
+  if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
+    if (threadIdx.x == 0) {
+      double pe = S->pe, vir = S->vir;
+      finish_step(a, rep, R, S, s_tot, false);
+      S->pe = pe; S->vir = vir;
+    }
+  }
+}
+
+// Total momentum and mass of the current velocities (calculateMomentum +
+// sumIdenticalArrays, IntegratorNVT.cu:176-183, 462-471), FP64.
+__global__ void __launch_bounds__(kMaxBlock) k_momentum(EngArgs a) {
+  __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
+  __shared__ double s_scr[kMaxBlock];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  const int tile = blockIdx.x;
+  const int rep = a.tile_rep[tile];
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  if (!R.active) return;
+  const int i = a.tile_first[tile] + threadIdx.x;
+  double acc[kNPart];
+#pragma unroll
+  for (int k = 0; k < kNPart; ++k) acc[k] = 0.0;
+  if (i < R.n) {
+    const float4 v = a.v[S->abuf][(size_t)R.p0 + i];
+    const double m = 1.0 / (double)v.w;
+    acc[P_PX] = m * v.x; acc[P_PY] = m * v.y; acc[P_PZ] = m * v.z; acc[P_M] = m;
+  }
+  block_sum8(acc, s_warp, s_blk);
+  if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
+    if (threadIdx.x == 0) {
+      S->P[0] = s_tot[P_PX]; S->P[1] = s_tot[P_PY]; S->P[2] = s_tot[P_PZ]; S->M = s_tot[P_M];
+    }
+  }
+}
+
+// zeroTotalMomentum (IntegratorNVT.cu:444-458) with the FP64 momentum.
+__global__ void k_apply_zero_momentum(EngArgs a) {
+  const int tile = blockIdx.x;
+  const int rep = a.tile_rep[tile];
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  if (!R.active || S->M <= 0.0) return;
+  const int i = a.tile_first[tile] + threadIdx.x;
+  if (i >= R.n) return;
+  const size_t gi = (size_t)R.p0 + i;
+  float4 v = a.v[S->abuf][gi];
+  v.x -= (float)(S->P[0] / S->M); v.y -= (float)(S->P[1] / S->M); v.z -= (float)(S->P[2] / S->M);
+  a.v[S->abuf][gi] = v;
+}
+
+// Sets the queued step counts of all replicas (lock-step run start).
+__global__ void k_set_steps(EngArgs a, long long nsteps, int reset_run_step) {
+  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rep >= a.nrep) return;
+  if (!a.rep[rep].active) return;
+  a.st[rep].steps_left = nsteps;
+  if (reset_run_step) a.st[rep].run_step = 0;
+}
+
+// Gate: publishes "any replica flagged for rebuild" to the first conditional node.
+__global__ void k_gate(EngArgs a, cudaGraphConditionalHandle h) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < a.nrep; r += blockDim.x)
+    if (a.rep[r].active && a.st[r].rebuild && !a.st[r].overflow) s_any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, s_any ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------
+// Neighbour-list rebuild (NeighborList::CalculateNBL_Sorting, NeighborList.cu:717-781).
+// Grid = tiles, block = pb (one thread per slot).  Every kernel returns at once
+// for replicas that are not flagged, so the same sequence serves batches.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool rb_active(const EngArgs& a, int rep) {
+  const RepState* S = a.st + rep;
+  return a.rep[rep].active && S->rebuild && !S->overflow;
+}
+
+__device__ __forceinline__ int cell_chunk(const RepDev& R) { return (R.ncell + R.ntiles - 1) / R.ntiles; }
+
+// (1) zero cell counts of this tile's chunk of the replica's cells
+__global__ void k_rb_clear(EngArgs a) {
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  const int ch = cell_chunk(R), lt = tile - R.tile0;
+  const int c0 = lt * ch, c1 = min(R.ncell, c0 + ch);
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) a.cnt[R.cell0 + c] = 0;
+}
+
+// (2) cell key per particle (calculateCellIndices, NeighborList.cu:1142-1172) and
+//     its arrival rank in the cell
+__global__ void k_rb_count(EngArgs a) {
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  const int i = a.tile_first[tile] + threadIdx.x;
+  if (i >= R.n) return;
+  const size_t gi = (size_t)R.p0 + i;
+  const float4 r = a.r[a.st[rep].rbuf][gi];
+  const int cx = cell_coord(r.x, R.invL[0], R.nc[0]);
+  const int cy = cell_coord(r.y, R.invL[1], R.nc[1]);
+  const int cz = cell_coord(r.z, R.invL[2], R.nc[2]);
+  const int key = cx + cy * R.nc[0] + cz * R.nc[0] * R.nc[1];
+  a.key[gi] = key;
+  a.slot[gi] = atomicAdd(&a.cnt[R.cell0 + key], 1);
+}
+
+// (3a) chunk-local exclusive prefix of cell counts; chunk total per tile
+__global__ void k_rb_scan_local(EngArgs a) {
+  __shared__ int s_w[kMaxBlock / 32];
+  __shared__ int s_carry;
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  const int ch = cell_chunk(R), lt = tile - R.tile0;
+  const int c0 = lt * ch, c1 = min(R.ncell, c0 + ch);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = c0; base < c1; base += blockDim.x) {
+    const int c = base + threadIdx.x;
+    const int x = c < c1 ? a.cnt[R.cell0 + c] : 0;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    int woff = 0;
+    for (int w = 0; w < wid; ++w) woff += s_w[w];
+    const int carry = s_carry;
+    if (c < c1) a.cstart[R.cell0 + c] = carry + woff + incl - x;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) {
+      int tot = 0;
+      for (int w = 0; w < nw; ++w) tot += s_w[w];
+      s_carry = carry + tot;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) a.ctot[tile] = s_carry;
+}
+
+// (3b) exclusive prefix of chunk totals over the replica's tiles (block per replica)
+__global__ void k_rb_scan_tiles(EngArgs a) {
+  __shared__ int s_w[32];
+  __shared__ int s_carry;
+  const int rep = blockIdx.x;
+  if (rep >= a.nrep || !rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  for (int base = 0; base < R.ntiles; base += blockDim.x) {
+    const int t = base + threadIdx.x;
+    const int x = t < R.ntiles ? a.ctot[R.tile0 + t] : 0;
+    int incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) s_w[wid] = incl;
+    __syncthreads();
+    int woff = 0;
+    for (int w = 0; w < wid; ++w) woff += s_w[w];
+    const int carry = s_carry;
+    if (t < R.ntiles) a.cpref[R.tile0 + t] = carry + woff + incl - x;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) {
+      int tot = 0;
+      for (int w = 0; w < nw; ++w) tot += s_w[w];
+      s_carry = carry + tot;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ int cell_begin(const EngArgs& a, const RepDev& R, int c, int ch) {
+  return a.cstart[R.cell0 + c] + a.cpref[R.tile0 + c / ch];
+}
+
+// (4) scatter particle ids to their cell buckets (arrival order)
+__global__ void k_rb_scatter(EngArgs a) {
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  const int i = a.tile_first[tile] + threadIdx.x;
+  if (i >= R.n) return;
+  const size_t gi = (size_t)R.p0 + i;
+  const int key = a.key[gi];
+  const int pos = cell_begin(a, R, key, cell_chunk(R)) + a.slot[gi];
+  a.order[(size_t)R.p0 + pos] = (unsigned)i;
+}
+
+// (5) order each bucket by old index: the result equals a stable sort by key
+//     (thrust::sort_by_key on (cellIndex, iota), Sample.h:174-188)
+__global__ void k_rb_fix(EngArgs a) {
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  const int ch = cell_chunk(R), lt = tile - R.tile0;
+  const int c0 = lt * ch, c1 = min(R.ncell, c0 + ch);
+  for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    const int b = cell_begin(a, R, c, ch), m = a.cnt[R.cell0 + c];
+    unsigned* o = a.order + (size_t)R.p0 + b;
+    for (int p = 1; p < m; ++p) {
+      unsigned x = o[p];
+      int q = p - 1;
+      while (q >= 0 && o[q] > x) { o[q + 1] = o[q]; --q; }
+      o[q + 1] = x;
+    }
+  }
+}
+
+// (6) gather r, v, images, unsorted index into the sorted order
+//     (ParticleData::UpdateAfterSorting, ParticleData.cu:493-528); the last
+//     block of the replica flips the buffer parities
+__global__ void k_rb_permute(EngArgs a) {
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) return;
+  RepState* S = a.st + rep;
+  const int s = a.tile_first[tile] + threadIdx.x;
+  const int rb = S->rbuf, ab = S->abuf;
+  if (s < R.n) {
+    const size_t gs = (size_t)R.p0 + s;
+    const size_t go = (size_t)R.p0 + a.order[gs];
+    a.r[rb ^ 1][gs] = a.r[rb][go];
+    a.v[ab ^ 1][gs] = a.v[ab][go];
+    a.im[ab ^ 1][gs] = a.im[ab][go];
+    a.uidx[ab ^ 1][gs] = a.uidx[ab][go];
+  }
+  __shared__ int s_last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    unsigned c = atomicAdd(&a.rctr[rep], 1u);
+    s_last = (c == (unsigned)(R.ntiles - 1));
+    if (s_last) {
+      a.rctr[rep] = 0u;
+      S->rbuf = rb ^ 1;
+      S->abuf = ab ^ 1;
+    }
+  }
+}
+
+// (7) sorted 5x5x5 cell scan (calculateNBL_CellsSorted, NeighborList.cu:1204-1319):
+//     neighbours in the reference's order (dz, dy, dx, ascending slot)
+__global__ void k_rb_build(EngArgs a) {
+  extern __shared__ float s_cs2[];
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  const int nt = R.ntypes;
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
+  __syncthreads();
+  const int i = a.tile_first[tile] + threadIdx.x;
+  const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
+  int count = 0;
+  if (i < R.n) {
+    const float4 ri = rc[i];
+    const int ti = __float_as_int(ri.w);
+    const float* cs2 = s_cs2 + ti * nt;
+    unsigned* col = a.nbl + R.nbl0 + i;
+    const size_t stride = (size_t)R.nbl_stride;
+    const int maxn = R.max_nbrs;
+    const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
+    const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+    if (R.nb_method == NB_CELLS) {
+      const int ch = cell_chunk(R);
+      const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
+      const int cx = cell_coord(ri.x, iLx, nx), cy = cell_coord(ri.y, iLy, ny), cz = cell_coord(ri.z, iLz, nz);
+      for (int dz = -2; dz <= 2; ++dz) {
+        const int oz = (cz + dz + nz) % nz;
+        for (int dy = -2; dy <= 2; ++dy) {
+          int oy = cy + dy;
+          oy += ((oy < 0) - (oy >= ny)) * ny;
+          for (int dx = -2; dx <= 2; ++dx) {
+            int ox = cx + dx;
+            ox += ((ox < 0) - (ox >= nx)) * nx;
+            const int c = ox + oy * nx + oz * nx * ny;
+            const int b = cell_begin(a, R, c, ch), m = a.cnt[R.cell0 + c];
+            for (int j = b; j < b + m; ++j) {
+              if (j == i) continue;
+              const float4 rj = __ldg(rc + j);
+              const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
+                                         mi_comp(ri.z - rj.z, Lz, iLz));
+              if (d2 < cs2[__float_as_int(rj.w)]) {
+                if (count < maxn) col[(size_t)count * stride] = (unsigned)j;
+                ++count;
+              }
+            }
+          }
+        }
+      }
+    } else {
+      // all pairs (calculateNBL_N2 criterion), ascending j
+      for (int j = 0; j < R.n; ++j) {
+        if (j == i) continue;
+        const float4 rj = __ldg(rc + j);
+        const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
+                                   mi_comp(ri.z - rj.z, Lz, iLz));
+        if (d2 < cs2[__float_as_int(rj.w)]) {
+          if (count < maxn) col[(size_t)count * stride] = (unsigned)j;
+          ++count;
+        }
+      }
+    }
+    a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
+    a.last_r[(size_t)R.p0 + i] = ri;
+  }
+  // block max of count, overflow if any count > capacity
+  int bmax = count;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
+  __shared__ int s_max;
+  if (threadIdx.x == 0) s_max = 0;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) atomicMax(&s_max, bmax);
+  __syncthreads();
+  __shared__ int s_last;
+  if (threadIdx.x == 0) {
+    atomicMax(&S->actual_max_nbrs, s_max);
+    if (s_max > R.max_nbrs) atomicExch(&S->overflow, 1);
+    __threadfence();
+    unsigned c = atomicAdd(&a.rctr[rep], 1u);
+    s_last = (c == (unsigned)(R.ntiles - 1));
+    if (s_last) {
+      a.rctr[rep] = 0u;
+      S->rebuild = 0;
+      S->nrebuilds += 1;
+    }
+  }
+}
+
+// Resets the per-build maximum before a rebuild sequence.
+__global__ void k_rb_begin(EngArgs a) {
+  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
+  if (rep >= a.nrep) return;
+  if (a.rep[rep].active && a.st[rep].rebuild && !a.st[rep].overflow) a.st[rep].actual_max_nbrs = 0;
+}
+
+}  // namespace b2md

@@ -1,0 +1,31 @@
+// Box and cell arithmetic shared by the kernels and the parity probes.
+//
+// These are the reference's FP32 expressions (SimulationBox.h:111-125,
+// NeighborList.cu:1106-1140) with the multiply-add contractions that nvcc
+// applies to them written out explicitly, so that every neighbour-list and
+// sort decision rounds exactly as the reference's device build does.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace b2md {
+
+__device__ __forceinline__ float mi_comp(float d, float L, float invL) {
+  // dr -= L * rintf(dr * invL)   (SimulationBox.h:117-122)
+  return __fmaf_rn(-L, rintf(__fmul_rn(d, invL)), d);
+}
+
+__device__ __forceinline__ float dist2_ref(float dx, float dy, float dz) {
+  // dx*dx + dy*dy + dz*dz as contracted by nvcc (SimulationBox.h:124)
+  return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+}
+
+__device__ __forceinline__ int cell_coord(float x, float invL, int nc) {
+  // calculateCellCoordinates (NeighborList.cu:1106-1133)
+  float scaled = __fmaf_rn(x, invL, 0.5f);
+  int c = __float2int_rz(__fmul_rn((float)nc, scaled));
+  if (c == nc) c -= 1;
+  else if (c < 0) c = 0;
+  return c;
+}
+
+}  // namespace b2md
