@@ -1,0 +1,408 @@
+#!/usr/bin/env python
+"""Benchmark: RUMD's LJ/NVT time step on B200 (particle-steps/s).
+
+Headline workload (one JSON line on rank 0): plain method, single large
+system -- Kob-Andersen 80:20 LJ, N=65536, density 1.2, T=0.45, Nose-Hoover
+NVT (tau=0.2), dt=0.005, skin 0.3, shifted-force cut-off 2.5 sigma_ij, FP32
+forces with FP64 reductions.  A "step" is one MD time step (momentum reset,
+neighbour-list check/rebuild, forces, integration).  The line also carries the
+batched form (256 mixed-size KA replicas in one launch sequence) against
+sequential plain runs of a sample of the same replicas.
+
+  python bench.py [--gpus N --steps K --warmup W]        # this implementation
+  python bench.py --impl reference ...                   # reference CPU path
+
+--gpus N > 1 runs under torchrun: every rank advances its own independent
+replica of the workload (the path has no data exchange); value is the sum.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PLAIN = 65536
+KA_DENSITY = 1.2
+T_PLAIN = 0.45
+DT = 0.005
+SKIN = 0.3
+TAU = 0.2
+METRIC = "particle-steps/s at 1 B200 (plain vs batched/served); p50/p99 job latency"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20000)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--pb", type=int, default=64)
+    p.add_argument("--tp", type=int, default=4)
+    p.add_argument("--batch-steps", type=int, default=2000)
+    p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile-launches", action="store_true",
+                   help="small plain run only (for the ncu launch list)")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class Dist:
+    """Barrier and max-over-ranks for timings (NCCL when launched by torchrun)."""
+
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+            self.dist = dist
+            self.torch = torch
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x):
+        if self.world == 1:
+            return x
+        t = self.torch.tensor([float(x)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.world > 1:
+            self.dist.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the fused step kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            return json.load(fh)
+    return None
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+
+def ka_params():
+    from rumd_b200 import initconf as I
+    return I.lj_params(2, I.KA)
+
+
+def prepare_plain(capi, device, pb, tp, seed):
+    """KA N=65536 melted at T=2 then brought to T=0.45 (untimed preparation)."""
+    from rumd_b200 import initconf as I
+    c = I.ka_config(N_PLAIN, density=KA_DENSITY, T=2.0, seed=seed)
+    params = ka_params()
+    e = capi.Engine(device=device, pb=pb, tp=tp)
+    rid = e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=2.0, tau=TAU, vel4=c["vel4"])
+    e.run(1000)
+    e.set_integrator(rid, DT, T_PLAIN, TAU)
+    e.run(2000)
+    return e, rid, c["box"], params
+
+
+def flush_l2(device):
+    import torch
+    buf = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{device}")
+    buf.fill_(1)
+    torch.cuda.synchronize(device)
+    del buf
+
+
+def time_run(capi, e, steps, device):
+    """Device time of Run(steps) with CUDA events on the engine's stream."""
+    import torch
+    stream = torch.cuda.ExternalStream(e.stream(), device=f"cuda:{device}")
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(device)
+    t0.record(stream)
+    e.run(steps)
+    t1.record(stream)
+    torch.cuda.synchronize(device)
+    return t0.elapsed_time(t1) / 1e3
+
+
+def launches_in_run(steps, rebuilds):
+    # per step: fused kernel; per graph launch: gate; per rebuild: 9 kernels;
+    # run start: steps + momentum; run end: rebuild sequence + force kernel
+    graph_launches = steps // 32 + steps % 32
+    return int(steps + graph_launches + 9 * rebuilds + 2 + 10)
+
+
+def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
+    """The oracle's FP32 step (cell list + full list + forces + NVT) on all host cores."""
+    from oracle import oracle as O
+    n = N_PLAIN
+    pos4 = e.get(rid, "pos", n)
+    vel4 = e.get(rid, "vel", n)
+    im3 = e.get(rid, "images", n)
+    kw = dict(L=box, ntypes=2, params=params, cutoff=O.SF, skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU)
+    t = time.perf_counter()
+    O.md_run(pos4, vel4, im3, nsteps=2, **kw)
+    one = max((time.perf_counter() - t) / 2, 1e-4)
+    steps = int(max(4, min(2000, seconds / one)))
+    t = time.perf_counter()
+    O.md_run(pos4, vel4, im3, nsteps=steps, **kw)
+    dt = time.perf_counter() - t
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"KA N={n} from the equilibrated T=0.45 state, {steps} FP32 steps (cell sort, full list, "
+                      f"SF forces, NVT) with OpenMP over particles"}
+
+
+def e2e_run(capi, device, pb, tp, pos4, vel4, im3, box, params, steps):
+    """Public API end to end: upload (H2D) + Run(steps) + read back (D2H)."""
+    e = capi.Engine(device=device, pb=pb, tp=tp)
+    e.run(0)
+    n = len(pos4)
+    t = time.perf_counter()
+    rid = e.add(pos4, box, params, 2, cutoff="SF", skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU, vel4=vel4, im3=im3)
+    e.run(steps)
+    p = e.get(rid, "pos", n)
+    v = e.get(rid, "vel", n)
+    im = e.get(rid, "images", n)
+    st = e.stats(rid)
+    dt = time.perf_counter() - t
+    e.close()
+    assert np.isfinite(p).all() and np.isfinite(st["pe"])
+    h2d = n * (16 + 16 + 16 + 16 + 4)          # r, last_r, v, images, ids
+    d2h = n * (3 * (16 + 4) + 4) + 256         # pos, vel, images (+ ids each), list lengths, state
+    return {"value": n * steps / dt, "unit": "particle-steps/s",
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps}
+
+
+def batched(capi, device, pb, tp, steps, seed=0):
+    """256 KA replicas, N log-uniform in [512, 8192], T log-spaced 0.45..2.0,
+    advanced together; against sequential plain runs of every 16th replica."""
+    from rumd_b200 import initconf as I
+    rng = np.random.default_rng(seed)
+    R = 256
+    ns = np.floor(np.exp(rng.uniform(np.log(512), np.log(8192), R))).astype(int)
+    Ts = np.exp(np.linspace(np.log(0.45), np.log(2.0), R))
+    params = ka_params()
+    confs = [I.ka_config(int(n), T=float(T), seed=seed + k) for k, (n, T) in enumerate(zip(ns, Ts))]
+    e = capi.Engine(device=device, max_particles=int(ns.sum() + 64 * R), max_replicas=R, pb=pb, tp=tp)
+    ids = [e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(T), tau=TAU,
+                 vel4=c["vel4"]) for c, T in zip(confs, Ts)]
+    e.run(500)
+    t_b = time_run(capi, e, steps, device)
+    rate_b = float(ns.sum()) * steps / t_b
+    e.close()
+    sample = list(range(0, R, 16))
+    t_seq, ps_seq = 0.0, 0.0
+    for k in sample:
+        c = confs[k]
+        s = capi.Engine(device=device, pb=pb, tp=tp)
+        s.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(Ts[k]), tau=TAU, vel4=c["vel4"])
+        s.run(500)
+        t_seq += time_run(capi, s, steps, device)
+        ps_seq += float(ns[k]) * steps
+        s.close()
+    rate_s = ps_seq / t_seq
+    return {"value": rate_b, "unit": "particle-steps/s", "replicas": R, "particles": int(ns.sum()),
+            "steps": steps, "sequential_plain_value": rate_s,
+            "sequential_sample": f"{len(sample)} of the {R} replicas run alone, one after another",
+            "speedup_vs_sequential": rate_b / rate_s}
+
+
+def config_block(args, world):
+    return {"workload": f"Kob-Andersen 80:20 LJ, N={N_PLAIN}, rho=1.2, T=0.45, NVT tau=0.2, dt=0.005, skin 0.3, "
+                        "SF cut-off 2.5 sigma_ij (plain method, single large system)",
+            "n_particles": N_PLAIN, "pb": args.pb, "tp": args.tp,
+            "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            "precision": "FP32 forces, FP64 reductions/thermostat, int32 images",
+            "l2_policy": "L2 flushed (512 MiB write) before the timed Run; inside a Run every step reads the "
+                         "state the previous step wrote, which stays L2-resident (30 MB) as in the reference"}
+
+
+def run_reference(args):
+    """The reference arm: the CPU implementation of the path (oracle port) on
+    all host cores, same workload and metric, K steps capped to ~60 s."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from rumd_b200 import initconf as I
+    c = I.ka_config(N_PLAIN, density=KA_DENSITY, T=T_PLAIN, seed=1)
+    params = ka_params()
+    kw = dict(L=c["box"], ntypes=2, params=params, cutoff=O.SF, skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU)
+    st = O.md_run(c["pos4"], c["vel4"], c["im3"], nsteps=max(args.warmup, 1), **kw)
+    t = time.perf_counter()
+    st2 = O.md_run(st["pos4"], st["vel4"], st["im3"], nsteps=2, xi=st["xi"], **kw)
+    one = (time.perf_counter() - t) / 2
+    steps = int(max(2, min(args.steps, 60.0 / max(one, 1e-6))))
+    t = time.perf_counter()
+    O.md_run(st2["pos4"], st2["vel4"], st2["im3"], nsteps=steps, xi=st2["xi"], **kw)
+    dt = time.perf_counter() - t
+    v = N_PLAIN * steps / dt
+    sample = (f"KA N={N_PLAIN} from the FCC start at T=0.45, {steps} of the requested {args.steps} steps "
+              "(capped at ~60 s), FP32 reference arithmetic, OpenMP over particles")
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_block(args, world),
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    rank, world, local = dist_env()
+    dist = Dist(world, local)
+    from rumd_b200 import capi
+    capi.lib()
+    device = local
+    e, rid, box, params = prepare_plain(capi, device, args.pb, args.tp, seed=1 + rank)
+    if args.profile_launches:
+        e.run(max(args.steps, 1))
+        e.close()
+        dist.close()
+        return
+    e.run(max(args.warmup, 3))          # untimed warm-up steps (graphs instantiated)
+    flush_l2(device)
+    rb0 = e.stats(rid)["rebuilds"]
+    clocks = ClockSampler(device)
+    clocks.start()
+    dist.barrier()
+    t = time_run(capi, e, args.steps, device)
+    dist.barrier()
+    clk = clocks.stop()
+    t_max = dist.max(t)
+    st = e.stats(rid)
+    rebuilds = st["rebuilds"] - rb0
+    total_ps = dist.sum(N_PLAIN * args.steps)
+    value = total_ps / t_max
+    # live roofline of the dominant kernel (the fused force+integrate step)
+    kms, _ = e.run_timed(2000)
+    st2 = e.stats(rid)
+    per_launch_s = kms / 2000 / 1e3
+    bytes_alg = N_PLAIN * (168.0 + 4.0 * st2["mean_nbrs"])
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_alg / per_launch_s / 1e9
+    tr = profiled_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tr or {}).get("bytes_per_launch"), "peak_source": peak_kind,
+                "kernel": "k_force<TP,fused>", "kernel_ms": per_launch_s * 1e3,
+                "bytes_per_launch_alg": bytes_alg, "mean_list_length": st2["mean_nbrs"],
+                "step_share_of_run": per_launch_s * args.steps / t}
+    extra = {}
+    if rank == 0:
+        pos4, vel4, im3 = e.get(rid, "pos", N_PLAIN), e.get(rid, "vel", N_PLAIN), e.get(rid, "images", N_PLAIN)
+        e2e = e2e_run(capi, device, args.pb, args.tp, pos4, vel4, im3, box, params, args.steps)
+        if not args.no_cpu_baseline:
+            extra["cpu_baseline"] = cpu_baseline_sample(e, rid, box, params)
+        if not args.no_batched:
+            extra["batched"] = batched(capi, device, args.pb, args.tp, args.batch_steps)
+    e.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic (seeded FCC start, melted and equilibrated untimed)",
+                "config": config_block(args, world), "clocks": clk, "e2e": e2e,
+                "gpu_launches": launches_in_run(args.steps, rebuilds), "rebuilds": rebuilds,
+                "roofline": roofline}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -72,7 +72,8 @@ extern "C" {
 #define B2MD_STAT_TARGET_T 9    /* current target temperature                   */
 #define B2MD_STAT_MAX_NBRS 10   /* list capacity per particle                   */
 #define B2MD_STAT_ACTUAL_MAX_NBRS 11 /* largest neighbour count of the last build */
-#define B2MD_NSTAT 12
+#define B2MD_STAT_MEAN_NBRS 12  /* mean neighbour-list length of the last build  */
+#define B2MD_NSTAT 13
 
 typedef struct b2md_engine b2md_engine;
 
@@ -145,7 +146,10 @@ B2MD_API int b2md_replica_set_nb_method(b2md_engine* e, int id, int method);
 /* FP64 scalars of the replica, B2MD_NSTAT doubles (Sample::GetPotentialEnergy,
  * GetVirial, IntegratorNVT::GetKineticEnergy/GetThermostatState). */
 B2MD_API int b2md_replica_stats(b2md_engine* e, int id, double* out);
-/* Energy log: up to cap entries of (step, pe, W, KE, xi); returns count. */
+/* (Re)configures the energy log: one entry every interval steps of a run,
+ * the last capacity entries kept; clears the log. */
+B2MD_API int b2md_replica_set_energy_log(b2md_engine* e, int id, int interval, int capacity);
+/* Energy log: up to cap entries of (run step, pe, W, KE, xi); returns count. */
 B2MD_API int b2md_replica_energy_log(b2md_engine* e, int id, double* out, int cap, int* count);
 /* Stress tensor sum (Sample::GetStress, Sample.cu:393-444): 6 doubles
  * (xx, yy, zz, yz, xz, xy), requires a force evaluation with stress. */
@@ -165,6 +169,11 @@ B2MD_API int b2md_zero_momentum(b2md_engine* e);
  * decided on the device; list overflow is repaired on the host (capacity
  * doubled, NeighborList.cu:657-676) and the run resumed. */
 B2MD_API int b2md_run(b2md_engine* e, long long nsteps);
+/* b2md_run with eager launches instead of graphs, for measurement: CUDA
+ * events on the engine's stream bracket every fused step kernel.  Returns the
+ * summed step-kernel time and the number of kernel launches in the run. */
+B2MD_API int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms,
+                            long long* launches);
 /* Batched/served form: each replica advances its own queued step count
  * (b2md_replica_queue_steps) in the same launches; returns when all queues
  * are empty or after max_steps launches-worth of steps (0 = until empty). */

@@ -103,6 +103,15 @@ static inline int cell_coord_ref(float x, float invL, int nc) {
   return c;
 }
 
+// Squared minimum-image distances of n pairs (calculateDistance).
+ORC_API void orc_dist2(int n, const float* a4, const float* b4, const float* L, float* out) {
+  float invL[3] = {1.f / L[0], 1.f / L[1], 1.f / L[2]};
+  for (int i = 0; i < n; ++i)
+    out[i] = dist2_ref(mi_f32(a4[4 * i] - b4[4 * i], L[0], invL[0]),
+                       mi_f32(a4[4 * i + 1] - b4[4 * i + 1], L[1], invL[1]),
+                       mi_f32(a4[4 * i + 2] - b4[4 * i + 2], L[2], invL[2]));
+}
+
 // NeighborList::CalculateNBL_Sorting cell grid: max(floor(2L/(rc+skin)), 5).
 ORC_API void orc_cell_grid(const float* L, float max_cut, float skin, int* nc) {
   for (int d = 0; d < 3; ++d) {

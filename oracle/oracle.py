@@ -38,6 +38,7 @@ def lib():
         i, f, d, u = ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_uint
         L.orc_lj_set_params.argtypes = [i, P, i, i, f, f, f]
         L.orc_cell_grid.argtypes = [P, f, f, P]
+        L.orc_dist2.argtypes = [i, P, P, P, P]
         L.orc_cell_keys.argtypes = [i, P, P, P, P]
         L.orc_stable_sort_perm.argtypes = [i, P, i, P]
         L.orc_nbl_build_cells.argtypes = [i, P, P, P, i, P, f, i, P, P]
@@ -86,6 +87,14 @@ def lj_table():
 
 def max_cutoff(params, ntypes):
     return float(params.reshape(ntypes * ntypes, NUM_PARAM)[:, 0].max())
+
+
+def dist2(a4, b4, L):
+    a4 = np.ascontiguousarray(a4, np.float32)
+    b4 = np.ascontiguousarray(b4, np.float32)
+    out = np.zeros(len(a4), np.float32)
+    lib().orc_dist2(len(a4), _p(a4), _p(b4), _p(np.asarray(L, np.float32)), _p(out))
+    return out
 
 
 def cell_grid(L, max_cut, skin):

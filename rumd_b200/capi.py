@@ -18,7 +18,7 @@ B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_O
 CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",
-              "target_T", "max_nbrs", "actual_max_nbrs"]
+              "target_T", "max_nbrs", "actual_max_nbrs", "mean_nbrs"]
 NSTAT = len(STAT_NAMES)
 NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
 
@@ -27,8 +27,8 @@ EXPORTS = [
     "b2md_engine_set_graph_mode", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
     "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_set_integrator",
     "b2md_replica_set_xi", "b2md_replica_set_reset_interval", "b2md_replica_set_nb_method",
-    "b2md_replica_stats", "b2md_replica_energy_log", "b2md_replica_stress", "b2md_calc_f",
-    "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_replica_queue_steps",
+    "b2md_replica_stats", "b2md_replica_set_energy_log", "b2md_replica_energy_log", "b2md_replica_stress", "b2md_calc_f",
+    "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
     "b2md_run_queued", "b2md_nbl_export", "b2md_sort_export", "b2md_cell_grid", "b2md_sync",
     "b2md_stream", "b2md_last_error", "b2md_version", "b2md_probe_dist2", "b2md_probe_cell",
 ]
@@ -74,12 +74,14 @@ def lib():
             "b2md_replica_set_reset_interval": [P, i, i],
             "b2md_replica_set_nb_method": [P, i, i],
             "b2md_replica_stats": [P, i, P],
+            "b2md_replica_set_energy_log": [P, i, i, i],
             "b2md_replica_energy_log": [P, i, P, i, ctypes.POINTER(i)],
             "b2md_replica_stress": [P, i, i, P],
             "b2md_calc_f": [P, i],
             "b2md_integrate": [P],
             "b2md_zero_momentum": [P],
             "b2md_run": [P, ll],
+            "b2md_run_timed": [P, ll, ctypes.POINTER(d), ctypes.POINTER(ll)],
             "b2md_replica_queue_steps": [P, i, ll],
             "b2md_run_queued": [P, ll, ctypes.POINTER(ll)],
             "b2md_nbl_export": [P, i, P, P, i],
@@ -238,6 +240,9 @@ class Engine:
         check(lib().b2md_replica_stats(self._h, rid, _ptr(out)))
         return dict(zip(STAT_NAMES, out.tolist()))
 
+    def set_energy_log(self, rid, interval, capacity):
+        check(lib().b2md_replica_set_energy_log(self._h, rid, int(interval), int(capacity)))
+
     def energy_log(self, rid, cap=1 << 20):
         out = np.zeros((cap, 5))
         cnt = ctypes.c_int()
@@ -260,6 +265,16 @@ class Engine:
 
     def run(self, nsteps):
         check(lib().b2md_run(self._h, int(nsteps)))
+
+    def run_timed(self, nsteps):
+        """Eager run with CUDA events around every fused step kernel: (kernel ms, launches)."""
+        ms = ctypes.c_double()
+        nl = ctypes.c_longlong()
+        check(lib().b2md_run_timed(self._h, int(nsteps), ctypes.byref(ms), ctypes.byref(nl)))
+        return ms.value, nl.value
+
+    def stream(self):
+        return lib().b2md_stream(self._h)
 
     def queue(self, rid, nsteps):
         check(lib().b2md_replica_queue_steps(self._h, rid, int(nsteps)))

@@ -662,7 +662,7 @@ int guarded(F&& fn) {
 void launch_momentum(b2md_engine* e) {
   if (e->ntiles == 0) return;
   EngArgs a = make_args(e);
-  k_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+  k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
   check_launch();
 }
 
@@ -1044,6 +1044,42 @@ int b2md_replica_stats(b2md_engine* e, int id, double* out) {
     out[B2MD_STAT_TARGET_T] = s.T;
     out[B2MD_STAT_MAX_NBRS] = h.d.max_nbrs;
     out[B2MD_STAT_ACTUAL_MAX_NBRS] = s.actual_max_nbrs;
+    std::vector<unsigned> nn(h.n);
+    CK(cudaMemcpyAsync(nn.data(), e->nn + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    double tot = 0;
+    for (unsigned c : nn) tot += c;
+    out[B2MD_STAT_MEAN_NBRS] = tot / h.n;
+  });
+}
+
+int b2md_replica_set_energy_log(b2md_engine* e, int id, int interval, int capacity) {
+  if (interval < 0 || capacity < 0) return fail(B2MD_ERR_ARG, "interval and capacity must be >= 0");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    if (h.elog0 >= 0) e->zalloc.release(h.elog0, h.ecap);
+    h.elog0 = -1;
+    h.ecap = 0;
+    h.d.energy_interval = 0;
+    h.d.energy_cap = 0;
+    h.d.elog0 = 0;
+    if (interval > 0 && capacity > 0) {
+      long long z = e->zalloc.alloc(capacity, 1);
+      if (z < 0) {
+        grow_elog(e, e->zalloc.used_end() + capacity);
+        z = e->zalloc.alloc(capacity, 1);
+      }
+      h.elog0 = z;
+      h.ecap = capacity;
+      h.d.elog0 = z;
+      h.d.energy_cap = capacity;
+      h.d.energy_interval = interval;
+    }
+    upload_rep(e, id);
+    WRITE_STATE(e, id, nlog, 0);
+    invalidate_graphs(e);
   });
 }
 
@@ -1112,7 +1148,7 @@ int b2md_integrate(b2md_engine* e) {
     CK(cudaSetDevice(e->device));
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
-    k_integrate<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    k_integrate<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
     check_launch();
   });
 }
@@ -1123,9 +1159,9 @@ int b2md_zero_momentum(b2md_engine* e) {
     CK(cudaSetDevice(e->device));
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
-    k_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
     k_apply_zero_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
-    k_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
+    k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
     check_launch();
   });
 }
@@ -1144,6 +1180,48 @@ int b2md_run(b2md_engine* e, long long nsteps) {
     if (nsteps > 0) run_steps(e, nsteps);
     calc_f(e, false);
     CK(cudaStreamSynchronize(e->stream));
+  });
+}
+
+int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, long long* launches) {
+  if (!e || !step_kernel_ms || !launches) return fail(B2MD_ERR_ARG, "null argument");
+  if (nsteps < 0) return fail(B2MD_ERR_ARG, "nsteps must be >= 0");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    *step_kernel_ms = 0.0;
+    *launches = 0;
+    if (e->ntiles == 0) return;
+    EngArgs a = make_args(e);
+    int R = (int)e->reps.size();
+    k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
+    launch_momentum(e);
+    long long nl = 2;
+    const int mt = max_types(e);
+    const size_t smem = (size_t)mt * mt * kParStride * sizeof(float);
+    ForceFn fstep = force_fn(e->tp, true, false);
+    std::vector<cudaEvent_t> ev(2 * nsteps);
+    for (auto& x : ev) CK(cudaEventCreate(&x));
+    for (long long k = 0; k < nsteps; ++k) {
+      launch_rebuild(e, e->stream, a);
+      CK(cudaEventRecord(ev[2 * k], e->stream));
+      fstep<<<e->ntiles, e->pb * e->tp, smem, e->stream>>>(a, 0, cudaGraphConditionalHandle{});
+      CK(cudaEventRecord(ev[2 * k + 1], e->stream));
+      nl += 10;
+    }
+    check_launch();
+    CK(cudaStreamSynchronize(e->stream));
+    double tot = 0.0;
+    for (long long k = 0; k < nsteps; ++k) {
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, ev[2 * k], ev[2 * k + 1]));
+      tot += ms;
+    }
+    for (auto& x : ev) cudaEventDestroy(x);
+    if (repair_overflow(e)) run_steps(e, nsteps);
+    calc_f(e, false);
+    CK(cudaStreamSynchronize(e->stream));
+    *step_kernel_ms = tot;
+    *launches = nl + 10;
   });
 }
 

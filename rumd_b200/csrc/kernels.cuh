@@ -162,6 +162,7 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   S->ke_t = tot[P_KET];
   if (with_forces) { S->pe = tot[P_PE]; S->vir = tot[P_W] / 6.0; }
   S->P[0] = tot[P_PX]; S->P[1] = tot[P_PY]; S->P[2] = tot[P_PZ]; S->M = tot[P_M];
+  const long long run_idx = S->run_step;  // step index inside the current run, before this step
   S->rbuf ^= 1;
   S->steps += 1;
   S->run_step += 1;
@@ -169,10 +170,12 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
   if (ex > 0) atomicAdd(a.any_rebuild, 1);
-  if (R.energy_interval > 0 && (S->steps % R.energy_interval) == 0 && R.energy_cap > 0) {
+  // energies at run steps i with i % interval == 0, as Simulation.Run's
+  // energies output schedule (Simulation.py:44, 587-589)
+  if (R.energy_interval > 0 && (run_idx % R.energy_interval) == 0 && R.energy_cap > 0) {
     int k = S->nlog % R.energy_cap;
     double* e = a.elog + (size_t)(R.elog0 + k) * 5;
-    e[0] = (double)S->steps; e[1] = S->pe; e[2] = S->vir; e[3] = S->ke_t; e[4] = S->xi;
+    e[0] = (double)run_idx; e[1] = S->pe; e[2] = S->vir; e[3] = S->ke_t; e[4] = S->xi;
     S->nlog += 1;
   }
 }
@@ -309,8 +312,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
   grid_final(a, has_cond, h);
 }
 
-// IntegratorNVT::Integrate alone (forces already in f).  One thread per particle.
-__global__ void __launch_bounds__(kMaxBlock) k_integrate(EngArgs a) {
+// IntegratorNVT::Integrate alone (forces already in f).  Particle p of the
+// tile sits on thread p*tp, as in k_force, so the FP64 reduction tree (and
+// hence every bit of the result) is the same as the fused step's.
+__global__ void __launch_bounds__(kMaxBlock) k_integrate(EngArgs a, int tp) {
   __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
   __shared__ double s_scr[kMaxBlock];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
@@ -319,13 +324,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(EngArgs a) {
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   if (S->overflow || !R.active) return;
-  const int i = a.tile_first[tile] + threadIdx.x;
+  const int i = a.tile_first[tile] + threadIdx.x / tp;
   double acc[kNPart];
 #pragma unroll
   for (int k = 0; k < kNPart; ++k) acc[k] = 0.0;
   bool exceed = false;
   const int rb = S->rbuf, ab = S->abuf;
-  if (i < R.n) {
+  if (i < R.n && threadIdx.x % tp == 0) {
     const size_t gi = (size_t)R.p0 + i;
     float4 r = a.r[rb][gi], f = a.f[gi], v = a.v[ab][gi];
     int4 im = a.im[ab][gi];
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(EngArgs a) {
 
 // Total momentum and mass of the current velocities (calculateMomentum +
 // sumIdenticalArrays, IntegratorNVT.cu:176-183, 462-471), FP64.
-__global__ void __launch_bounds__(kMaxBlock) k_momentum(EngArgs a) {
+__global__ void __launch_bounds__(kMaxBlock) k_momentum(EngArgs a, int tp) {
   __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
   __shared__ double s_scr[kMaxBlock];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
@@ -357,11 +362,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_momentum(EngArgs a) {
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   if (!R.active) return;
-  const int i = a.tile_first[tile] + threadIdx.x;
+  const int i = a.tile_first[tile] + threadIdx.x / tp;
   double acc[kNPart];
 #pragma unroll
   for (int k = 0; k < kNPart; ++k) acc[k] = 0.0;
-  if (i < R.n) {
+  if (i < R.n && threadIdx.x % tp == 0) {
     const float4 v = a.v[S->abuf][(size_t)R.p0 + i];
     const double m = 1.0 / (double)v.w;
     acc[P_PX] = m * v.x; acc[P_PY] = m * v.y; acc[P_PZ] = m * v.z; acc[P_M] = m;

@@ -1,0 +1,102 @@
+"""Host-side logic of the RUMD class surface (no GPU calls).
+
+Parameter mapping, configuration files and error behaviour run entirely on
+the host until the first force evaluation creates the device replica."""
+import gzip
+
+import numpy as np
+import pytest
+
+from conftest import golden_files, load_golden
+
+
+@pytest.fixture(scope="module")
+def rumd():
+    from rumd_b200 import build
+    build.build()
+    from rumd_b200 import rumd
+    return rumd
+
+
+def write_xyz(path, g):
+    n = len(g["type"])
+    L = g["L"]
+    with gzip.open(path, "wt") as fh:
+        fh.write(f"{n}\n")
+        fh.write(f"ioformat=1 dt=0.005 boxLengths={L[0]:.9f},{L[1]:.9f},{L[2]:.9f} numTypes=2 "
+                 f"Nose-Hoover-Ps={g['xi']:.9f} Barostat-Pv=0.0 mass=1.0,1.0 columns=type,x,y,z,vx,vy,vz,fx,fy,fz,pe\n")
+        for i in range(n):
+            p, v, f = g["pos"][i], g["vel"][i], g["force"][i]
+            fh.write(f"{g['type'][i]} {p[0]:.6f} {p[1]:.6f} {p[2]:.6f} {v[0]:.6f} {v[1]:.6f} {v[2]:.6f} "
+                     f"{f[0]:.6f} {f[1]:.6f} {f[2]:.6f} {g['pe'][i]:.6f}\n")
+
+
+def ka_potential(rumd, method):
+    pot = rumd.Pot_LJ_12_6(cutoff_method=method)
+    pot.SetParams(0, 0, 1.0, 1.0, 2.5)
+    pot.SetParams(0, 1, 0.8, 1.5, 2.5)
+    pot.SetParams(1, 1, 0.88, 0.5, 2.5)
+    return pot
+
+
+def test_lj_parameter_table_equals_oracle(rumd, oracle):
+    pot = ka_potential(rumd, rumd.ShiftedForce)
+    table = np.array(pot.ParamTable(2), np.float32)
+    ref = oracle.lj_params(2, oracle.ka_table())
+    assert np.array_equal(table.view(np.uint32), ref.view(np.uint32))
+    # GetPotentialParameter(i, j, 0) is the absolute cut-off Rcut*sigma
+    assert pot.GetPotentialParameter(1, 0, 0) == np.float32(2.5) * np.float32(0.8)
+    assert pot.GetMaxCutoff() == np.float32(2.5)
+    assert len(pot.GetPotentialParameters(2)) == 4 * 10
+
+
+def test_ipl_and_lj_agree(rumd):
+    lj = rumd.Pot_LJ_12_6(rumd.ShiftedPotential)
+    lj.SetParams(0, 0, 1.0, 1.0, 2.5)
+    ipl = rumd.Pot_IPL_12_6(rumd.ShiftedPotential)
+    ipl.SetParams(0, 0, 4.0, -4.0, 2.5)
+    assert lj.ParamTable(1) == ipl.ParamTable(1)
+
+
+def test_readconf_host_side(rumd, tmp_path):
+    g = load_golden([p for p in golden_files() if "N1000_T0.5" in p][0])
+    path = tmp_path / "conf.xyz.gz"
+    write_xyz(path, g)
+    s = rumd.Sample(0, 0)
+    s.ReadConf(str(path))
+    assert s.GetNumberOfParticles() == 1000
+    assert s.GetNumberOfTypes() == 2
+    assert s.GetNumberThisType(1) == int((g["type"] == 1).sum())
+    assert np.allclose(s.GetPositions(), g["pos"], atol=1e-6)
+    assert np.allclose(s.GetVelocities(), g["vel"], atol=1e-6)
+    assert s.GetNumberOfDOFs() == 3 * 1000 - 3
+    assert abs(s.GetVolume() - float(np.prod(g["L"]))) < 1e-3
+
+
+def test_errors_map_to_python_exceptions(rumd, tmp_path):
+    s = rumd.Sample(0, 0)
+    with pytest.raises(RuntimeError):
+        s.CalcF()  # no configuration
+    with pytest.raises(ValueError):
+        s.SetPB_TP(48, 4)  # pb not a multiple of 32
+    pot = rumd.Pot_LJ_12_6(rumd.ShiftedForce)
+    with pytest.raises(RuntimeError):
+        pot.SetNB_Method("cells")
+    with pytest.raises(RuntimeError):
+        s.ReadConf(str(tmp_path / "missing.xyz.gz"))
+    sim = rumd.Simulation(sample=rumd.Sample())
+    with pytest.raises(ValueError):
+        sim.Run(10)  # no integrator
+
+
+def test_integrator_settings_before_sample(rumd):
+    itg = rumd.IntegratorNVT(timeStep=0.005, targetTemperature=0.8, thermostatRelaxationTime=0.2)
+    assert itg.GetTimeStep() == np.float32(0.005)
+    assert itg.GetTargetTemperature() == 0.8
+    assert itg.GetThermostatOn()
+    itg.SetThermostatOn(False)
+    assert itg.GetThermostatState() == 0.0
+    nve = rumd.IntegratorNVE(timeStep=0.004)
+    assert not nve.GetThermostatOn()
+    with pytest.raises(RuntimeError):
+        itg.SetThermostatOnParticleType(40, True)
