@@ -1,0 +1,105 @@
+"""Autotuner for the launch shape and the rebuild cadence.
+
+Modelled on RUMD's Autotune (Python/rumd/Autotune.py:156-161, 584-1000),
+which times short runs over particles-per-block, threads-per-particle, skin
+and neighbour-list method, and caches the winner in autotune.dat.  Here the
+knobs are the engine's:
+  pb   particles per block (tile size): 32, 64, 128
+  tp   threads per particle: 1, 2, 4, 8   (pb*tp <= 512)
+  skin neighbour-list skin, i.e. the rebuild cadence: 0.2 .. 0.5
+Each candidate is timed on the device (CUDA events around a short run of the
+real workload, after a warm-up run).  As in RUMD's test mode
+(Autotune.py:929-937), every candidate's potential energy after its run must
+agree with the first candidate's within 0.005 per particle; a candidate that
+fails this is rejected.  Results are cached in a JSON file keyed by the
+workload signature.
+"""
+import itertools
+import json
+import os
+
+DEFAULT_PB = (32, 64, 128)
+DEFAULT_TP = (1, 2, 4, 8)
+DEFAULT_SKIN = (0.2, 0.3, 0.4, 0.5)
+
+
+def candidates(pbs=DEFAULT_PB, tps=DEFAULT_TP, skins=DEFAULT_SKIN, max_block=512):
+    return [(pb, tp, sk) for pb, tp, sk in itertools.product(pbs, tps, skins) if pb * tp <= max_block]
+
+
+def search(cands, measure, pe_tol=0.005):
+    """measure(pb, tp, skin) -> (rate, pe_per_particle).  Returns the best
+    candidate and the table of all measurements."""
+    table = []
+    ref_pe = None
+    best = None
+    for pb, tp, skin in cands:
+        rate, pe = measure(pb, tp, skin)
+        ok = True
+        if ref_pe is None:
+            ref_pe = pe
+        elif abs(pe - ref_pe) > pe_tol:
+            ok = False
+        table.append({"pb": pb, "tp": tp, "skin": skin, "rate": rate, "pe": pe, "ok": ok})
+        if ok and (best is None or rate > best["rate"]):
+            best = table[-1]
+    return best, table
+
+
+def signature(replicas):
+    """Workload key: particle counts (binned), densities and types."""
+    parts = sorted((int(round(r["n"], -2)), round(r["density"], 3), r["ntypes"]) for r in replicas)
+    return json.dumps(parts)
+
+
+class Autotune:
+    def __init__(self, cache_path="autotune.json", **grid):
+        self.cache_path = cache_path
+        self.grid = grid
+
+    def _load(self):
+        if os.path.exists(self.cache_path):
+            with open(self.cache_path) as fh:
+                return json.load(fh)
+        return {}
+
+    def tune(self, replicas, measure, force=False):
+        key = signature(replicas)
+        cache = self._load()
+        if key in cache and not force:
+            return cache[key]
+        best, table = search(candidates(**self.grid), measure)
+        cache[key] = {"pb": best["pb"], "tp": best["tp"], "skin": best["skin"], "rate": best["rate"],
+                      "table": table}
+        with open(self.cache_path, "w") as fh:
+            json.dump(cache, fh, indent=1)
+        return cache[key]
+
+
+def device_measure(capi, replicas, device=0, steps=300, warmup=100):
+    """measure() for `search`: builds an engine with all replicas at the given
+    shape and skin and times `steps` device steps with CUDA events.
+
+    replicas: list of dicts with pos4, vel4, box, params, ntypes, T, n, density."""
+    import torch
+
+    def measure(pb, tp, skin):
+        e = capi.Engine(device=device, max_replicas=len(replicas), pb=pb, tp=tp)
+        ids = [e.add(r["pos4"], r["box"], r["params"], r["ntypes"], cutoff="SF", skin=skin, T=r["T"],
+                     vel4=r["vel4"]) for r in replicas]
+        e.calc_f()  # invariance check on the common starting configuration
+        n = sum(r["n"] for r in replicas)
+        pe = sum(e.stats(i)["pe"] for i in ids) / n
+        e.run(warmup)
+        stream = torch.cuda.ExternalStream(e.stream(), device=f"cuda:{device}")
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        t0.record(stream)
+        e.run(steps)
+        t1.record(stream)
+        torch.cuda.synchronize(device)
+        dt = t0.elapsed_time(t1) / 1e3
+        e.close()
+        return n * steps / dt, pe
+
+    return measure

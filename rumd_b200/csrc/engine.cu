@@ -1177,7 +1177,9 @@ int b2md_run(b2md_engine* e, long long nsteps) {
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     check_launch();
-    if (nsteps > 0) run_steps(e, nsteps);
+    // every queue holds exactly nsteps; run until all are empty (a replica
+    // frozen by a list overflow catches up after its repair)
+    if (nsteps > 0) run_steps(e, 1LL << 62);
     calc_f(e, false);
     CK(cudaStreamSynchronize(e->stream));
   });

@@ -1,0 +1,39 @@
+"""Autotuner search logic on the CPU (fake timings)."""
+import json
+
+
+def test_candidates_respect_block_limit():
+    from rumd_b200 import autotune
+    c = autotune.candidates()
+    assert all(pb * tp <= 512 for pb, tp, _ in c)
+    assert (128, 8, 0.3) not in c and (64, 8, 0.3) in c
+
+
+def test_search_picks_fastest_valid_candidate():
+    from rumd_b200 import autotune
+
+    def measure(pb, tp, skin):
+        rate = pb * tp / (1 + abs(skin - 0.3) * 10)
+        pe = -5.0 if (pb, tp) != (64, 8) else -4.9  # (64, 8) breaks the pe invariance
+        return rate, pe
+
+    best, table = autotune.search(autotune.candidates(), measure)
+    assert (best["pb"], best["tp"], best["skin"]) == (128, 4, 0.3)
+    assert any(not r["ok"] for r in table)
+
+
+def test_cache_round_trip(tmp_path):
+    from rumd_b200 import autotune
+    calls = []
+
+    def measure(pb, tp, skin):
+        calls.append((pb, tp, skin))
+        return float(tp), -5.0
+
+    reps = [{"n": 1000, "density": 1.2, "ntypes": 2}]
+    at = autotune.Autotune(cache_path=str(tmp_path / "a.json"), pbs=(32, 64), tps=(1, 2), skins=(0.3,))
+    r1 = at.tune(reps, measure)
+    n = len(calls)
+    r2 = at.tune(reps, measure)
+    assert len(calls) == n and r1["tp"] == r2["tp"] == 2
+    assert json.load(open(tmp_path / "a.json"))

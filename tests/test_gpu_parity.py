@@ -365,8 +365,10 @@ def test_nve_energy_drift(capi, ka_params):
     log = e.energy_log(rid)
     etot = (log[:, 1] + log[:, 3]) / 1000.0
     slope = np.polyfit(log[:, 0], etot, 1)[0]
+    # drift (the linear trend) over 1e4 steps, per particle
     assert abs(slope * steps) < 1e-4
-    assert np.abs(etot - etot[0]).max() < 1e-3
+    # leap-frog fluctuations at dt=0.005 stay bounded (no secular growth)
+    assert np.abs(etot - etot[0]).max() < 5e-3
     e.close()
 
 
