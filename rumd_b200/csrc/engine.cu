@@ -161,6 +161,7 @@ struct b2md_engine {
 namespace {
 
 constexpr int kChunk = 32;
+constexpr int kMaxDynSmemBytes = 220 * 1024;  // dynamic shared memory a list-tile kernel may use
 
 template <class T>
 void dev_grow(b2md_engine* e, T*& p, long long old_n, long long new_n, bool zero_new) {
@@ -267,7 +268,18 @@ EngArgs make_args(b2md_engine* e) {
   a.gctr = e->gctr; a.rctr = e->rctr; a.fctr = e->fctr; a.any_rebuild = e->any_rebuild; a.elog = e->elog;
   a.ntiles = e->ntiles;
   a.nrep = (int)e->reps.size();
+  // staged list tile: pb columns + padding so that the tp rows a warp reads
+  // at once fall in different shared-memory banks
+  a.idx_pitch = e->pb + (e->tp > 1 ? 32 / e->tp : 0);
+  a.idx_rows = 0;
+  for (auto& h : e->reps)
+    if (h.active) a.idx_rows = std::max(a.idx_rows, h.d.max_nbrs);
   return a;
+}
+
+// Dynamic shared memory of k_force: pair table + staged list tile.
+size_t force_smem(const EngArgs& a) {
+  return (size_t)kParSmemFloats * sizeof(float) + (size_t)a.idx_rows * a.idx_pitch * sizeof(unsigned);
 }
 
 // Re-lays out tiles and reduction groups over the active replicas and uploads
@@ -369,6 +381,7 @@ void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, floa
   for (int k = 0; k < ntypes * ntypes; ++k) h.rcmax = std::max(h.rcmax, params[k * kNumParam]);
   if (!(h.rcmax > 0.f)) api_fail(B2MD_ERR_ARG, "all cut-offs are zero");
   h.d.skin2_4 = (float)(0.25 * skin * skin);
+  for (int d = 0; d < 3; ++d) h.d.ilim[d] = 0.5f * h.d.L[d] - (h.rcmax + 2.f * skin) - 0.01f;
   int ncheck[3];
   for (int d = 0; d < 3; ++d) {
     float q = 2 * h.d.L[d] / (h.rcmax + skin);
@@ -388,12 +401,15 @@ std::vector<float> pack_params(const HostRep& h) {
     const float* p = &h.params[k * kNumParam];
     float* q = &out[k * kParStride];
     float rc = p[0];
+    const float sc = p[kNumParam - 2], uc = p[kNumParam - 1];  // s(rc)*rc, u(rc)
     q[0] = rc * rc;
     q[1] = p[1];
     q[2] = p[2];
-    q[3] = p[kNumParam - 2];
-    q[4] = p[kNumParam - 1];
-    q[5] = rc;
+    // fij's cut-off terms (PairPotential.h:1208-1221) as s -= c_s/r, u += c_ur r + c_u0
+    const bool sf = h.d.cutoff == CUT_SF, sp = h.d.cutoff == CUT_SP;
+    q[3] = sf ? sc : 0.f;
+    q[4] = sf ? -(sc * rc + uc) : (sp ? -uc : 0.f);
+    q[5] = sf ? sc : 0.f;
     float cs = rc + h.skin;  // calculateNBL_*: (params + skin)^2 in float
     q[6] = cs * cs;
     q[7] = 0.f;
@@ -464,8 +480,6 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   const int T = e->ntiles;
   const int R = (int)e->reps.size();
   if (T == 0) return;
-  int maxt = 1;
-  for (auto& h : e->reps) if (h.active) maxt = std::max(maxt, h.d.ntypes);
   k_rb_begin<<<(R + 127) / 128, 128, 0, s>>>(a);
   k_rb_clear<<<T, e->pb, 0, s>>>(a);
   k_rb_count<<<T, e->pb, 0, s>>>(a);
@@ -474,18 +488,19 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   k_rb_scatter<<<T, e->pb, 0, s>>>(a);
   k_rb_fix<<<T, e->pb, 0, s>>>(a);
   k_rb_permute<<<T, e->pb, 0, s>>>(a);
-  k_rb_build<<<T, e->pb, maxt * maxt * sizeof(float), s>>>(a);
-}
-
-int max_types(b2md_engine* e) {
-  int m = 1;
-  for (auto& h : e->reps) if (h.active) m = std::max(m, h.d.ntypes);
-  return m;
+  // list build: LP lanes per particle, the tile's list staged in shared memory
+  const size_t smem = (size_t)kCs2Floats * sizeof(float) + (size_t)a.idx_rows * (e->pb + 4) * sizeof(unsigned);
+  if (smem > kMaxDynSmemBytes)
+    api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
+  const int lp = std::min(8, kMaxBlock / e->pb);
+  void (*fb)(EngArgs) = lp >= 8 ? k_rb_build<8> : lp >= 4 ? k_rb_build<4> : lp >= 2 ? k_rb_build<2> : k_rb_build<1>;
+  const int lanes = lp >= 8 ? 8 : lp >= 4 ? 4 : lp >= 2 ? 2 : 1;
+  fb<<<T, e->pb * lanes, smem, s>>>(a);
 }
 
 typedef void (*ForceFn)(EngArgs, int, cudaGraphConditionalHandle);
 
-ForceFn force_fn(int tp, bool fused, bool stress) {
+ForceFn force_fn_raw(int tp, bool fused, bool stress) {
 #define SEL(TPV)                                               \
   if (tp == TPV) {                                             \
     if (fused) return k_force<TPV, true, false>;               \
@@ -496,12 +511,35 @@ ForceFn force_fn(int tp, bool fused, bool stress) {
   return nullptr;
 }
 
+// The force kernel for (tp, fused, stress), allowed to use the dynamic
+// shared memory the staged list tile `a` needs.
+ForceFn force_fn(int tp, bool fused, bool stress, const EngArgs& a) {
+  ForceFn fn = force_fn_raw(tp, fused, stress);
+  if (force_smem(a) > kMaxDynSmemBytes)
+    api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
+  return fn;
+}
+
+// Lets every kernel that stages list tiles use up to kMaxDynSmemBytes of
+// dynamic shared memory (set once, before any stream capture).
+void init_func_attrs(int device) {
+  static unsigned long long done_mask = 0ull;  // one bit per device
+  const unsigned long long bit = 1ull << (device & 63);
+  if (done_mask & bit) return;
+  const void* fns[] = {(const void*)k_rb_build<1>, (const void*)k_rb_build<2>, (const void*)k_rb_build<4>,
+                       (const void*)k_rb_build<8>};
+  for (const void* f : fns) CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
+  for (int tp : {1, 2, 4, 8})
+    for (int v = 0; v < 3; ++v)
+      CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2),
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
+  done_mask |= bit;
+}
+
 void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
   if (e->ntiles == 0) return;
-  int mt = max_types(e);
-  size_t smem = (size_t)mt * mt * kParStride * sizeof(float);
-  ForceFn fn = force_fn(e->tp, fused, stress);
-  fn<<<e->ntiles, e->pb * e->tp, smem, s>>>(a, 0, cudaGraphConditionalHandle{});
+  ForceFn fn = force_fn(e->tp, fused, stress, a);
+  fn<<<e->ntiles, e->pb * e->tp, force_smem(a), s>>>(a, 0, cudaGraphConditionalHandle{});
 }
 
 void check_launch() { CK(cudaGetLastError()); }
@@ -511,9 +549,8 @@ void build_graph(b2md_engine* e, int which, int K) {
   EngArgs a = make_args(e);
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
-  const int mt = max_types(e);
-  const size_t smem = (size_t)mt * mt * kParStride * sizeof(float);
-  ForceFn fstep = force_fn(e->tp, true, false);
+  const size_t smem = force_smem(a);
+  ForceFn fstep = force_fn(e->tp, true, false, a);
   if (e->cond_mode) {
     std::vector<cudaGraphConditionalHandle> hs(K);
     for (int k = 0; k < K; ++k) CK(cudaGraphConditionalHandleCreate(&hs[k], g, 0, cudaGraphCondAssignDefault));
@@ -582,6 +619,10 @@ void ensure_graphs(b2md_engine* e) {
 bool repair_overflow(b2md_engine* e) {
   std::vector<RepState> s = read_states(e);
   bool any = false;
+  for (size_t r = 0; r < e->reps.size(); ++r)
+    if (e->reps[r].active && s[r].err)
+      api_fail(B2MD_ERR_CUDA, "a bounded device wait for the neighbour-list copy gave up (replica " +
+                                  std::to_string(r) + ")");
   for (size_t r = 0; r < e->reps.size(); ++r) {
     HostRep& h = e->reps[r];
     if (!h.active || !s[r].overflow) continue;
@@ -701,6 +742,7 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
     grow_params(e, 1024);
     grow_elog(e, 16);
     grow_reps(e, std::max(max_replicas, 1));
+    init_func_attrs(device);
     CK(cudaMalloc(&e->fctr, sizeof(unsigned)));
     CK(cudaMalloc(&e->any_rebuild, sizeof(int)));
     CK(cudaMemsetAsync(e->fctr, 0, sizeof(unsigned), e->stream));
@@ -1198,9 +1240,8 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     long long nl = 2;
-    const int mt = max_types(e);
-    const size_t smem = (size_t)mt * mt * kParStride * sizeof(float);
-    ForceFn fstep = force_fn(e->tp, true, false);
+    const size_t smem = force_smem(a);
+    ForceFn fstep = force_fn(e->tp, true, false, a);
     std::vector<cudaEvent_t> ev(2 * nsteps);
     for (auto& x : ev) CK(cudaEventCreate(&x));
     for (long long k = 0; k < nsteps; ++k) {

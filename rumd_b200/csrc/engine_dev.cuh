@@ -32,7 +32,8 @@ enum { P_PE = 0, P_W, P_KE2, P_KET, P_PX, P_PY, P_PZ, P_M };
 enum { CUT_NS = 0, CUT_SP = 1, CUT_SF = 2 };
 enum { NB_CELLS = 0, NB_N2 = 1 };
 
-// Packed pair row: rc^2, A12, A6, p10 = s(rc)*rc, p11 = u(rc), rc, (rc+skin)^2, 0
+// Packed pair row (8 floats): rc^2, A12, A6, c_s, c_u0, c_ur, (rc+skin)^2, 0.
+// The cut-off method is folded into c_s, c_u0, c_ur (see lj_pair).
 struct RepDev {
   int n, p0, tile0, ntiles;
   int group0, ngroups;
@@ -43,6 +44,7 @@ struct RepDev {
   int max_nbrs, nbl_stride;
   long long nbl0;
   float L[3], invL[3];
+  float ilim[3];  // |x| below L/2 - (rc_max + 2 skin): no minimum image needed (k_force)
   float skin2_4;
   float dt, omega2;
   int cutoff;
@@ -66,6 +68,8 @@ struct RepState {
   int rebuild, exceed;
   int overflow, nrebuilds;
   int actual_max_nbrs, nlog;
+  int err;               // a bounded device wait gave up (reported to the host)
+  int pad_;
 };
 
 struct EngArgs {
@@ -100,6 +104,8 @@ struct EngArgs {
   double* elog;
   int ntiles;
   int nrep;
+  int idx_pitch;  // k_force: shared-memory row pitch of the staged list tile (pb + bank padding)
+  int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
 };
 
 }  // namespace b2md

@@ -14,6 +14,7 @@
 #pragma once
 #include "engine_dev.cuh"
 #include "pbc_math.cuh"
+#include "tma.cuh"
 
 namespace b2md {
 
@@ -184,72 +185,161 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
 // Pair force (+ fused integration).  FUSED = one MD step: forces from r[rbuf],
 // integrate, write r[rbuf^1].  Otherwise Sample::CalcF only.
 // ---------------------------------------------------------------------------
+// Per-thread force accumulators of one particle.
+struct PairAcc {
+  float fx = 0.f, fy = 0.f, fz = 0.f, uu = 0.f, ww = 0.f;
+  float sxx = 0.f, syy = 0.f, szz = 0.f, syz = 0.f, sxz = 0.f, sxy = 0.f;
+};
+
+// fij + Pot_IPL_12_6::ComputeInteraction (PairPotential.h:161-168, 1198-1244)
+// for one neighbour, without branches so that consecutive pairs interleave.
+// 1/r comes from one MUFU rsqrt refined by one Newton-Raphson step
+// (y <- y (3/2 - x y^2 / 2)); 1/r^2 = y^2.  The cut-off method is folded into
+// the packed pair row: s -= c_s / r and u += c_ur r + c_u0, which is
+// s(rc) rc / r and s(rc) rc (r - rc) - u(rc) for SF, -u(rc) for SP, 0 for NS.
+// WRAP = false skips the minimum-image step; the caller uses it only when it
+// is exactly the identity (see k_force).
+template <bool STRESS, bool WRAP>
+__device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const float4& rj, const float* prow, float Lx,
+                                        float Ly, float Lz, float iLx, float iLy, float iLz) {
+  float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
+  if (WRAP) {
+    dx = mi_comp(dx, Lx, iLx);
+    dy = mi_comp(dy, Ly, iLy);
+    dz = mi_comp(dz, Lz, iLz);
+  }
+  const float d2 = dist2_ref(dx, dy, dz);
+  const float* pp = prow + __float_as_int(rj.w) * kParStride;
+  const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, A12, A6, c_s
+  const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);  // c_u0, c_ur
+  float y = rsqrtf(d2);
+  y = y * __fmaf_rn(-0.5f * d2 * y, y, 1.5f);
+  const float i2 = y * y;
+  const float i6 = i2 * i2 * i2;
+  const float t = q.y * i6;
+  float s = __fmaf_rn(-q.w, y, i6 * i2 * __fmaf_rn(12.f, t, 6.f * q.z));
+  float u = __fmaf_rn(i6, t + q.z, __fmaf_rn(q2.y, d2 * y, q2.x));
+  const bool in = d2 < q.x;
+  s = in ? s : 0.f;
+  u = in ? u : 0.f;
+  A.fx = __fmaf_rn(dx, s, A.fx);
+  A.fy = __fmaf_rn(dy, s, A.fy);
+  A.fz = __fmaf_rn(dz, s, A.fz);
+  A.ww = __fmaf_rn(d2, s, A.ww);
+  A.uu += u;
+  if (STRESS) {
+    A.sxx -= dx * dx * s; A.syy -= dy * dy * s; A.szz -= dz * dz * s;
+    A.syz -= dy * dz * s; A.sxz -= dx * dz * s; A.sxy -= dx * dy * s;
+  }
+}
+
+// The neighbour loop of one thread: entries k = lane_t, lane_t + TP, ... of
+// the staged list column, four gathers in flight.
+template <int TP, bool STRESS, bool WRAP>
+__device__ __forceinline__ void force_loop(PairAcc& A, const unsigned* sc, int pitch, unsigned lane_t, unsigned nn,
+                                           const float4* __restrict__ rc, const float4& ri, const float* prow,
+                                           float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
+  unsigned k = lane_t;
+  for (; k + 3 * TP < nn; k += 4 * TP) {
+    const unsigned j0 = sc[k * pitch], j1 = sc[(k + TP) * pitch];
+    const unsigned j2 = sc[(k + 2 * TP) * pitch], j3 = sc[(k + 3 * TP) * pitch];
+    const float4 r0 = __ldg(rc + j0), r1 = __ldg(rc + j1), r2 = __ldg(rc + j2), r3 = __ldg(rc + j3);
+    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+  }
+  for (; k < nn; k += TP) {
+    const float4 r0 = __ldg(rc + sc[k * pitch]);
+    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+  }
+}
+
+// Shared memory of k_force: [packed pair table, kParSmemFloats] [index tile]
+constexpr int kParSmemFloats = kMaxTypes * kMaxTypes * kParStride;
+constexpr unsigned kWaitPolls = 1u << 22;
+
 template <int TP, bool FUSED, bool STRESS>
 __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cudaGraphConditionalHandle h) {
-  extern __shared__ float s_par[];
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  float* s_par = reinterpret_cast<float*>(s_dyn);
+  unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
   __shared__ double s_scr[kMaxBlock];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ unsigned s_rows;
   const int tile = blockIdx.x;
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   const bool skip = (S->overflow != 0) || (FUSED && S->steps_left <= 0) || !R.active;
   if (!skip) {
+    const int pb = blockDim.x / TP;
+    const int first = a.tile_first[tile];
+    const int pitch = a.idx_pitch;
+    // 1. rows of the list this tile needs: the largest neighbour count in it
+    if (threadIdx.x == 0) {
+      s_rows = 0u;
+      mbar_init(&s_bar, 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+    {
+      unsigned c = (threadIdx.x < pb && first + (int)threadIdx.x < R.n) ? a.nn[R.p0 + first + threadIdx.x] : 0u;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+      if ((threadIdx.x & 31) == 0 && c) atomicMax(&s_rows, c);
+    }
+    __syncthreads();
+    const unsigned rows = min(s_rows, (unsigned)a.idx_rows);
+    // 2. one TMA bulk copy per list row: slots [first, first+width) of rows 0..rows-1
+    if (threadIdx.x < 32) {
+      const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
+      if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, rows * width * 4u);
+      __syncwarp();
+      const unsigned* src = a.nbl + R.nbl0 + first;
+      for (unsigned r = threadIdx.x; r < rows; r += 32)
+        bulk_g2s(s_idx + r * pitch, src + (size_t)r * R.nbl_stride, width * 4u, &s_bar);
+    }
+    // 3. meanwhile: pair table and this particle's data
     const int nt = R.ntypes;
     for (int k = threadIdx.x; k < nt * nt * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
-    __syncthreads();
     const int lp = threadIdx.x / TP, lane_t = threadIdx.x % TP;
-    const int i = a.tile_first[tile] + lp;
+    const int i = first + lp;
     const bool valid = i < R.n;
     const int rb = S->rbuf;
     const float4* __restrict__ rc = a.r[rb] + R.p0;
     const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
-    const int cutoff = R.cutoff;
-    float4 ri = valid ? rc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 ri = valid ? rc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const int ti = valid ? __float_as_int(ri.w) : 0;
     const float* prow = s_par + ti * nt * kParStride;
-    float fx = 0.f, fy = 0.f, fz = 0.f, uu = 0.f, ww = 0.f;
-    float sxx = 0.f, syy = 0.f, szz = 0.f, syz = 0.f, sxz = 0.f, sxy = 0.f;
     const unsigned nn = valid ? a.nn[R.p0 + i] : 0u;
-    const unsigned* __restrict__ col = a.nbl + R.nbl0 + i;
-    const size_t stride = (size_t)R.nbl_stride;
-#pragma unroll 4
-    for (unsigned k = lane_t; k < nn; k += TP) {
-      const unsigned j = __ldg(col + k * stride);
-      const float4 rj = __ldg(rc + j);
-      const float dx = mi_comp(ri.x - rj.x, Lx, iLx);
-      const float dy = mi_comp(ri.y - rj.y, Ly, iLy);
-      const float dz = mi_comp(ri.z - rj.z, Lz, iLz);
-      const float d2 = dist2_ref(dx, dy, dz);
-      const float* pp = prow + __float_as_int(rj.w) * kParStride;
-      const float4 q = *reinterpret_cast<const float4*>(pp);
-      if (d2 < q.x) {
-        const float i2 = __frcp_rn(d2);
-        const float i6 = i2 * i2 * i2;
-        const float t = q.y * i6;
-        float s = i6 * i2 * __fmaf_rn(12.f, t, 6.f * q.z);
-        float u = i6 * (t + q.z);
-        if (cutoff == CUT_SF) {
-          const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);
-          const float ir = rsqrtf(d2);
-          s = __fmaf_rn(-q.w, ir, s);
-          u += __fmaf_rn(q.w, __fmaf_rn(d2, ir, -q2.y), -q2.x);
-        } else if (cutoff == CUT_SP) {
-          u -= pp[4];
-        }
-        fx = __fmaf_rn(dx, s, fx);
-        fy = __fmaf_rn(dy, s, fy);
-        fz = __fmaf_rn(dz, s, fz);
-        ww = __fmaf_rn(d2, s, ww);
-        uu += u;
-        if (STRESS) {
-          sxx -= dx * dx * s; syy -= dy * dy * s; szz -= dz * dz * s;
-          syz -= dy * dz * s; sxz -= dx * dz * s; sxy -= dx * dy * s;
-        }
-      }
+    // A particle farther than rc_max + 2 skin from every face of the box has
+    // all its listed neighbours (within rc + skin at the build, each moved at
+    // most skin/2 since) inside the box at their minimum image, so the
+    // minimum-image correction is exactly zero; warps made only of such
+    // particles skip it.
+    const bool inner = fabsf(ri.x) < R.ilim[0] && fabsf(ri.y) < R.ilim[1] && fabsf(ri.z) < R.ilim[2];
+    const bool fast = __all_sync(0xffffffffu, !valid || inner);
+    // 4. bounded wait for the index tile
+    const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
+    PairAcc A;
+    if (ok) {
+      const unsigned* sc = s_idx + lp;
+      if (fast)
+        force_loop<TP, STRESS, false>(A, sc, pitch, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+      else
+        force_loop<TP, STRESS, true>(A, sc, pitch, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    } else {
+      // the copies did not land in time: record it for the host and wait
+      // (bounded) for them before this block's shared memory is released
+      if (threadIdx.x == 0) atomicExch(&S->err, 1);
+      mbar_wait_bounded(&s_bar, 0, kWaitPolls);
     }
+    float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
+    float sxx = A.sxx, syy = A.syy, szz = A.szz, syz = A.syz, sxz = A.sxz, sxy = A.sxy;
     if (TP > 1) {
 #pragma unroll
       for (int o = TP / 2; o > 0; o >>= 1) {
@@ -604,28 +694,65 @@ __global__ void k_rb_permute(EngArgs a) {
 }
 
 // (7) sorted 5x5x5 cell scan (calculateNBL_CellsSorted, NeighborList.cu:1204-1319):
-//     neighbours in the reference's order (dz, dy, dx, ascending slot)
-__global__ void k_rb_build(EngArgs a) {
-  extern __shared__ float s_cs2[];
+//     neighbours in the reference's order (dz, dy, dx, ascending slot).
+//     LP lanes share one particle: each round they test LP consecutive
+//     candidates and append the accepted ones in candidate order (group
+//     ballot + prefix count), so the list is the reference's entry for entry.
+//     The tile's list is assembled in shared memory, then written row by row
+//     with TMA bulk stores.
+constexpr int kCs2Floats = kMaxTypes * kMaxTypes;
+
+template <int LP>
+__global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  float* s_cs2 = reinterpret_cast<float*>(s_dyn);
+  unsigned* s_list = reinterpret_cast<unsigned*>(s_dyn + kCs2Floats * sizeof(float));
+  __shared__ int s_max;
   const int tile = blockIdx.x, rep = a.tile_rep[tile];
   if (!rb_active(a, rep)) return;
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   const int nt = R.ntypes;
+  const int pb = blockDim.x / LP;
+  const int lpitch = pb + 4;  // rows 16 bytes apart: a group's 8 rows hit 8 different banks
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
+  if (threadIdx.x == 0) s_max = 0;
   __syncthreads();
-  const int i = a.tile_first[tile] + threadIdx.x;
+  const int lp = threadIdx.x / LP, q = threadIdx.x % LP;
+  const int first = a.tile_first[tile];
+  const int i = first + lp;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned gshift = lane & ~(unsigned)(LP - 1);
+  const unsigned gmask = ((1u << LP) - 1u) << gshift;
+  const unsigned below = (1u << (lane - gshift)) - 1u;
   const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
+  const int maxn = R.max_nbrs;
   int count = 0;
   if (i < R.n) {
     const float4 ri = rc[i];
     const int ti = __float_as_int(ri.w);
     const float* cs2 = s_cs2 + ti * nt;
-    unsigned* col = a.nbl + R.nbl0 + i;
-    const size_t stride = (size_t)R.nbl_stride;
-    const int maxn = R.max_nbrs;
     const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+    // appends the accepted candidates of slots [b, e) in slot order
+    auto scan = [&](int b, int e) {
+      for (int base = b; base < e; base += LP) {
+        const int j = base + q;
+        bool in = false;
+        if (j < e) {
+          const float4 rj = __ldg(rc + j);
+          const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
+                                     mi_comp(ri.z - rj.z, Lz, iLz));
+          in = (j != i) && d2 < cs2[__float_as_int(rj.w)];
+        }
+        const unsigned g = (__ballot_sync(gmask, in) >> gshift) & ((1u << LP) - 1u);
+        if (in) {
+          const int pos = count + __popc(g & below);
+          if (pos < maxn) s_list[pos * lpitch + lp] = (unsigned)j;
+        }
+        count += __popc(g);
+      }
+    };
     if (R.nb_method == NB_CELLS) {
       const int ch = cell_chunk(R);
       const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
@@ -635,53 +762,51 @@ __global__ void k_rb_build(EngArgs a) {
         for (int dy = -2; dy <= 2; ++dy) {
           int oy = cy + dy;
           oy += ((oy < 0) - (oy >= ny)) * ny;
-          for (int dx = -2; dx <= 2; ++dx) {
-            int ox = cx + dx;
-            ox += ((ox < 0) - (ox >= nx)) * nx;
-            const int c = ox + oy * nx + oz * nx * ny;
-            const int b = cell_begin(a, R, c, ch), m = a.cnt[R.cell0 + c];
-            for (int j = b; j < b + m; ++j) {
-              if (j == i) continue;
-              const float4 rj = __ldg(rc + j);
-              const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
-                                         mi_comp(ri.z - rj.z, Lz, iLz));
-              if (d2 < cs2[__float_as_int(rj.w)]) {
-                if (count < maxn) col[(size_t)count * stride] = (unsigned)j;
-                ++count;
-              }
-            }
+          // the five cells cx-2..cx+2 of this row are consecutive keys, so
+          // their particles are one slot range (two when the row wraps); the
+          // scan order dx = -2..2, ascending slot, is the reference's
+          const int row = oy * nx + oz * nx * ny;
+          const int lo = cx - 2, hi = cx + 2;
+          if (lo >= 0 && hi < nx) {
+            const int c1 = row + hi;
+            scan(cell_begin(a, R, row + lo, ch), cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1]);
+          } else if (lo < 0) {
+            const int cw = row + nx - 1, c1 = row + hi;
+            scan(cell_begin(a, R, row + nx + lo, ch), cell_begin(a, R, cw, ch) + a.cnt[R.cell0 + cw]);
+            scan(cell_begin(a, R, row, ch), cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1]);
+          } else {
+            const int cw = row + nx - 1, c1 = row + hi - nx;
+            scan(cell_begin(a, R, row + lo, ch), cell_begin(a, R, cw, ch) + a.cnt[R.cell0 + cw]);
+            scan(cell_begin(a, R, row, ch), cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1]);
           }
         }
       }
     } else {
-      // all pairs (calculateNBL_N2 criterion), ascending j
-      for (int j = 0; j < R.n; ++j) {
-        if (j == i) continue;
-        const float4 rj = __ldg(rc + j);
-        const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
-                                   mi_comp(ri.z - rj.z, Lz, iLz));
-        if (d2 < cs2[__float_as_int(rj.w)]) {
-          if (count < maxn) col[(size_t)count * stride] = (unsigned)j;
-          ++count;
-        }
-      }
+      scan(0, R.n);  // all pairs (calculateNBL_N2 criterion), ascending j
     }
-    a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
-    a.last_r[(size_t)R.p0 + i] = ri;
+    if (q == 0) {
+      a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
+      a.last_r[(size_t)R.p0 + i] = ri;
+      atomicMax(&s_max, count);
+    }
   }
-  // block max of count, overflow if any count > capacity
-  int bmax = count;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) bmax = max(bmax, __shfl_xor_sync(0xffffffffu, bmax, o));
-  __shared__ int s_max;
-  if (threadIdx.x == 0) s_max = 0;
+  // write the tile's rows [0, rows) of the list: slots [first, first+width)
+  fence_async_shared();
   __syncthreads();
-  if ((threadIdx.x & 31) == 0) atomicMax(&s_max, bmax);
-  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int rows = min(s_max, maxn);
+    const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
+    unsigned* dst = a.nbl + R.nbl0 + first;
+    for (int r = threadIdx.x; r < rows; r += 32)
+      bulk_s2g(dst + (size_t)r * R.nbl_stride, s_list + r * lpitch, width * 4u);
+    bulk_commit();
+    bulk_wait_all();
+  }
   __shared__ int s_last;
   if (threadIdx.x == 0) {
-    atomicMax(&S->actual_max_nbrs, s_max);
-    if (s_max > R.max_nbrs) atomicExch(&S->overflow, 1);
+    const int s_max_v = s_max;
+    atomicMax(&S->actual_max_nbrs, s_max_v);
+    if (s_max_v > R.max_nbrs) atomicExch(&S->overflow, 1);
     __threadfence();
     unsigned c = atomicAdd(&a.rctr[rep], 1u);
     s_last = (c == (unsigned)(R.ntiles - 1));
