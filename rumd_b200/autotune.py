@@ -76,6 +76,22 @@ class Autotune:
         return cache[key]
 
 
+def equilibrated_ka(capi, n, T, device=0, seed=1, melt_steps=1000, eq_steps=1000):
+    """A KA liquid at temperature T: FCC start melted at T=2, then brought to T."""
+    from . import initconf
+    c = initconf.ka_config(n, T=2.0, seed=seed)
+    params = initconf.lj_params(2, initconf.KA)
+    e = capi.Engine(device=device)
+    rid = e.add(c["pos4"], c["box"], params, 2, cutoff="SF", T=2.0, vel4=c["vel4"])
+    e.run(melt_steps)
+    e.set_integrator(rid, 0.005, T, 0.2)
+    e.run(eq_steps)
+    rep = dict(pos4=e.get(rid, "pos", n), vel4=e.get(rid, "vel", n), box=c["box"], params=params, ntypes=2, T=T,
+               n=n, density=1.2)
+    e.close()
+    return rep
+
+
 def device_measure(capi, replicas, device=0, steps=300, warmup=100):
     """measure() for `search`: builds an engine with all replicas at the given
     shape and skin and times `steps` device steps with CUDA events.
@@ -103,3 +119,31 @@ def device_measure(capi, replicas, device=0, steps=300, warmup=100):
         return n * steps / dt, pe
 
     return measure
+
+
+def main(argv=None):
+    """python -m rumd_b200.autotune --n 65536 --T 0.45 [--pbs 32,64 --tps 2,4 --skins 0.3]"""
+    import argparse
+    from . import capi
+    p = argparse.ArgumentParser()
+    p.add_argument("--n", type=int, default=65536)
+    p.add_argument("--T", type=float, default=0.45)
+    p.add_argument("--pbs", default="32,64,128")
+    p.add_argument("--tps", default="1,2,4,8")
+    p.add_argument("--skins", default="0.3")
+    p.add_argument("--steps", type=int, default=1000)
+    p.add_argument("--cache", default="autotune.json")
+    args = p.parse_args(argv)
+    reps = [equilibrated_ka(capi, args.n, args.T)]
+    at = Autotune(cache_path=args.cache, pbs=tuple(int(x) for x in args.pbs.split(",")),
+                  tps=tuple(int(x) for x in args.tps.split(",")),
+                  skins=tuple(float(x) for x in args.skins.split(",")))
+    best = at.tune(reps, device_measure(capi, reps, steps=args.steps, warmup=200), force=True)
+    for r in best["table"]:
+        print(f"pb={r['pb']:4d} tp={r['tp']} skin={r['skin']:.2f}  {r['rate']:.4e} particle-steps/s  "
+              f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
+    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate")}))
+
+
+if __name__ == "__main__":
+    main()

@@ -492,10 +492,7 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   const size_t smem = (size_t)kCs2Floats * sizeof(float) + (size_t)a.idx_rows * (e->pb + 4) * sizeof(unsigned);
   if (smem > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
-  const int lp = std::min(8, kMaxBlock / e->pb);
-  void (*fb)(EngArgs) = lp >= 8 ? k_rb_build<8> : lp >= 4 ? k_rb_build<4> : lp >= 2 ? k_rb_build<2> : k_rb_build<1>;
-  const int lanes = lp >= 8 ? 8 : lp >= 4 ? 4 : lp >= 2 ? 2 : 1;
-  fb<<<T, e->pb * lanes, smem, s>>>(a);
+  k_rb_build<<<T, e->pb, smem, s>>>(a);
 }
 
 typedef void (*ForceFn)(EngArgs, int, cudaGraphConditionalHandle);
@@ -526,9 +523,7 @@ void init_func_attrs(int device) {
   static unsigned long long done_mask = 0ull;  // one bit per device
   const unsigned long long bit = 1ull << (device & 63);
   if (done_mask & bit) return;
-  const void* fns[] = {(const void*)k_rb_build<1>, (const void*)k_rb_build<2>, (const void*)k_rb_build<4>,
-                       (const void*)k_rb_build<8>};
-  for (const void* f : fns) CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
+  CK(cudaFuncSetAttribute((const void*)k_rb_build, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
   for (int tp : {1, 2, 4, 8})
     for (int v = 0; v < 3; ++v)
       CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2),

@@ -240,14 +240,33 @@ __device__ __forceinline__ void force_loop(PairAcc& A, const unsigned* sc, int p
                                            const float4* __restrict__ rc, const float4& ri, const float* prow,
                                            float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
   unsigned k = lane_t;
-  for (; k + 3 * TP < nn; k += 4 * TP) {
-    const unsigned j0 = sc[k * pitch], j1 = sc[(k + TP) * pitch];
-    const unsigned j2 = sc[(k + 2 * TP) * pitch], j3 = sc[(k + 3 * TP) * pitch];
-    const float4 r0 = __ldg(rc + j0), r1 = __ldg(rc + j1), r2 = __ldg(rc + j2), r3 = __ldg(rc + j3);
-    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+  // software pipeline: the gathers of the next batch of four are in flight
+  // while the current batch is computed
+  bool have = k + 3 * TP < nn;
+  float4 c0, c1, c2, c3;
+  if (have) {
+    c0 = __ldg(rc + sc[k * pitch]);
+    c1 = __ldg(rc + sc[(k + TP) * pitch]);
+    c2 = __ldg(rc + sc[(k + 2 * TP) * pitch]);
+    c3 = __ldg(rc + sc[(k + 3 * TP) * pitch]);
+  }
+  while (have) {
+    const unsigned kn = k + 4 * TP;
+    const bool next = kn + 3 * TP < nn;
+    float4 n0, n1, n2, n3;
+    if (next) {
+      n0 = __ldg(rc + sc[kn * pitch]);
+      n1 = __ldg(rc + sc[(kn + TP) * pitch]);
+      n2 = __ldg(rc + sc[(kn + 2 * TP) * pitch]);
+      n3 = __ldg(rc + sc[(kn + 3 * TP) * pitch]);
+    }
+    lj_pair<STRESS, WRAP>(A, ri, c0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, c1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, c2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, c3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+    k = kn;
+    have = next;
   }
   for (; k < nn; k += TP) {
     const float4 r0 = __ldg(rc + sc[k * pitch]);
@@ -695,14 +714,12 @@ __global__ void k_rb_permute(EngArgs a) {
 
 // (7) sorted 5x5x5 cell scan (calculateNBL_CellsSorted, NeighborList.cu:1204-1319):
 //     neighbours in the reference's order (dz, dy, dx, ascending slot).
-//     LP lanes share one particle: each round they test LP consecutive
-//     candidates and append the accepted ones in candidate order (group
-//     ballot + prefix count), so the list is the reference's entry for entry.
-//     The tile's list is assembled in shared memory, then written row by row
-//     with TMA bulk stores.
+//     One thread per particle walks the 25 (dz, dy) rows as contiguous slot
+//     ranges with eight gathers in flight.  The tile's list is assembled in
+//     shared memory, then written row by row with TMA bulk stores (the
+//     column-major rows are contiguous slot runs, so each row is one copy).
 constexpr int kCs2Floats = kMaxTypes * kMaxTypes;
 
-template <int LP>
 __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   float* s_cs2 = reinterpret_cast<float*>(s_dyn);
@@ -713,18 +730,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   const int nt = R.ntypes;
-  const int pb = blockDim.x / LP;
-  const int lpitch = pb + 4;  // rows 16 bytes apart: a group's 8 rows hit 8 different banks
+  const int pb = blockDim.x;
+  const int lpitch = pb + 4;
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
   if (threadIdx.x == 0) s_max = 0;
   __syncthreads();
-  const int lp = threadIdx.x / LP, q = threadIdx.x % LP;
+  const int lp = threadIdx.x;
   const int first = a.tile_first[tile];
   const int i = first + lp;
-  const unsigned lane = threadIdx.x & 31u;
-  const unsigned gshift = lane & ~(unsigned)(LP - 1);
-  const unsigned gmask = ((1u << LP) - 1u) << gshift;
-  const unsigned below = (1u << (lane - gshift)) - 1u;
   const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
   const int maxn = R.max_nbrs;
   int count = 0;
@@ -734,24 +747,25 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
     const float* cs2 = s_cs2 + ti * nt;
     const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+    auto test = [&](const float4& rj, int j) {
+      const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
+                                 mi_comp(ri.z - rj.z, Lz, iLz));
+      if (j != i && d2 < cs2[__float_as_int(rj.w)]) {
+        if (count < maxn) s_list[count * lpitch + lp] = (unsigned)j;
+        ++count;
+      }
+    };
     // appends the accepted candidates of slots [b, e) in slot order
     auto scan = [&](int b, int e) {
-      for (int base = b; base < e; base += LP) {
-        const int j = base + q;
-        bool in = false;
-        if (j < e) {
-          const float4 rj = __ldg(rc + j);
-          const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
-                                     mi_comp(ri.z - rj.z, Lz, iLz));
-          in = (j != i) && d2 < cs2[__float_as_int(rj.w)];
-        }
-        const unsigned g = (__ballot_sync(gmask, in) >> gshift) & ((1u << LP) - 1u);
-        if (in) {
-          const int pos = count + __popc(g & below);
-          if (pos < maxn) s_list[pos * lpitch + lp] = (unsigned)j;
-        }
-        count += __popc(g);
+      int j = b;
+      for (; j + 7 < e; j += 8) {
+        float4 rr[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) rr[u] = __ldg(rc + j + u);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) test(rr[u], j + u);
       }
+      for (; j < e; ++j) test(__ldg(rc + j), j);
     };
     if (R.nb_method == NB_CELLS) {
       const int ch = cell_chunk(R);
@@ -784,11 +798,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
     } else {
       scan(0, R.n);  // all pairs (calculateNBL_N2 criterion), ascending j
     }
-    if (q == 0) {
-      a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
-      a.last_r[(size_t)R.p0 + i] = ri;
-      atomicMax(&s_max, count);
-    }
+    a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
+    a.last_r[(size_t)R.p0 + i] = ri;
+    atomicMax(&s_max, count);
   }
   // write the tile's rows [0, rows) of the list: slots [first, first+width)
   fence_async_shared();
