@@ -492,7 +492,12 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   const size_t smem = (size_t)kCs2Floats * sizeof(float) + (size_t)a.idx_rows * (e->pb + 4) * sizeof(unsigned);
   if (smem > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
-  k_rb_build<<<T, e->pb, smem, s>>>(a);
+  // lanes per particle: 8, or fewer for tiles so large that pb*8 > 512
+  const int lanes = std::min(8, kMaxBlock / e->pb);
+  if (lanes >= 8) k_rb_build<8><<<T, e->pb * 8, smem, s>>>(a);
+  else if (lanes >= 4) k_rb_build<4><<<T, e->pb * 4, smem, s>>>(a);
+  else if (lanes >= 2) k_rb_build<2><<<T, e->pb * 2, smem, s>>>(a);
+  else k_rb_build<1><<<T, e->pb, smem, s>>>(a);
 }
 
 typedef void (*ForceFn)(EngArgs, int, cudaGraphConditionalHandle);
@@ -523,7 +528,10 @@ void init_func_attrs(int device) {
   static unsigned long long done_mask = 0ull;  // one bit per device
   const unsigned long long bit = 1ull << (device & 63);
   if (done_mask & bit) return;
-  CK(cudaFuncSetAttribute((const void*)k_rb_build, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
+  const void* builds[] = {(const void*)k_rb_build<1>, (const void*)k_rb_build<2>, (const void*)k_rb_build<4>,
+                          (const void*)k_rb_build<8>};
+  for (const void* f : builds)
+    CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
   for (int tp : {1, 2, 4, 8})
     for (int v = 0; v < 3; ++v)
       CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2),

@@ -240,33 +240,14 @@ __device__ __forceinline__ void force_loop(PairAcc& A, const unsigned* sc, int p
                                            const float4* __restrict__ rc, const float4& ri, const float* prow,
                                            float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
   unsigned k = lane_t;
-  // software pipeline: the gathers of the next batch of four are in flight
-  // while the current batch is computed
-  bool have = k + 3 * TP < nn;
-  float4 c0, c1, c2, c3;
-  if (have) {
-    c0 = __ldg(rc + sc[k * pitch]);
-    c1 = __ldg(rc + sc[(k + TP) * pitch]);
-    c2 = __ldg(rc + sc[(k + 2 * TP) * pitch]);
-    c3 = __ldg(rc + sc[(k + 3 * TP) * pitch]);
-  }
-  while (have) {
-    const unsigned kn = k + 4 * TP;
-    const bool next = kn + 3 * TP < nn;
-    float4 n0, n1, n2, n3;
-    if (next) {
-      n0 = __ldg(rc + sc[kn * pitch]);
-      n1 = __ldg(rc + sc[(kn + TP) * pitch]);
-      n2 = __ldg(rc + sc[(kn + 2 * TP) * pitch]);
-      n3 = __ldg(rc + sc[(kn + 3 * TP) * pitch]);
-    }
-    lj_pair<STRESS, WRAP>(A, ri, c0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, c1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, c2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, c3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    c0 = n0; c1 = n1; c2 = n2; c3 = n3;
-    k = kn;
-    have = next;
+  for (; k + 3 * TP < nn; k += 4 * TP) {
+    const unsigned j0 = sc[k * pitch], j1 = sc[(k + TP) * pitch];
+    const unsigned j2 = sc[(k + 2 * TP) * pitch], j3 = sc[(k + 3 * TP) * pitch];
+    const float4 r0 = __ldg(rc + j0), r1 = __ldg(rc + j1), r2 = __ldg(rc + j2), r3 = __ldg(rc + j3);
+    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
   for (; k < nn; k += TP) {
     const float4 r0 = __ldg(rc + sc[k * pitch]);
@@ -714,12 +695,17 @@ __global__ void k_rb_permute(EngArgs a) {
 
 // (7) sorted 5x5x5 cell scan (calculateNBL_CellsSorted, NeighborList.cu:1204-1319):
 //     neighbours in the reference's order (dz, dy, dx, ascending slot).
-//     One thread per particle walks the 25 (dz, dy) rows as contiguous slot
-//     ranges with eight gathers in flight.  The tile's list is assembled in
-//     shared memory, then written row by row with TMA bulk stores (the
-//     column-major rows are contiguous slot runs, so each row is one copy).
+//     LP lanes share one particle.  Its 25 (dz, dy) rows are contiguous slot
+//     ranges (two when a row wraps); each round the LP lanes test LP
+//     consecutive candidates and append the accepted ones in candidate order
+//     (ballot + prefix count), so the list is the reference's entry for entry.
+//     All groups of a warp run the same number of rounds per range (the warp
+//     maximum), so the warp never diverges.  The tile's list is assembled in
+//     shared memory and written row by row with TMA bulk stores (a
+//     column-major row of the tile is one contiguous slot run).
 constexpr int kCs2Floats = kMaxTypes * kMaxTypes;
 
+template <int LP>
 __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   float* s_cs2 = reinterpret_cast<float*>(s_dyn);
@@ -730,74 +716,97 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   const int nt = R.ntypes;
-  const int pb = blockDim.x;
-  const int lpitch = pb + 4;
+  const int pb = blockDim.x / LP;
+  const int lpitch = pb + 4;  // rows 16 bytes apart: a group's LP rows fall in different banks
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
   if (threadIdx.x == 0) s_max = 0;
   __syncthreads();
-  const int lp = threadIdx.x;
+  const int lp = threadIdx.x / LP, q = threadIdx.x % LP;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned gshift = lane & ~(unsigned)(LP - 1);
+  const unsigned gbits = LP == 32 ? 0xffffffffu : ((1u << LP) - 1u);
+  const unsigned below = (1u << (lane - gshift)) - 1u;
   const int first = a.tile_first[tile];
   const int i = first + lp;
+  const bool valid = i < R.n;
   const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
   const int maxn = R.max_nbrs;
+  const float4 ri = valid ? rc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float* cs2 = s_cs2 + (valid ? __float_as_int(ri.w) : 0) * nt;
+  const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
+  const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
   int count = 0;
-  if (i < R.n) {
-    const float4 ri = rc[i];
-    const int ti = __float_as_int(ri.w);
-    const float* cs2 = s_cs2 + ti * nt;
-    const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
-    const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
-    auto test = [&](const float4& rj, int j) {
-      const float d2 = dist2_ref(mi_comp(ri.x - rj.x, Lx, iLx), mi_comp(ri.y - rj.y, Ly, iLy),
-                                 mi_comp(ri.z - rj.z, Lz, iLz));
-      if (j != i && d2 < cs2[__float_as_int(rj.w)]) {
-        if (count < maxn) s_list[count * lpitch + lp] = (unsigned)j;
-        ++count;
+  // appends the accepted candidates of slots [b, e); every lane of the warp
+  // calls it (invalid groups with an empty range)
+  auto seg = [&](int b, int e, bool wrap) {
+    int rounds = e > b ? (e - b + LP - 1) / LP : 0;
+    rounds = __reduce_max_sync(0xffffffffu, rounds);
+    for (int r = 0; r < rounds; ++r) {
+      const int j = b + r * LP + q;
+      bool in = false;
+      if (j < e) {
+        const float4 rj = __ldg(rc + j);
+        float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
+        if (wrap) {
+          dx = mi_comp(dx, Lx, iLx);
+          dy = mi_comp(dy, Ly, iLy);
+          dz = mi_comp(dz, Lz, iLz);
+        }
+        in = (j != i) && dist2_ref(dx, dy, dz) < cs2[__float_as_int(rj.w)];
       }
-    };
-    // appends the accepted candidates of slots [b, e) in slot order
-    auto scan = [&](int b, int e) {
-      int j = b;
-      for (; j + 7 < e; j += 8) {
-        float4 rr[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) rr[u] = __ldg(rc + j + u);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) test(rr[u], j + u);
+      const unsigned g = (__ballot_sync(0xffffffffu, in) >> gshift) & gbits;
+      if (in) {
+        const int pos = count + __popc(g & below);
+        if (pos < maxn) s_list[pos * lpitch + lp] = (unsigned)j;
       }
-      for (; j < e; ++j) test(__ldg(rc + j), j);
-    };
-    if (R.nb_method == NB_CELLS) {
-      const int ch = cell_chunk(R);
-      const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
-      const int cx = cell_coord(ri.x, iLx, nx), cy = cell_coord(ri.y, iLy, ny), cz = cell_coord(ri.z, iLz, nz);
-      for (int dz = -2; dz <= 2; ++dz) {
-        const int oz = (cz + dz + nz) % nz;
-        for (int dy = -2; dy <= 2; ++dy) {
-          int oy = cy + dy;
-          oy += ((oy < 0) - (oy >= ny)) * ny;
-          // the five cells cx-2..cx+2 of this row are consecutive keys, so
-          // their particles are one slot range (two when the row wraps); the
-          // scan order dx = -2..2, ascending slot, is the reference's
-          const int row = oy * nx + oz * nx * ny;
-          const int lo = cx - 2, hi = cx + 2;
+      count += __popc(g);
+    }
+  };
+  if (R.nb_method == NB_CELLS) {
+    const int ch = cell_chunk(R);
+    const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
+    const int cx = cell_coord(ri.x, iLx, nx), cy = cell_coord(ri.y, iLy, ny), cz = cell_coord(ri.z, iLz, nz);
+    // With at least 7 cells per side and no wrapped cell among the 5x5x5,
+    // every candidate is within 3/7 of a box length of the particle, so the
+    // minimum-image step is exactly the identity; warps made only of such
+    // particles skip it.
+    const bool inner = nx >= 7 && ny >= 7 && nz >= 7 && cx >= 2 && cx < nx - 2 && cy >= 2 && cy < ny - 2 &&
+                       cz >= 2 && cz < nz - 2;
+    const bool wrap = !__all_sync(0xffffffffu, !valid || inner);
+    for (int dz = -2; dz <= 2; ++dz) {
+      const int oz = (cz + dz + nz) % nz;
+      for (int dy = -2; dy <= 2; ++dy) {
+        int oy = cy + dy;
+        oy += ((oy < 0) - (oy >= ny)) * ny;
+        // the five cells cx-2..cx+2 of this row are consecutive keys, so
+        // their particles are one slot range (two when the row wraps); the
+        // scan order dx = -2..2, ascending slot, is the reference's
+        const int row = oy * nx + oz * nx * ny;
+        const int lo = cx - 2, hi = cx + 2;
+        int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
+        if (valid) {
           if (lo >= 0 && hi < nx) {
             const int c1 = row + hi;
-            scan(cell_begin(a, R, row + lo, ch), cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1]);
-          } else if (lo < 0) {
-            const int cw = row + nx - 1, c1 = row + hi;
-            scan(cell_begin(a, R, row + nx + lo, ch), cell_begin(a, R, cw, ch) + a.cnt[R.cell0 + cw]);
-            scan(cell_begin(a, R, row, ch), cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1]);
+            b0 = cell_begin(a, R, row + lo, ch);
+            e0 = cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1];
           } else {
-            const int cw = row + nx - 1, c1 = row + hi - nx;
-            scan(cell_begin(a, R, row + lo, ch), cell_begin(a, R, cw, ch) + a.cnt[R.cell0 + cw]);
-            scan(cell_begin(a, R, row, ch), cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1]);
+            const int cw = row + nx - 1;
+            const int ca = lo < 0 ? row + nx + lo : row + lo;  // first cell of the wrapped part order
+            const int cb = lo < 0 ? row + hi : row + hi - nx;
+            b0 = cell_begin(a, R, ca, ch);
+            e0 = cell_begin(a, R, cw, ch) + a.cnt[R.cell0 + cw];
+            b1 = cell_begin(a, R, row, ch);
+            e1 = cell_begin(a, R, cb, ch) + a.cnt[R.cell0 + cb];
           }
         }
+        seg(b0, e0, wrap);
+        seg(b1, e1, wrap);
       }
-    } else {
-      scan(0, R.n);  // all pairs (calculateNBL_N2 criterion), ascending j
     }
+  } else {
+    seg(0, valid ? R.n : 0, true);  // all pairs (calculateNBL_N2 criterion), ascending j
+  }
+  if (valid && q == 0) {
     a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
     a.last_r[(size_t)R.p0 + i] = ri;
     atomicMax(&s_max, count);
