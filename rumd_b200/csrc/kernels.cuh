@@ -6,8 +6,9 @@
 //     (SimulationBox.h:111-125, NeighborList.cu:1106-1140, 1282-1285) with the
 //     multiply-add contractions that nvcc applies to it written out as
 //     __fmaf_rn, so list sets and the sort permutation are bit-exact.
-//   * Pair forces are FP32 (PairPotential.h:161-168, 1198-1244); 1/d^2 is a
-//     correctly rounded reciprocal, the shifted-force 1/r term uses rsqrtf.
+//   * Pair forces are FP32 (PairPotential.h:161-168, 1198-1244); 1/r is the
+//     hardware reciprocal square root refined by one Newton-Raphson step and
+//     1/r^2 its square.
 //   * Reductions (pe, virial, kinetic energy, momentum) are FP64 with a fixed
 //     summation tree, so results do not depend on scheduling or on which other
 //     replicas share the launch; the thermostat state is FP64.
@@ -212,7 +213,7 @@ __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const floa
   const float* pp = prow + __float_as_int(rj.w) * kParStride;
   const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, A12, A6, c_s
   const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);  // c_u0, c_ur
-  float y = rsqrtf(d2);
+  float y = rsqrt_approx(d2);
   y = y * __fmaf_rn(-0.5f * d2 * y, y, 1.5f);
   const float i2 = y * y;
   const float i6 = i2 * i2 * i2;

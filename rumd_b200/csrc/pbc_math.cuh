@@ -9,14 +9,33 @@
 
 namespace b2md {
 
+// Round to nearest, ties to even, for |x| < 2^22: adding and subtracting
+// 1.5 * 2^23 rounds x to an integer in the IEEE addition itself (the sum's
+// unit in the last place is 1), so the result equals rintf(x) bit for bit.
+// Two adds on the FMA pipe instead of a round instruction on the slower
+// conversion pipe.  __fadd_rn keeps the compiler from contracting or folding.
+__device__ __forceinline__ float rint_small(float x) {
+  const float M = 12582912.0f;  // 1.5 * 2^23
+  return __fsub_rn(__fadd_rn(x, M), M);
+}
+
 __device__ __forceinline__ float mi_comp(float d, float L, float invL) {
-  // dr -= L * rintf(dr * invL)   (SimulationBox.h:117-122)
-  return __fmaf_rn(-L, rintf(__fmul_rn(d, invL)), d);
+  // dr -= L * rintf(dr * invL)   (SimulationBox.h:117-122); |dr * invL| < 1
+  return __fmaf_rn(-L, rint_small(__fmul_rn(d, invL)), d);
 }
 
 __device__ __forceinline__ float dist2_ref(float dx, float dy, float dz) {
   // dx*dx + dy*dy + dz*dz as contracted by nvcc (SimulationBox.h:124)
   return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
+}
+
+// Hardware approximate 1/sqrt(x) (one MUFU operation, denormals flushed);
+// callers refine it with a Newton-Raphson step.  Arguments here are squared
+// distances, far from the denormal range.
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 }
 
 __device__ __forceinline__ int cell_coord(float x, float invL, int nc) {
