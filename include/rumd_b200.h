@@ -204,6 +204,27 @@ B2MD_API int b2md_probe_dist2(const float* a4, const float* b4, const float* box
  * out 2*n ints (reference expression, explicit form). */
 B2MD_API int b2md_probe_cell(const float* x, int n, float box, int nc, int* out);
 
+/* LJ forces, per-particle energies, total potential energy and virial of one
+ * configuration, for callers that cannot allocate device memory during the
+ * call: for example a host program that owns every device buffer and lends
+ * this library only pointers, or a real-time loop that must not call
+ * cudaMalloc/cudaFree (they may synchronise the device and take unbounded
+ * time).  No counterpart in the reference; it allocates nothing.
+ *   pos4    DEVICE pointer, n*4 floats (x, y, z, type bits), caller-owned
+ *   box     host, 3 floats;  params host, ntypes*ntypes*12 floats (RUMD layout)
+ *   force4  DEVICE pointer, n*4 floats out (fx, fy, fz, u_i)
+ *   sums    DEVICE pointer, 2 doubles out (sum u_i, virial W)
+ *   stream  cudaStream_t to run on (NULL = default stream); returns at launch
+ * All pairs within the cut-off are summed (no neighbour list).  n is at most
+ * 65536: the only scratch is a fixed array of that capacity in the library's
+ * device image, one per GPU, kept until the process exits and shared by every
+ * call, so calls that overlap on the GPU race; order them on one stream.  The
+ * first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. */
+B2MD_API int b2md_forces_noalloc(const float* pos4, int n, const float* box, int ntypes, const float* params,
+                                 int cutoff_method, float* force4, double* sums, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

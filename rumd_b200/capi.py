@@ -31,6 +31,7 @@ EXPORTS = [
     "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
     "b2md_run_queued", "b2md_nbl_export", "b2md_sort_export", "b2md_cell_grid", "b2md_sync",
     "b2md_stream", "b2md_last_error", "b2md_version", "b2md_probe_dist2", "b2md_probe_cell",
+    "b2md_forces_noalloc",
 ]
 
 
@@ -90,6 +91,7 @@ def lib():
             "b2md_sync": [P],
             "b2md_probe_dist2": [P, P, P, i, P],
             "b2md_probe_cell": [P, i, f, i, P],
+            "b2md_forces_noalloc": [P, i, P, i, P, i, P, P, P],
         }
         for name, args in sig.items():
             fn = getattr(L, name)

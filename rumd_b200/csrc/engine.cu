@@ -712,6 +712,12 @@ void launch_momentum(b2md_engine* e) {
 
 }  // namespace
 
+// Lets other translation units of the library report a message through
+// b2md_last_error (not exported).
+namespace b2md_internal {
+void set_last_error(const char* msg) { g_err = msg; }
+}  // namespace b2md_internal
+
 // ============================================================================
 // C ABI
 // ============================================================================
