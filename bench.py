@@ -44,7 +44,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--pb", type=int, default=64)
-    p.add_argument("--tp", type=int, default=4)
+    p.add_argument("--tp", type=int, default=2)
     p.add_argument("--batch-steps", type=int, default=2000)
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -361,9 +361,16 @@ def main():
         e.run_timed(600)
         e.set_integrator(rid, DT, T_PLAIN, TAU)
         e.run_timed(400)
-        ms, _ = e.run_timed(max(args.steps, 1))
+        # the profiled segment: ncu --profile-from-start off sees only these launches
+        import torch
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.start()
+        r0 = e.stats(rid)["rebuilds"]
+        ms, nl = e.run_timed(max(args.steps, 1))
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.stop()
         print(json.dumps({"profile_steps": args.steps, "step_kernel_ms_avg": ms / max(args.steps, 1),
-                          "rebuilds": e.stats(rid)["rebuilds"]}), flush=True)
+                          "rebuilds": e.stats(rid)["rebuilds"] - r0, "launches": nl}), flush=True)
         e.close()
         dist.close()
         return

@@ -116,6 +116,20 @@ B2MD_API int b2md_engine_memory(b2md_engine* e, long long* bytes);
 /* Chooses CUDA-graph conditional rebuild nodes (1, default) or unconditional
  * early-exit rebuild kernels (0) for b2md_run. */
 B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
+/* Kernel variants, picked by the autotuner next to pb and tp (the analogue of
+ * the kernel plan that Autotune.py tunes).  Every variant gives the same
+ * neighbour lists and forces bit for bit.
+ *   B2MD_VARIANT_FORCE_STAGED  1: the force kernel copies its tile's list rows
+ *                              to shared memory (TMA bulk copies) first;
+ *                              0: it streams them from global memory.
+ *   B2MD_VARIANT_BUILD_LANES   lanes per particle in the list build: 1,2,4,8.
+ *   B2MD_VARIANT_BUILD_SMEM    1: the list build assembles a tile's list in
+ *                              shared memory and writes it with bulk stores;
+ *                              0: it stores entries straight to the list.
+ * No reference counterpart beyond Sample::SetPB_TP (Sample.h:96). */
+enum { B2MD_VARIANT_FORCE_STAGED = 0, B2MD_VARIANT_BUILD_LANES = 1, B2MD_VARIANT_BUILD_SMEM = 2 };
+B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
+B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);
 
 /* Admission of one system (Sample::ReadConf + SetPotential + SetIntegrator,
  * Simulation.py:29-31,157-214).  vel4/im3 may be NULL (zero). */
@@ -170,8 +184,11 @@ B2MD_API int b2md_zero_momentum(b2md_engine* e);
  * doubled, NeighborList.cu:657-676) and the run resumed. */
 B2MD_API int b2md_run(b2md_engine* e, long long nsteps);
 /* b2md_run with eager launches instead of graphs, for measurement: CUDA
- * events on the engine's stream bracket every fused step kernel.  Returns the
- * summed step-kernel time and the number of kernel launches in the run. */
+ * events on the engine's stream bracket every fused step kernel, and the host
+ * reads the rebuild decision before each step (one small kernel and a 4-byte
+ * copy), launching the rebuild kernels only when a list is due, as the step
+ * graph's conditional node does.  Returns the summed step-kernel time and the
+ * number of kernel launches in the run. */
 B2MD_API int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms,
                             long long* launches);
 /* Batched/served form: each replica advances its own queued step count
@@ -224,6 +241,34 @@ B2MD_API int b2md_probe_cell(const float* x, int n, float box, int nc, int* out)
  * before any stream capture. */
 B2MD_API int b2md_forces_noalloc(const float* pos4, int n, const float* box, int ntypes, const float* params,
                                  int cutoff_method, float* force4, double* sums, void* stream);
+
+/* ---- FP64 engine: the accuracy oracle on the GPU ----
+ * The same step (neighbour list, LJ pair forces, Nose-Hoover leap-frog,
+ * energy/virial/kinetic sums) in double precision throughout: what RUMD
+ * becomes after changeToDouble.sh (changeToDouble.sh:1-189).  One system per
+ * engine, particles in the caller's order.  Pair constants: rc, A12, A6 from
+ * the RUMD table (params[k*12 + 0..2]); s(rc) rc and u(rc) recomputed in FP64.
+ *   pos4: x, y, z, type (as a whole number);  vel4: vx, vy, vz, 1/m;  im3 may
+ *   be NULL.  max_nbrs 0 = 1.6 x the ideal-gas estimate + 32.
+ *   b2md_f64_run: energies (NULL or nsteps*4 doubles) = pe, W, KE(t), xi per
+ *   step, as Simulation.Run's energies file rows.
+ *   b2md_f64_stats: out[7] = pe, W, KE(t), KE2, xi, rebuilds, steps. */
+typedef struct b2md_f64 b2md_f64;
+#define B2MD_F64_POS 0    /* double4 per particle */
+#define B2MD_F64_VEL 1    /* double4 per particle */
+#define B2MD_F64_FORCE 2  /* double4: fx, fy, fz, u_i */
+#define B2MD_F64_IMAGES 3 /* 3 ints per particle */
+B2MD_API int b2md_f64_create(int device, int n, int ntypes, const double* box3, const float* params,
+                             int cutoff_method, double skin, int max_nbrs, b2md_f64** out);
+B2MD_API int b2md_f64_destroy(b2md_f64* h);
+B2MD_API int b2md_f64_set_state(b2md_f64* h, const double* pos4, const double* vel4, const int* im3);
+B2MD_API int b2md_f64_set_integrator(b2md_f64* h, double dt, double target_T, double tau, int thermostat_on,
+                                     int reset_interval);
+B2MD_API int b2md_f64_set_xi(b2md_f64* h, double xi);
+B2MD_API int b2md_f64_calc_f(b2md_f64* h);
+B2MD_API int b2md_f64_run(b2md_f64* h, long long nsteps, double* energies);
+B2MD_API int b2md_f64_get(b2md_f64* h, int field, void* out);
+B2MD_API int b2md_f64_stats(b2md_f64* h, double* out);
 
 #ifdef __cplusplus
 }

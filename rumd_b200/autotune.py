@@ -7,6 +7,9 @@ knobs are the engine's:
   pb   particles per block (tile size): 32, 64, 128
   tp   threads per particle: 1, 2, 4, 8   (pb*tp <= 512)
   skin neighbour-list skin, i.e. the rebuild cadence: 0.2 .. 0.5
+and, in a second stage at the winning shape, the kernel variants
+  force_staged  list tile staged in shared memory (1) or streamed (0)
+  build_lanes   lanes per particle in the list build: 1, 2, 4, 8
 Each candidate is timed on the device (CUDA events around a short run of the
 real workload, after a warm-up run).  As in RUMD's test mode
 (Autotune.py:929-937), every candidate's potential energy after its run must
@@ -21,6 +24,7 @@ import os
 DEFAULT_PB = (32, 64, 128)
 DEFAULT_TP = (1, 2, 4, 8)
 DEFAULT_SKIN = (0.2, 0.3, 0.4, 0.5)
+VARIANTS = tuple(itertools.product((0, 1), (1, 2, 4, 8)))  # (force_staged, build_lanes)
 
 
 def candidates(pbs=DEFAULT_PB, tps=DEFAULT_TP, skins=DEFAULT_SKIN, max_block=512):
@@ -46,6 +50,34 @@ def search(cands, measure, pe_tol=0.005):
     return best, table
 
 
+def search_variants(shape, measure, variants=VARIANTS, pe_tol=0.005):
+    """Second stage: the kernel variants at a fixed (pb, tp, skin).
+    measure(pb, tp, skin, force_staged=, build_lanes=) -> (rate, pe)."""
+    table = []
+    ref_pe = None
+    best = None
+    for fs, bl in variants:
+        rate, pe = measure(shape["pb"], shape["tp"], shape["skin"], force_staged=fs, build_lanes=bl)
+        ok = True
+        if ref_pe is None:
+            ref_pe = pe
+        elif abs(pe - ref_pe) > pe_tol:
+            ok = False
+        table.append({"force_staged": fs, "build_lanes": bl, "rate": rate, "pe": pe, "ok": ok})
+        if ok and (best is None or rate > best["rate"]):
+            best = table[-1]
+    return best, table
+
+
+def apply(engine, entry):
+    """Sets a tuned entry's launch shape and kernel variants on an engine."""
+    from . import capi
+    engine.set_launch(entry["pb"], entry["tp"])
+    if "force_staged" in entry:
+        engine.set_variant(capi.VARIANT_FORCE_STAGED, entry["force_staged"])
+        engine.set_variant(capi.VARIANT_BUILD_LANES, entry["build_lanes"])
+
+
 def signature(replicas):
     """Workload key: particle counts (binned), densities and types."""
     parts = sorted((int(round(r["n"], -2)), round(r["density"], 3), r["ntypes"]) for r in replicas)
@@ -63,14 +95,21 @@ class Autotune:
                 return json.load(fh)
         return {}
 
-    def tune(self, replicas, measure, force=False):
+    def tune(self, replicas, measure, force=False, variants=False):
+        """Stage 1 over (pb, tp, skin); with variants=True, stage 2 over the
+        kernel variants at the winning shape (measure then takes
+        force_staged= and build_lanes= keywords)."""
         key = signature(replicas)
         cache = self._load()
         if key in cache and not force:
             return cache[key]
         best, table = search(candidates(**self.grid), measure)
-        cache[key] = {"pb": best["pb"], "tp": best["tp"], "skin": best["skin"], "rate": best["rate"],
-                      "table": table}
+        entry = {"pb": best["pb"], "tp": best["tp"], "skin": best["skin"], "rate": best["rate"], "table": table}
+        if variants:
+            vbest, vtable = search_variants(entry, measure)
+            entry.update(force_staged=vbest["force_staged"], build_lanes=vbest["build_lanes"],
+                         rate=max(entry["rate"], vbest["rate"]), variant_table=vtable)
+        cache[key] = entry
         with open(self.cache_path, "w") as fh:
             json.dump(cache, fh, indent=1)
         return cache[key]
@@ -99,8 +138,12 @@ def device_measure(capi, replicas, device=0, steps=300, warmup=100):
     replicas: list of dicts with pos4, vel4, box, params, ntypes, T, n, density."""
     import torch
 
-    def measure(pb, tp, skin):
+    def measure(pb, tp, skin, force_staged=None, build_lanes=None):
         e = capi.Engine(device=device, max_replicas=len(replicas), pb=pb, tp=tp)
+        if force_staged is not None:
+            e.set_variant(capi.VARIANT_FORCE_STAGED, force_staged)
+        if build_lanes is not None:
+            e.set_variant(capi.VARIANT_BUILD_LANES, build_lanes)
         ids = [e.add(r["pos4"], r["box"], r["params"], r["ntypes"], cutoff="SF", skin=skin, T=r["T"],
                      vel4=r["vel4"]) for r in replicas]
         e.calc_f()  # invariance check on the common starting configuration
@@ -133,16 +176,21 @@ def main(argv=None):
     p.add_argument("--skins", default="0.3")
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--cache", default="autotune.json")
+    p.add_argument("--no-variants", action="store_true", help="skip the kernel-variant stage")
     args = p.parse_args(argv)
     reps = [equilibrated_ka(capi, args.n, args.T)]
     at = Autotune(cache_path=args.cache, pbs=tuple(int(x) for x in args.pbs.split(",")),
                   tps=tuple(int(x) for x in args.tps.split(",")),
                   skins=tuple(float(x) for x in args.skins.split(",")))
-    best = at.tune(reps, device_measure(capi, reps, steps=args.steps, warmup=200), force=True)
+    best = at.tune(reps, device_measure(capi, reps, steps=args.steps, warmup=200), force=True,
+                   variants=not args.no_variants)
     for r in best["table"]:
         print(f"pb={r['pb']:4d} tp={r['tp']} skin={r['skin']:.2f}  {r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
-    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate")}))
+    for r in best.get("variant_table", []):
+        print(f"force_staged={r['force_staged']} build_lanes={r['build_lanes']}  {r['rate']:.4e} particle-steps/s  "
+              f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
+    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate", "force_staged", "build_lanes") if k in best}))
 
 
 if __name__ == "__main__":

@@ -40,7 +40,8 @@ def _sources(exts):
 
 
 def build_lib(force=False):
-    cu = [os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "probe.cu"), os.path.join(CSRC, "noalloc.cu")]
+    cu = [os.path.join(CSRC, "engine.cu"), os.path.join(CSRC, "probe.cu"), os.path.join(CSRC, "noalloc.cu"),
+          os.path.join(CSRC, "f64.cu")]
     deps = _sources((".cu", ".cuh", ".h"))
     if not force and _newer(LIB, deps):
         return LIB

@@ -16,6 +16,8 @@ LIB_PATH = os.path.join(_HERE, "librumd_b200.so")
 
 B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_OVERFLOW = range(6)
 CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
+# kernel variants (b2md_engine_set_variant)
+VARIANT_FORCE_STAGED, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM = 0, 1, 2
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",
               "target_T", "max_nbrs", "actual_max_nbrs", "mean_nbrs"]
@@ -24,14 +26,16 @@ NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
 
 EXPORTS = [
     "b2md_engine_create", "b2md_engine_destroy", "b2md_engine_set_launch", "b2md_engine_memory",
-    "b2md_engine_set_graph_mode", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
+    "b2md_engine_set_graph_mode", "b2md_engine_set_variant", "b2md_engine_get_variant", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
     "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_set_integrator",
     "b2md_replica_set_xi", "b2md_replica_set_reset_interval", "b2md_replica_set_nb_method",
     "b2md_replica_stats", "b2md_replica_set_energy_log", "b2md_replica_energy_log", "b2md_replica_stress", "b2md_calc_f",
     "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
     "b2md_run_queued", "b2md_nbl_export", "b2md_sort_export", "b2md_cell_grid", "b2md_sync",
     "b2md_stream", "b2md_last_error", "b2md_version", "b2md_probe_dist2", "b2md_probe_cell",
-    "b2md_forces_noalloc",
+    "b2md_forces_noalloc", "b2md_f64_create", "b2md_f64_destroy", "b2md_f64_set_state",
+    "b2md_f64_set_integrator", "b2md_f64_set_xi", "b2md_f64_calc_f", "b2md_f64_run", "b2md_f64_get",
+    "b2md_f64_stats",
 ]
 
 
@@ -65,6 +69,8 @@ def lib():
             "b2md_engine_set_launch": [P, i, i],
             "b2md_engine_memory": [P, ctypes.POINTER(ll)],
             "b2md_engine_set_graph_mode": [P, i],
+            "b2md_engine_set_variant": [P, i, i],
+            "b2md_engine_get_variant": [P, i, ctypes.POINTER(ctypes.c_int)],
             "b2md_replica_add": [P, ctypes.POINTER(ReplicaDesc), P, P, P, ctypes.POINTER(i)],
             "b2md_replica_remove": [P, i],
             "b2md_replica_get": [P, i, i, P],
@@ -92,6 +98,15 @@ def lib():
             "b2md_probe_dist2": [P, P, P, i, P],
             "b2md_probe_cell": [P, i, f, i, P],
             "b2md_forces_noalloc": [P, i, P, i, P, i, P, P, P],
+            "b2md_f64_create": [i, i, i, P, P, i, d, i, ctypes.POINTER(P)],
+            "b2md_f64_destroy": [P],
+            "b2md_f64_set_state": [P, P, P, P],
+            "b2md_f64_set_integrator": [P, d, d, d, i, i],
+            "b2md_f64_set_xi": [P, d],
+            "b2md_f64_calc_f": [P],
+            "b2md_f64_run": [P, ll, P],
+            "b2md_f64_get": [P, i, P],
+            "b2md_f64_stats": [P, P],
         }
         for name, args in sig.items():
             fn = getattr(L, name)
@@ -172,6 +187,15 @@ class Engine:
 
     def set_graph_mode(self, conditional):
         check(lib().b2md_engine_set_graph_mode(self._h, int(bool(conditional))))
+
+    def set_variant(self, which, value):
+        """which: VARIANT_FORCE_STAGED, VARIANT_BUILD_LANES or VARIANT_BUILD_SMEM."""
+        check(lib().b2md_engine_set_variant(self._h, int(which), int(value)))
+
+    def get_variant(self, which):
+        v = ctypes.c_int()
+        check(lib().b2md_engine_get_variant(self._h, int(which), ctypes.byref(v)))
+        return v.value
 
     def memory(self):
         b = ctypes.c_longlong()
@@ -320,3 +344,89 @@ def probe_cell(x, box, nc):
     out = np.zeros((len(x), 2), np.int32)
     check(lib().b2md_probe_cell(_ptr(x), len(x), float(box), int(nc), _ptr(out)))
     return out
+
+
+F64_STAT_NAMES = ["pe", "virial", "ke", "ke2", "xi", "rebuilds", "steps"]
+
+
+class F64Engine:
+    """One system in the FP64 engine (b2md_f64_*): the accuracy oracle on the GPU.
+
+    pos4 / vel4 as for Engine.add, but float64, with the type as a whole
+    number in pos4[:, 3] (Engine's float32 pos4 with type bits is accepted
+    too and converted)."""
+
+    def __init__(self, pos4, box, params, ntypes, cutoff="SF", skin=0.3, dt=0.005, T=1.0, tau=0.2,
+                 thermostat=True, reset_interval=100, vel4=None, im3=None, max_nbrs=0, device=0):
+        pos4 = np.asarray(pos4)
+        n = len(pos4)
+        if pos4.dtype == np.float32:
+            types = np.ascontiguousarray(pos4[:, 3]).view(np.int32).astype(np.float64)
+            p = np.zeros((n, 4))
+            p[:, :3] = pos4[:, :3]
+            p[:, 3] = types
+            pos4 = p
+        pos4 = np.ascontiguousarray(pos4, np.float64)
+        if vel4 is None:
+            vel4 = np.zeros((n, 4))
+            vel4[:, 3] = 1.0
+        vel4 = np.ascontiguousarray(vel4, np.float64)
+        im3 = None if im3 is None else np.ascontiguousarray(im3, np.int32)
+        params = np.ascontiguousarray(params, np.float32)
+        box3 = np.ascontiguousarray(np.broadcast_to(np.asarray(box, np.float64), (3,)))
+        c = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
+        self.n = n
+        self._h = ctypes.c_void_p()
+        check(lib().b2md_f64_create(int(device), n, int(ntypes), _ptr(box3), _ptr(params), c, float(skin),
+                                    int(max_nbrs), ctypes.byref(self._h)))
+        self.set_state(pos4, vel4, im3)
+        self.set_integrator(dt, T, tau, thermostat, reset_interval)
+
+    def close(self):
+        if self._h:
+            lib().b2md_f64_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_state(self, pos4, vel4, im3=None):
+        pos4 = np.ascontiguousarray(pos4, np.float64)
+        vel4 = np.ascontiguousarray(vel4, np.float64)
+        im3 = None if im3 is None else np.ascontiguousarray(im3, np.int32)
+        check(lib().b2md_f64_set_state(self._h, _ptr(pos4), _ptr(vel4), _ptr(im3)))
+
+    def set_integrator(self, dt, T, tau, thermostat=True, reset_interval=100):
+        check(lib().b2md_f64_set_integrator(self._h, float(dt), float(T), float(tau), int(bool(thermostat)),
+                                            int(reset_interval)))
+
+    def set_xi(self, xi):
+        check(lib().b2md_f64_set_xi(self._h, float(xi)))
+
+    def calc_f(self):
+        check(lib().b2md_f64_calc_f(self._h))
+
+    def run(self, nsteps, energies=False):
+        """Runs nsteps; with energies=True returns [nsteps, 4] = pe, W, KE(t), xi."""
+        en = np.zeros((int(nsteps), 4)) if energies else None
+        check(lib().b2md_f64_run(self._h, int(nsteps), _ptr(en)))
+        return en
+
+    def get(self, field):
+        """field: "pos", "vel", "force" ([n,4] float64) or "images" ([n,3] int32)."""
+        if field == "images":
+            out = np.zeros((self.n, 3), np.int32)
+            check(lib().b2md_f64_get(self._h, 3, _ptr(out)))
+            return out
+        code = {"pos": 0, "vel": 1, "force": 2}[field]
+        out = np.zeros((self.n, 4))
+        check(lib().b2md_f64_get(self._h, code, _ptr(out)))
+        return out
+
+    def stats(self):
+        out = np.zeros(len(F64_STAT_NAMES))
+        check(lib().b2md_f64_stats(self._h, _ptr(out)))
+        return dict(zip(F64_STAT_NAMES, out.tolist()))

@@ -128,6 +128,10 @@ struct b2md_engine {
   // pools
   long long pcap = 0, ecap = 0, ccap = 0, qcap = 0, zcap = 0;
   int rcap = 0;
+  // kernel variants (b2md_engine_set_variant)
+  bool force_staged = false;  // force kernel: list tile staged in shared memory
+  int build_lanes = 2;         // list build: lanes per particle
+  bool build_smem = false;     // list build: tile assembled in shared memory
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
   float4* r[2] = {nullptr, nullptr};
   float4* v[2] = {nullptr, nullptr};
@@ -277,9 +281,15 @@ EngArgs make_args(b2md_engine* e) {
   return a;
 }
 
-// Dynamic shared memory of k_force: pair table + staged list tile.
-size_t force_smem(const EngArgs& a) {
-  return (size_t)kParSmemFloats * sizeof(float) + (size_t)a.idx_rows * a.idx_pitch * sizeof(unsigned);
+// Dynamic shared memory of k_force: pair table [+ staged list tile].
+size_t force_smem(const EngArgs& a, bool staged) {
+  return (size_t)kParSmemFloats * sizeof(float) + (staged ? (size_t)a.idx_rows * a.idx_pitch * sizeof(unsigned) : 0);
+}
+
+// Dynamic shared memory of k_rb_build: cut-off table [+ list tile].
+size_t build_smem(const b2md_engine* e, const EngArgs& a) {
+  const int pb = e->pb;
+  return (size_t)kCs2Floats * sizeof(float) + (e->build_smem ? (size_t)a.idx_rows * (pb + 4) * sizeof(unsigned) : 0);
 }
 
 // Re-lays out tiles and reduction groups over the active replicas and uploads
@@ -488,36 +498,46 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   k_rb_scatter<<<T, e->pb, 0, s>>>(a);
   k_rb_fix<<<T, e->pb, 0, s>>>(a);
   k_rb_permute<<<T, e->pb, 0, s>>>(a);
-  // list build: LP lanes per particle, the tile's list staged in shared memory
-  const size_t smem = (size_t)kCs2Floats * sizeof(float) + (size_t)a.idx_rows * (e->pb + 4) * sizeof(unsigned);
+  // list build: build_lanes lanes per particle (fewer when pb*lanes would
+  // exceed a block), the list either assembled in shared memory or stored
+  // straight to global memory
+  const size_t smem = build_smem(e, a);
   if (smem > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
-  // lanes per particle: 8, or fewer for tiles so large that pb*8 > 512
-  const int lanes = std::min(8, kMaxBlock / e->pb);
-  if (lanes >= 8) k_rb_build<8><<<T, e->pb * 8, smem, s>>>(a);
-  else if (lanes >= 4) k_rb_build<4><<<T, e->pb * 4, smem, s>>>(a);
-  else if (lanes >= 2) k_rb_build<2><<<T, e->pb * 2, smem, s>>>(a);
-  else k_rb_build<1><<<T, e->pb, smem, s>>>(a);
+  const int lanes = std::min(e->build_lanes, kMaxBlock / e->pb);
+#define LB(LPV)                                                                    \
+  if (lanes >= LPV) {                                                              \
+    if (e->build_smem) k_rb_build<LPV, true><<<T, e->pb * LPV, smem, s>>>(a);     \
+    else k_rb_build<LPV, false><<<T, e->pb * LPV, smem, s>>>(a);                  \
+    return;                                                                        \
+  }
+  LB(8) LB(4) LB(2) LB(1)
+#undef LB
 }
 
 typedef void (*ForceFn)(EngArgs, int, cudaGraphConditionalHandle);
 
-ForceFn force_fn_raw(int tp, bool fused, bool stress) {
-#define SEL(TPV)                                               \
-  if (tp == TPV) {                                             \
-    if (fused) return k_force<TPV, true, false>;               \
-    return stress ? k_force<TPV, false, true> : k_force<TPV, false, false>; \
+template <bool STAGED>
+ForceFn force_fn_var(int tp, bool fused, bool stress) {
+#define SEL(TPV)                                                                          \
+  if (tp == TPV) {                                                                        \
+    if (fused) return k_force<TPV, true, false, STAGED>;                                  \
+    return stress ? k_force<TPV, false, true, STAGED> : k_force<TPV, false, false, STAGED>; \
   }
   SEL(1) SEL(2) SEL(4) SEL(8)
 #undef SEL
   return nullptr;
 }
 
+ForceFn force_fn_raw(int tp, bool fused, bool stress, bool staged) {
+  return staged ? force_fn_var<true>(tp, fused, stress) : force_fn_var<false>(tp, fused, stress);
+}
+
 // The force kernel for (tp, fused, stress), allowed to use the dynamic
 // shared memory the staged list tile `a` needs.
-ForceFn force_fn(int tp, bool fused, bool stress, const EngArgs& a) {
-  ForceFn fn = force_fn_raw(tp, fused, stress);
-  if (force_smem(a) > kMaxDynSmemBytes)
+ForceFn force_fn(const b2md_engine* e, bool fused, bool stress, const EngArgs& a) {
+  ForceFn fn = force_fn_raw(e->tp, fused, stress, e->force_staged);
+  if (force_smem(a, e->force_staged) > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
   return fn;
 }
@@ -528,21 +548,21 @@ void init_func_attrs(int device) {
   static unsigned long long done_mask = 0ull;  // one bit per device
   const unsigned long long bit = 1ull << (device & 63);
   if (done_mask & bit) return;
-  const void* builds[] = {(const void*)k_rb_build<1>, (const void*)k_rb_build<2>, (const void*)k_rb_build<4>,
-                          (const void*)k_rb_build<8>};
+  const void* builds[] = {(const void*)k_rb_build<1, true>, (const void*)k_rb_build<2, true>,
+                          (const void*)k_rb_build<4, true>, (const void*)k_rb_build<8, true>};
   for (const void* f : builds)
     CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
   for (int tp : {1, 2, 4, 8})
     for (int v = 0; v < 3; ++v)
-      CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2),
+      CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2, true),
                               cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
   done_mask |= bit;
 }
 
 void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
   if (e->ntiles == 0) return;
-  ForceFn fn = force_fn(e->tp, fused, stress, a);
-  fn<<<e->ntiles, e->pb * e->tp, force_smem(a), s>>>(a, 0, cudaGraphConditionalHandle{});
+  ForceFn fn = force_fn(e, fused, stress, a);
+  fn<<<e->ntiles, e->pb * e->tp, force_smem(a, e->force_staged), s>>>(a, 0, cudaGraphConditionalHandle{});
 }
 
 void check_launch() { CK(cudaGetLastError()); }
@@ -552,8 +572,8 @@ void build_graph(b2md_engine* e, int which, int K) {
   EngArgs a = make_args(e);
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
-  const size_t smem = force_smem(a);
-  ForceFn fstep = force_fn(e->tp, true, false, a);
+  const size_t smem = force_smem(a, e->force_staged);
+  ForceFn fstep = force_fn(e, true, false, a);
   if (e->cond_mode) {
     std::vector<cudaGraphConditionalHandle> hs(K);
     for (int k = 0; k < K; ++k) CK(cudaGraphConditionalHandleCreate(&hs[k], g, 0, cudaGraphCondAssignDefault));
@@ -753,9 +773,11 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
     grow_reps(e, std::max(max_replicas, 1));
     init_func_attrs(device);
     CK(cudaMalloc(&e->fctr, sizeof(unsigned)));
-    CK(cudaMalloc(&e->any_rebuild, sizeof(int)));
+    // [0]: "a replica needs a rebuild" raised by the step kernel;
+    // [1]: the same decision read by the host in b2md_run_timed
+    CK(cudaMalloc(&e->any_rebuild, 2 * sizeof(int)));
     CK(cudaMemsetAsync(e->fctr, 0, sizeof(unsigned), e->stream));
-    CK(cudaMemsetAsync(e->any_rebuild, 0, sizeof(int), e->stream));
+    CK(cudaMemsetAsync(e->any_rebuild, 0, 2 * sizeof(int), e->stream));
     CK(cudaStreamSynchronize(e->stream));
   });
   if (rc != B2MD_OK) {
@@ -806,6 +828,40 @@ int b2md_engine_set_graph_mode(b2md_engine* e, int conditional) {
   if (!e) return fail(B2MD_ERR_ARG, "null engine");
   e->cond_mode = conditional ? 1 : 0;
   invalidate_graphs(e);
+  return B2MD_OK;
+}
+
+int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
+  if (!e) return fail(B2MD_ERR_ARG, "null engine");
+  switch (which) {
+    case B2MD_VARIANT_FORCE_STAGED:
+      if (value != 0 && value != 1) return fail(B2MD_ERR_ARG, "force_staged must be 0 or 1");
+      e->force_staged = value != 0;
+      break;
+    case B2MD_VARIANT_BUILD_LANES:
+      if (value != 1 && value != 2 && value != 4 && value != 8)
+        return fail(B2MD_ERR_ARG, "build lanes must be 1, 2, 4 or 8 (got %d)", value);
+      e->build_lanes = value;
+      break;
+    case B2MD_VARIANT_BUILD_SMEM:
+      if (value != 0 && value != 1) return fail(B2MD_ERR_ARG, "build_smem must be 0 or 1");
+      e->build_smem = value != 0;
+      break;
+    default:
+      return fail(B2MD_ERR_ARG, "unknown variant %d", which);
+  }
+  invalidate_graphs(e);
+  return B2MD_OK;
+}
+
+int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
+  if (!e || !value) return fail(B2MD_ERR_ARG, "null argument");
+  switch (which) {
+    case B2MD_VARIANT_FORCE_STAGED: *value = e->force_staged ? 1 : 0; break;
+    case B2MD_VARIANT_BUILD_LANES: *value = e->build_lanes; break;
+    case B2MD_VARIANT_BUILD_SMEM: *value = e->build_smem ? 1 : 0; break;
+    default: return fail(B2MD_ERR_ARG, "unknown variant %d", which);
+  }
   return B2MD_OK;
 }
 
@@ -1249,19 +1305,30 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     long long nl = 2;
-    const size_t smem = force_smem(a);
-    ForceFn fstep = force_fn(e->tp, true, false, a);
+    const size_t smem = force_smem(a, e->force_staged);
+    ForceFn fstep = force_fn(e, true, false, a);
     std::vector<cudaEvent_t> ev(2 * nsteps);
     for (auto& x : ev) CK(cudaEventCreate(&x));
+    int* h_any = nullptr;
+    CK(cudaMallocHost(&h_any, sizeof(int)));
+    // the launch sequence of the step graph, with the host taking the
+    // conditional node's decision: rebuild kernels only when a replica is due
     for (long long k = 0; k < nsteps; ++k) {
-      launch_rebuild(e, e->stream, a);
+      k_gate_flag<<<1, 128, 0, e->stream>>>(a, e->any_rebuild + 1);
+      CK(cudaMemcpyAsync(h_any, e->any_rebuild + 1, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      if (*h_any) {
+        launch_rebuild(e, e->stream, a);
+        nl += 9;
+      }
       CK(cudaEventRecord(ev[2 * k], e->stream));
       fstep<<<e->ntiles, e->pb * e->tp, smem, e->stream>>>(a, 0, cudaGraphConditionalHandle{});
       CK(cudaEventRecord(ev[2 * k + 1], e->stream));
-      nl += 10;
+      nl += 2;
     }
     check_launch();
     CK(cudaStreamSynchronize(e->stream));
+    cudaFreeHost(h_any);
     double tot = 0.0;
     for (long long k = 0; k < nsteps; ++k) {
       float ms = 0.f;

@@ -234,16 +234,37 @@ __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const floa
   }
 }
 
+// One list entry, read once: streamed past L1 so that L1 keeps the gathered
+// neighbour positions (which neighbouring particles share).
+__device__ __forceinline__ unsigned ld_stream(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.global.nc.L1::no_allocate.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+// List-entry readers for force_loop: entry k of the particle's column.
+// Staged: the tile's list copied to shared memory (row pitch `pitch`).
+struct IdxStaged {
+  const unsigned* p;
+  int pitch;
+  __device__ __forceinline__ unsigned operator()(unsigned k) const { return p[k * pitch]; }
+};
+// Streamed: read from the global list inside the loop (ld_stream).
+struct IdxStreamed {
+  const unsigned* p;
+  size_t stride;
+  __device__ __forceinline__ unsigned operator()(unsigned k) const { return ld_stream(p + k * stride); }
+};
+
 // The neighbour loop of one thread: entries k = lane_t, lane_t + TP, ... of
-// the staged list column, four gathers in flight.
-template <int TP, bool STRESS, bool WRAP>
-__device__ __forceinline__ void force_loop(PairAcc& A, const unsigned* sc, int pitch, unsigned lane_t, unsigned nn,
+// the particle's list column, four gathers in flight.
+template <int TP, bool STRESS, bool WRAP, class Idx>
+__device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, unsigned lane_t, unsigned nn,
                                            const float4* __restrict__ rc, const float4& ri, const float* prow,
                                            float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
   unsigned k = lane_t;
   for (; k + 3 * TP < nn; k += 4 * TP) {
-    const unsigned j0 = sc[k * pitch], j1 = sc[(k + TP) * pitch];
-    const unsigned j2 = sc[(k + 2 * TP) * pitch], j3 = sc[(k + 3 * TP) * pitch];
+    const unsigned j0 = idx(k), j1 = idx(k + TP), j2 = idx(k + 2 * TP), j3 = idx(k + 3 * TP);
     const float4 r0 = __ldg(rc + j0), r1 = __ldg(rc + j1), r2 = __ldg(rc + j2), r3 = __ldg(rc + j3);
     lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
     lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
@@ -251,16 +272,21 @@ __device__ __forceinline__ void force_loop(PairAcc& A, const unsigned* sc, int p
     lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
   for (; k < nn; k += TP) {
-    const float4 r0 = __ldg(rc + sc[k * pitch]);
+    const float4 r0 = __ldg(rc + idx(k));
     lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
 }
 
-// Shared memory of k_force: [packed pair table, kParSmemFloats] [index tile]
+// Shared memory of k_force: [packed pair table, kParSmemFloats] [index tile
+// when STAGED]
 constexpr int kParSmemFloats = kMaxTypes * kMaxTypes * kParStride;
 constexpr unsigned kWaitPolls = 1u << 22;
 
-template <int TP, bool FUSED, bool STRESS>
+// One tile of pb particles per block, tp threads per particle.
+// STAGED = true copies the tile's list rows to shared memory with TMA bulk
+// copies before the pair loop; STAGED = false streams the list entries from
+// global memory inside the loop and leaves the shared memory to L1.
+template <int TP, bool FUSED, bool STRESS, bool STAGED>
 __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cudaGraphConditionalHandle h) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   float* s_par = reinterpret_cast<float*>(s_dyn);
@@ -279,29 +305,31 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     const int pb = blockDim.x / TP;
     const int first = a.tile_first[tile];
     const int pitch = a.idx_pitch;
-    // 1. rows of the list this tile needs: the largest neighbour count in it
-    if (threadIdx.x == 0) {
-      s_rows = 0u;
-      mbar_init(&s_bar, 1);
-      mbar_fence_init();
-    }
-    __syncthreads();
-    {
-      unsigned c = (threadIdx.x < pb && first + (int)threadIdx.x < R.n) ? a.nn[R.p0 + first + threadIdx.x] : 0u;
+    if (STAGED) {
+      // 1. rows of the list this tile needs: the largest neighbour count in it
+      if (threadIdx.x == 0) {
+        s_rows = 0u;
+        mbar_init(&s_bar, 1);
+        mbar_fence_init();
+      }
+      __syncthreads();
+      {
+        unsigned c = (threadIdx.x < pb && first + (int)threadIdx.x < R.n) ? a.nn[R.p0 + first + threadIdx.x] : 0u;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
-      if ((threadIdx.x & 31) == 0 && c) atomicMax(&s_rows, c);
-    }
-    __syncthreads();
-    const unsigned rows = min(s_rows, (unsigned)a.idx_rows);
-    // 2. one TMA bulk copy per list row: slots [first, first+width) of rows 0..rows-1
-    if (threadIdx.x < 32) {
-      const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
-      if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, rows * width * 4u);
-      __syncwarp();
-      const unsigned* src = a.nbl + R.nbl0 + first;
-      for (unsigned r = threadIdx.x; r < rows; r += 32)
-        bulk_g2s(s_idx + r * pitch, src + (size_t)r * R.nbl_stride, width * 4u, &s_bar);
+        for (int o = 16; o > 0; o >>= 1) c = max(c, __shfl_xor_sync(0xffffffffu, c, o));
+        if ((threadIdx.x & 31) == 0 && c) atomicMax(&s_rows, c);
+      }
+      __syncthreads();
+      const unsigned rows = min(s_rows, (unsigned)a.idx_rows);
+      // 2. one TMA bulk copy per list row: slots [first, first+width) of rows 0..rows-1
+      if (threadIdx.x < 32) {
+        const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, rows * width * 4u);
+        __syncwarp();
+        const unsigned* src = a.nbl + R.nbl0 + first;
+        for (unsigned r = threadIdx.x; r < rows; r += 32)
+          bulk_g2s(s_idx + r * pitch, src + (size_t)r * R.nbl_stride, width * 4u, &s_bar);
+      }
     }
     // 3. meanwhile: pair table and this particle's data
     const int nt = R.ntypes;
@@ -324,21 +352,31 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     // particles skip it.
     const bool inner = fabsf(ri.x) < R.ilim[0] && fabsf(ri.y) < R.ilim[1] && fabsf(ri.z) < R.ilim[2];
     const bool fast = __all_sync(0xffffffffu, !valid || inner);
-    // 4. bounded wait for the index tile
-    const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
     PairAcc A;
-    if (ok) {
-      const unsigned* sc = s_idx + lp;
-      if (fast)
-        force_loop<TP, STRESS, false>(A, sc, pitch, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-      else
-        force_loop<TP, STRESS, true>(A, sc, pitch, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    if (STAGED) {
+      // 4. bounded wait for the index tile (also publishes the pair table)
+      const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
+      if (ok) {
+        const IdxStaged idx{s_idx + lp, pitch};
+        if (fast)
+          force_loop<TP, STRESS, false>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+        else
+          force_loop<TP, STRESS, true>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+      } else {
+        // the copies did not land in time: record it for the host and wait
+        // (bounded) for them before this block's shared memory is released
+        if (threadIdx.x == 0) atomicExch(&S->err, 1);
+        mbar_wait_bounded(&s_bar, 0, kWaitPolls);
+      }
     } else {
-      // the copies did not land in time: record it for the host and wait
-      // (bounded) for them before this block's shared memory is released
-      if (threadIdx.x == 0) atomicExch(&S->err, 1);
-      mbar_wait_bounded(&s_bar, 0, kWaitPolls);
+      __syncthreads();  // the pair table
+      const IdxStreamed idx{a.nbl + R.nbl0 + i, (size_t)R.nbl_stride};
+      if (fast)
+        force_loop<TP, STRESS, false>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+      else
+        force_loop<TP, STRESS, true>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
     }
+
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
     float sxx = A.sxx, syy = A.syy, szz = A.szz, syz = A.syz, sxz = A.sxz, sxy = A.sxy;
     if (TP > 1) {
@@ -503,6 +541,18 @@ __global__ void k_gate(EngArgs a, cudaGraphConditionalHandle h) {
     if (a.rep[r].active && a.st[r].rebuild && !a.st[r].overflow) s_any = 1;
   __syncthreads();
   if (threadIdx.x == 0) cudaGraphSetConditional(h, s_any ? 1u : 0u);
+}
+
+// The gate's decision written to memory (for a host that takes it instead of
+// a conditional graph node).
+__global__ void k_gate_flag(EngArgs a, int* out) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < a.nrep; r += blockDim.x)
+    if (a.rep[r].active && a.st[r].rebuild && !a.st[r].overflow) s_any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) *out = s_any;
 }
 
 // ---------------------------------------------------------------------------
@@ -706,7 +756,9 @@ __global__ void k_rb_permute(EngArgs a) {
 //     column-major row of the tile is one contiguous slot run).
 constexpr int kCs2Floats = kMaxTypes * kMaxTypes;
 
-template <int LP>
+//     SMEM_LIST = false writes the entries straight to the global list (one
+//     lane per particle needs no shared-memory tile and keeps occupancy high).
+template <int LP, bool SMEM_LIST>
 __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   float* s_cs2 = reinterpret_cast<float*>(s_dyn);
@@ -758,7 +810,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
       const unsigned g = (__ballot_sync(0xffffffffu, in) >> gshift) & gbits;
       if (in) {
         const int pos = count + __popc(g & below);
-        if (pos < maxn) s_list[pos * lpitch + lp] = (unsigned)j;
+        if (pos < maxn) {
+          if (SMEM_LIST) s_list[pos * lpitch + lp] = (unsigned)j;
+          else a.nbl[R.nbl0 + (size_t)pos * R.nbl_stride + i] = (unsigned)j;
+        }
       }
       count += __popc(g);
     }
@@ -813,9 +868,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
     atomicMax(&s_max, count);
   }
   // write the tile's rows [0, rows) of the list: slots [first, first+width)
-  fence_async_shared();
+  if (SMEM_LIST) fence_async_shared();
   __syncthreads();
-  if (threadIdx.x < 32) {
+  if (SMEM_LIST && threadIdx.x < 32) {
     const int rows = min(s_max, maxn);
     const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
     unsigned* dst = a.nbl + R.nbl0 + first;

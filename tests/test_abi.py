@@ -45,3 +45,7 @@ def test_error_reporting_without_gpu():
     rc = lib.b2md_engine_create(0, 0, 1, 0, 64, 3, ctypes.byref(h))  # tp not a power of two
     assert rc == capi.B2MD_ERR_ARG
     assert lib.b2md_version().startswith(b"rumd_b200")
+    # a null engine is rejected before any device work
+    assert lib.b2md_engine_set_variant(None, capi.VARIANT_BUILD_LANES, 4) == capi.B2MD_ERR_ARG
+    v = ctypes.c_int()
+    assert lib.b2md_engine_get_variant(None, capi.VARIANT_BUILD_LANES, ctypes.byref(v)) == capi.B2MD_ERR_ARG

@@ -288,6 +288,43 @@ def test_fused_run_equals_separate_calcf_integrate(capi, ka_params):
     assert s1["xi"] == s2["xi"]
 
 
+VARIANTS = [  # (force_staged, build_lanes, build_smem)
+    (1, 8, 1), (0, 8, 1), (1, 1, 0), (0, 1, 0), (0, 2, 0), (0, 4, 0), (0, 8, 0), (0, 1, 1)]
+
+
+@pytest.mark.parametrize("tp", [1, 4])
+def test_kernel_variants_give_identical_lists_and_trajectories(capi, oracle, ka_params, tp):
+    """Every (force index staging, list-build lanes, list-build staging) choice
+    gives the oracle's list and the same trajectory bit for bit."""
+    n = 6000
+    m = melted_ka(capi, ka_params, n, steps=100, seed=21)
+    nc, old, counts, nbl, ov = oracle_sorted_list(oracle, m["pos4"], m["box"], ka_params, 2, 0.3, 400)
+    assert not ov
+    res = []
+    for fs, lanes, bs in VARIANTS:
+        e = new_engine(capi, pb=64, tp=tp)
+        e.set_variant(capi.VARIANT_FORCE_STAGED, fs)
+        e.set_variant(capi.VARIANT_BUILD_LANES, lanes)
+        e.set_variant(capi.VARIANT_BUILD_SMEM, bs)
+        assert e.get_variant(capi.VARIANT_BUILD_LANES) == lanes
+        rid = e.add(m["pos4"], m["box"], ka_params, 2, cutoff="SF", dt=0.005, T=0.9, vel4=m["vel4"])
+        e.calc_f()
+        gc, gl = e.nbl(rid, n, 400)
+        for s in range(0, n, 7):
+            i = old[s]
+            assert gc[i] == counts[s]
+            assert np.array_equal(gl[i, : gc[i]], old[nbl[s, : counts[s]]])
+        f0 = e.get(rid, "force", n)
+        e.run(200)
+        res.append((f0, e.get(rid, "pos", n), e.get(rid, "vel", n), e.stats(rid)))
+        e.close()
+    for f0, p, v, st in res[1:]:
+        assert np.array_equal(f0, res[0][0])
+        assert np.array_equal(p, res[0][1])
+        assert np.array_equal(v, res[0][2])
+        assert st["xi"] == res[0][3]["xi"] and st["rebuilds"] == res[0][3]["rebuilds"]
+
+
 def test_conditional_and_plain_graphs_agree(capi, ka_params):
     n = 3000
     m = melted_ka(capi, ka_params, n, steps=50, seed=12)
