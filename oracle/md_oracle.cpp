@@ -24,6 +24,11 @@
 //   * host FP64 sums (pe, virial)       src/Sample.cu:353-391
 //   * degrees of freedom 3N-3           src/Sample.cu:301
 //
+// FP64 mode (orc_md_run_f64) restates the reference built after
+// changeToDouble.sh (changeToDouble.sh:1-189): every quantity is a double,
+// including the shift constants s(rc) rc, u(rc) (from rc, A12, A6 of the
+// table) and omega^2 = 4 pi^2 / tau^2.
+//
 // Arithmetic: compiled with -ffp-contract=off so that every float operation
 // rounds exactly where it is written.  Where the reference's device build
 // contracts a product and a sum into one fused multiply-add, the restatement
@@ -400,6 +405,9 @@ template <class R> struct MDState {
   int max_nbrs, nc[3];
   const float* params;
   float skin;
+  // FP64 mode only: s(rc) rc and u(rc) per type pair, computed in double from
+  // rc, A12, A6 (what CopyParamsToGPU computes in a changeToDouble.sh build)
+  std::vector<double> cs64, cu64;
 };
 
 template <class R> static inline R mi(R dr, R L, R invL) {
@@ -512,12 +520,15 @@ template <class R> static void md_forces(MDState<R>& S) {
           s = i6 * i2 * (R(12) * t + R(6) * (R)p[2]);
           fw += i6 * (t + (R)p[2]);
         }
+        const int pk = ti * ntypes + S.type[j];
+        const R cs = sizeof(R) == 8 ? (R)S.cs64[pk] : (R)p[NP - 2];
+        const R cu = sizeof(R) == 8 ? (R)S.cu64[pk] : (R)p[NP - 1];
         if (S.cutoff == ORC_SP) {
-          fw -= (R)p[NP - 1];
+          fw -= cu;
         } else if (S.cutoff == ORC_SF) {
           R r = std::sqrt(d2);
-          s -= (R)p[NP - 2] / r;
-          fw += (R)p[NP - 2] * (r - rc) - (R)p[NP - 1];
+          s -= cs / r;
+          fw += cs * (r - rc) - cu;
         }
         fx += dx * s; fy += dy * s; fz += dz * s;
         ww += d2 * s;
@@ -560,8 +571,18 @@ static int md_run(int n, float* pos4, float* vel4, int* im3, const float* L, int
     std::memcpy(&S.type[i], &pos4[4 * i + 3], 4);
     S.uidx[i] = (unsigned)i;
   }
+  S.cs64.resize(ntypes * ntypes);
+  S.cu64.resize(ntypes * ntypes);
+  for (int k = 0; k < ntypes * ntypes; ++k) {
+    const double rc = params[k * NP], a12 = params[k * NP + 1], a6 = params[k * NP + 2];
+    const double i2 = 1.0 / (rc * rc), i6 = i2 * i2 * i2;
+    S.cu64[k] = i6 * (a12 * i6 + a6);
+    S.cs64[k] = i6 * i2 * (12.0 * a12 * i6 + 6.0 * a6) * rc;
+  }
   double xi = *xi_io;
-  const float omega2 = (float)(4. * M_PI * M_PI / (tau * tau));
+  // omega^2 = 4 pi^2 / tau^2: a float in the reference, a double in its FP64 build
+  const double omega2 = sizeof(R) == 4 ? (double)(float)(4. * M_PI * M_PI / (tau * tau))
+                                       : 4. * M_PI * M_PI / (tau * tau);
   const int dof = 3 * n - 3;
   const float s2_4 = (float)(0.25 * skin * skin);
   int rebuilds = 0;

@@ -691,7 +691,9 @@ __global__ void k_rb_scatter(EngArgs a) {
 }
 
 // (5) order each bucket by old index: the result equals a stable sort by key
-//     (thrust::sort_by_key on (cellIndex, iota), Sample.h:174-188)
+//     (thrust::sort_by_key on (cellIndex, iota), Sample.h:174-188).  Also
+//     turns cstart into each cell's absolute first slot (cstart + the chunk's
+//     prefix), which the list build reads without a division.
 __global__ void k_rb_fix(EngArgs a) {
   const int tile = blockIdx.x, rep = a.tile_rep[tile];
   if (!rb_active(a, rep)) return;
@@ -699,8 +701,10 @@ __global__ void k_rb_fix(EngArgs a) {
   if (R.nb_method != NB_CELLS) return;
   const int ch = cell_chunk(R), lt = tile - R.tile0;
   const int c0 = lt * ch, c1 = min(R.ncell, c0 + ch);
+  const int pref = a.cpref[R.tile0 + lt];
   for (int c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-    const int b = cell_begin(a, R, c, ch), m = a.cnt[R.cell0 + c];
+    const int b = a.cstart[R.cell0 + c] + pref, m = a.cnt[R.cell0 + c];
+    a.cstart[R.cell0 + c] = b;
     unsigned* o = a.order + (size_t)R.p0 + b;
     for (int p = 1; p < m; ++p) {
       unsigned x = o[p];
@@ -819,7 +823,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
     }
   };
   if (R.nb_method == NB_CELLS) {
-    const int ch = cell_chunk(R);
+    const int* __restrict__ cbeg = a.cstart + R.cell0;  // absolute first slot (k_rb_fix)
+    const int* __restrict__ ccnt = a.cnt + R.cell0;
     const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
     const int cx = cell_coord(ri.x, iLx, nx), cy = cell_coord(ri.y, iLy, ny), cz = cell_coord(ri.z, iLz, nz);
     // With at least 7 cells per side and no wrapped cell among the 5x5x5,
@@ -830,7 +835,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
                        cz >= 2 && cz < nz - 2;
     const bool wrap = !__all_sync(0xffffffffu, !valid || inner);
     for (int dz = -2; dz <= 2; ++dz) {
-      const int oz = (cz + dz + nz) % nz;
+      int oz = cz + dz;
+      oz += ((oz < 0) - (oz >= nz)) * nz;
       for (int dy = -2; dy <= 2; ++dy) {
         int oy = cy + dy;
         oy += ((oy < 0) - (oy >= ny)) * ny;
@@ -843,16 +849,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
         if (valid) {
           if (lo >= 0 && hi < nx) {
             const int c1 = row + hi;
-            b0 = cell_begin(a, R, row + lo, ch);
-            e0 = cell_begin(a, R, c1, ch) + a.cnt[R.cell0 + c1];
+            b0 = cbeg[row + lo];
+            e0 = cbeg[c1] + ccnt[c1];
           } else {
             const int cw = row + nx - 1;
             const int ca = lo < 0 ? row + nx + lo : row + lo;  // first cell of the wrapped part order
             const int cb = lo < 0 ? row + hi : row + hi - nx;
-            b0 = cell_begin(a, R, ca, ch);
-            e0 = cell_begin(a, R, cw, ch) + a.cnt[R.cell0 + cw];
-            b1 = cell_begin(a, R, row, ch);
-            e1 = cell_begin(a, R, cb, ch) + a.cnt[R.cell0 + cb];
+            b0 = cbeg[ca];
+            e0 = cbeg[cw] + ccnt[cw];
+            b1 = cbeg[row];
+            e1 = cbeg[cb] + ccnt[cb];
           }
         }
         seg(b0, e0, wrap);
