@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=2000)
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--force-mode", type=int, default=None, help="kernel variant: 0 streamed, 1 staged, 2 window")
+    p.add_argument("--build-lanes", type=int, default=None, help="kernel variant: list-build lanes per particle")
     p.add_argument("--profile-launches", action="store_true",
                    help="small plain run only (for the ncu launch list)")
     return p.parse_args()
@@ -175,6 +177,18 @@ def profiled_traffic():
 # workloads
 # ---------------------------------------------------------------------------
 
+# kernel variants for every engine the bench makes (None: the engine's default)
+KERNEL_VARIANTS = {}
+
+
+def new_engine(capi, **kw):
+    e = capi.Engine(**kw)
+    for which, value in KERNEL_VARIANTS.items():
+        if value is not None:
+            e.set_variant(which, value)
+    return e
+
+
 def ka_params():
     from rumd_b200 import initconf as I
     return I.lj_params(2, I.KA)
@@ -185,7 +199,7 @@ def prepare_plain(capi, device, pb, tp, seed):
     from rumd_b200 import initconf as I
     c = I.ka_config(N_PLAIN, density=KA_DENSITY, T=2.0, seed=seed)
     params = ka_params()
-    e = capi.Engine(device=device, pb=pb, tp=tp)
+    e = new_engine(capi, device=device, pb=pb, tp=tp)
     rid = e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=2.0, tau=TAU, vel4=c["vel4"])
     e.run(1000)
     e.set_integrator(rid, DT, T_PLAIN, TAU)
@@ -215,11 +229,12 @@ def time_run(capi, e, steps, device):
     return t0.elapsed_time(t1) / 1e3
 
 
-def launches_in_run(steps, rebuilds):
-    # per step: fused kernel; per graph launch: gate; per rebuild: 9 kernels;
-    # run start: steps + momentum; run end: rebuild sequence + force kernel
+def launches_in_run(steps, rebuilds, per_rebuild=9):
+    # per step: fused kernel; per graph launch: gate; per rebuild: 9 kernels
+    # (10 with position windows); run start: steps + momentum; run end:
+    # rebuild sequence + force kernel
     graph_launches = steps // 32 + steps % 32
-    return int(steps + graph_launches + 9 * rebuilds + 2 + 10)
+    return int(steps + graph_launches + per_rebuild * rebuilds + 2 + per_rebuild + 1)
 
 
 def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
@@ -244,7 +259,7 @@ def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
 
 def e2e_run(capi, device, pb, tp, pos4, vel4, im3, box, params, steps):
     """Public API end to end: upload (H2D) + Run(steps) + read back (D2H)."""
-    e = capi.Engine(device=device, pb=pb, tp=tp)
+    e = new_engine(capi, device=device, pb=pb, tp=tp)
     e.run(0)
     n = len(pos4)
     t = time.perf_counter()
@@ -273,7 +288,7 @@ def batched(capi, device, pb, tp, steps, seed=0):
     Ts = np.exp(np.linspace(np.log(0.45), np.log(2.0), R))
     params = ka_params()
     confs = [I.ka_config(int(n), T=float(T), seed=seed + k) for k, (n, T) in enumerate(zip(ns, Ts))]
-    e = capi.Engine(device=device, max_particles=int(ns.sum() + 64 * R), max_replicas=R, pb=pb, tp=tp)
+    e = new_engine(capi, device=device, max_particles=int(ns.sum() + 64 * R), max_replicas=R, pb=pb, tp=tp)
     ids = [e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(T), tau=TAU,
                  vel4=c["vel4"]) for c, T in zip(confs, Ts)]
     e.run(500)
@@ -284,7 +299,7 @@ def batched(capi, device, pb, tp, steps, seed=0):
     t_seq, ps_seq = 0.0, 0.0
     for k in sample:
         c = confs[k]
-        s = capi.Engine(device=device, pb=pb, tp=tp)
+        s = new_engine(capi, device=device, pb=pb, tp=tp)
         s.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(Ts[k]), tau=TAU, vel4=c["vel4"])
         s.run(500)
         t_seq += time_run(capi, s, steps, device)
@@ -297,10 +312,15 @@ def batched(capi, device, pb, tp, steps, seed=0):
             "speedup_vs_sequential": rate_b / rate_s}
 
 
-def config_block(args, world):
+def config_block(args, world, engine=None):
+    variants = {}
+    if engine is not None:
+        from rumd_b200 import capi
+        variants = {"force_mode": engine.get_variant(capi.VARIANT_FORCE_MODE),
+                    "build_lanes": engine.get_variant(capi.VARIANT_BUILD_LANES)}
     return {"workload": f"Kob-Andersen 80:20 LJ, N={N_PLAIN}, rho=1.2, T=0.45, NVT tau=0.2, dt=0.005, skin 0.3, "
                         "SF cut-off 2.5 sigma_ij (plain method, single large system)",
-            "n_particles": N_PLAIN, "pb": args.pb, "tp": args.tp,
+            "n_particles": N_PLAIN, "pb": args.pb, "tp": args.tp, **variants,
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "precision": "FP32 forces, FP64 reductions/thermostat, int32 images",
             "l2_policy": "L2 flushed (512 MiB write) before the timed Run; inside a Run every step reads the "
@@ -348,6 +368,8 @@ def main():
     dist = Dist(world, local)
     from rumd_b200 import capi
     capi.lib()
+    KERNEL_VARIANTS[capi.VARIANT_FORCE_MODE] = args.force_mode
+    KERNEL_VARIANTS[capi.VARIANT_BUILD_LANES] = args.build_lanes
     device = local
     if args.profile_launches:
         # Same workload driven with eager launches only (b2md_run_timed): the
@@ -355,7 +377,7 @@ def main():
         # launches (it stalls on graphs with conditional nodes).
         from rumd_b200 import initconf as I
         c = I.ka_config(N_PLAIN, density=KA_DENSITY, T=2.0, seed=1)
-        e = capi.Engine(device=device, pb=args.pb, tp=args.tp)
+        e = new_engine(capi, device=device, pb=args.pb, tp=args.tp)
         rid = e.add(c["pos4"], c["box"], ka_params(), 2, cutoff="SF", skin=SKIN, dt=DT, T=2.0, tau=TAU,
                     vel4=c["vel4"])
         e.run_timed(600)
@@ -403,6 +425,8 @@ def main():
                 "bytes_per_launch_alg": bytes_alg, "mean_list_length": st2["mean_nbrs"],
                 "step_share_of_run": per_launch_s * args.steps / t}
     extra = {}
+    cfg = config_block(args, world, e)
+    per_rebuild = 10 if cfg.get("force_mode") == capi.FORCE_WINDOW else 9
     if rank == 0:
         pos4, vel4, im3 = e.get(rid, "pos", N_PLAIN), e.get(rid, "vel", N_PLAIN), e.get(rid, "images", N_PLAIN)
         e2e = e2e_run(capi, device, args.pb, args.tp, pos4, vel4, im3, box, params, args.steps)
@@ -416,8 +440,8 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded FCC start, melted and equilibrated untimed)",
-                "config": config_block(args, world), "clocks": clk, "e2e": e2e,
-                "gpu_launches": launches_in_run(args.steps, rebuilds), "rebuilds": rebuilds,
+                "config": cfg, "clocks": clk, "e2e": e2e,
+                "gpu_launches": launches_in_run(args.steps, rebuilds, per_rebuild), "rebuilds": rebuilds,
                 "roofline": roofline}
         line.update(extra)
         print(json.dumps(line), flush=True)

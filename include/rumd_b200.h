@@ -73,7 +73,9 @@ extern "C" {
 #define B2MD_STAT_MAX_NBRS 10   /* list capacity per particle                   */
 #define B2MD_STAT_ACTUAL_MAX_NBRS 11 /* largest neighbour count of the last build */
 #define B2MD_STAT_MEAN_NBRS 12  /* mean neighbour-list length of the last build  */
-#define B2MD_NSTAT 13
+#define B2MD_STAT_WINDOW_TILES 13 /* tiles with a position window (force mode 2)  */
+#define B2MD_STAT_TILES 14      /* tiles (blocks) of the replica                 */
+#define B2MD_NSTAT 15
 
 typedef struct b2md_engine b2md_engine;
 
@@ -119,15 +121,34 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
 /* Kernel variants, picked by the autotuner next to pb and tp (the analogue of
  * the kernel plan that Autotune.py tunes).  Every variant gives the same
  * neighbour lists and forces bit for bit.
- *   B2MD_VARIANT_FORCE_STAGED  1: the force kernel copies its tile's list rows
- *                              to shared memory (TMA bulk copies) first;
- *                              0: it streams them from global memory.
- *   B2MD_VARIANT_BUILD_LANES   lanes per particle in the list build: 1,2,4,8.
+ *   B2MD_VARIANT_FORCE_MODE    how the force kernel reads neighbours:
+ *                              0 list entries and positions from global
+ *                                memory inside the loop (streamed);
+ *                              1 the tile's list rows first copied to shared
+ *                                memory (TMA bulk copies);
+ *                              2 the tile's position window -- every slot
+ *                                segment holding a listed neighbour of the
+ *                                tile, made with the list -- copied to shared
+ *                                memory (one TMA bulk copy per segment), with
+ *                                a 16-bit list of window offsets.
+ *   B2MD_VARIANT_BUILD_LANES   lanes per particle in the list build: 1,2,4,8;
+ *                              32: one warp per cell, the cell's candidates
+ *                              staged in shared memory and shared by its
+ *                              particles (with force mode 2 the lane build
+ *                              runs instead, with min(8, 512/pb) lanes).
  *   B2MD_VARIANT_BUILD_SMEM    1: the list build assembles a tile's list in
  *                              shared memory and writes it with bulk stores;
  *                              0: it stores entries straight to the list.
+ *   B2MD_VARIANT_WINDOW_CAP    mode 2: window capacity in particles (shared
+ *                              memory of the force kernel, 16 bytes each);
+ *                              tiles with larger windows stream.
  * No reference counterpart beyond Sample::SetPB_TP (Sample.h:96). */
-enum { B2MD_VARIANT_FORCE_STAGED = 0, B2MD_VARIANT_BUILD_LANES = 1, B2MD_VARIANT_BUILD_SMEM = 2 };
+enum {
+  B2MD_VARIANT_FORCE_MODE = 0,
+  B2MD_VARIANT_BUILD_LANES = 1,
+  B2MD_VARIANT_BUILD_SMEM = 2,
+  B2MD_VARIANT_WINDOW_CAP = 3
+};
 B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
 B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);
 

@@ -8,8 +8,10 @@ knobs are the engine's:
   tp   threads per particle: 1, 2, 4, 8   (pb*tp <= 512)
   skin neighbour-list skin, i.e. the rebuild cadence: 0.2 .. 0.5
 and, in a second stage at the winning shape, the kernel variants
-  force_staged  list tile staged in shared memory (1) or streamed (0)
-  build_lanes   lanes per particle in the list build: 1, 2, 4, 8
+  force_mode    neighbours streamed (0), list tile staged (1) or position
+                window staged (2) in shared memory
+  build_lanes   lanes per particle in the list build: 1, 2, 4, 8, or 32 (one
+                warp per cell)
 Each candidate is timed on the device (CUDA events around a short run of the
 real workload, after a warm-up run).  As in RUMD's test mode
 (Autotune.py:929-937), every candidate's potential energy after its run must
@@ -24,7 +26,7 @@ import os
 DEFAULT_PB = (32, 64, 128)
 DEFAULT_TP = (1, 2, 4, 8)
 DEFAULT_SKIN = (0.2, 0.3, 0.4, 0.5)
-VARIANTS = tuple(itertools.product((0, 1), (1, 2, 4, 8)))  # (force_staged, build_lanes)
+VARIANTS = tuple(itertools.product((0, 1, 2), (1, 2, 4, 8, 32)))  # (force_mode, build_lanes)
 
 
 def candidates(pbs=DEFAULT_PB, tps=DEFAULT_TP, skins=DEFAULT_SKIN, max_block=512):
@@ -52,18 +54,18 @@ def search(cands, measure, pe_tol=0.005):
 
 def search_variants(shape, measure, variants=VARIANTS, pe_tol=0.005):
     """Second stage: the kernel variants at a fixed (pb, tp, skin).
-    measure(pb, tp, skin, force_staged=, build_lanes=) -> (rate, pe)."""
+    measure(pb, tp, skin, force_mode=, build_lanes=) -> (rate, pe)."""
     table = []
     ref_pe = None
     best = None
     for fs, bl in variants:
-        rate, pe = measure(shape["pb"], shape["tp"], shape["skin"], force_staged=fs, build_lanes=bl)
+        rate, pe = measure(shape["pb"], shape["tp"], shape["skin"], force_mode=fs, build_lanes=bl)
         ok = True
         if ref_pe is None:
             ref_pe = pe
         elif abs(pe - ref_pe) > pe_tol:
             ok = False
-        table.append({"force_staged": fs, "build_lanes": bl, "rate": rate, "pe": pe, "ok": ok})
+        table.append({"force_mode": fs, "build_lanes": bl, "rate": rate, "pe": pe, "ok": ok})
         if ok and (best is None or rate > best["rate"]):
             best = table[-1]
     return best, table
@@ -73,8 +75,8 @@ def apply(engine, entry):
     """Sets a tuned entry's launch shape and kernel variants on an engine."""
     from . import capi
     engine.set_launch(entry["pb"], entry["tp"])
-    if "force_staged" in entry:
-        engine.set_variant(capi.VARIANT_FORCE_STAGED, entry["force_staged"])
+    if "force_mode" in entry:
+        engine.set_variant(capi.VARIANT_FORCE_MODE, entry["force_mode"])
         engine.set_variant(capi.VARIANT_BUILD_LANES, entry["build_lanes"])
 
 
@@ -98,7 +100,7 @@ class Autotune:
     def tune(self, replicas, measure, force=False, variants=False):
         """Stage 1 over (pb, tp, skin); with variants=True, stage 2 over the
         kernel variants at the winning shape (measure then takes
-        force_staged= and build_lanes= keywords)."""
+        force_mode= and build_lanes= keywords)."""
         key = signature(replicas)
         cache = self._load()
         if key in cache and not force:
@@ -107,7 +109,7 @@ class Autotune:
         entry = {"pb": best["pb"], "tp": best["tp"], "skin": best["skin"], "rate": best["rate"], "table": table}
         if variants:
             vbest, vtable = search_variants(entry, measure)
-            entry.update(force_staged=vbest["force_staged"], build_lanes=vbest["build_lanes"],
+            entry.update(force_mode=vbest["force_mode"], build_lanes=vbest["build_lanes"],
                          rate=max(entry["rate"], vbest["rate"]), variant_table=vtable)
         cache[key] = entry
         with open(self.cache_path, "w") as fh:
@@ -138,10 +140,10 @@ def device_measure(capi, replicas, device=0, steps=300, warmup=100):
     replicas: list of dicts with pos4, vel4, box, params, ntypes, T, n, density."""
     import torch
 
-    def measure(pb, tp, skin, force_staged=None, build_lanes=None):
+    def measure(pb, tp, skin, force_mode=None, build_lanes=None):
         e = capi.Engine(device=device, max_replicas=len(replicas), pb=pb, tp=tp)
-        if force_staged is not None:
-            e.set_variant(capi.VARIANT_FORCE_STAGED, force_staged)
+        if force_mode is not None:
+            e.set_variant(capi.VARIANT_FORCE_MODE, force_mode)
         if build_lanes is not None:
             e.set_variant(capi.VARIANT_BUILD_LANES, build_lanes)
         ids = [e.add(r["pos4"], r["box"], r["params"], r["ntypes"], cutoff="SF", skin=skin, T=r["T"],
@@ -188,9 +190,9 @@ def main(argv=None):
         print(f"pb={r['pb']:4d} tp={r['tp']} skin={r['skin']:.2f}  {r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
     for r in best.get("variant_table", []):
-        print(f"force_staged={r['force_staged']} build_lanes={r['build_lanes']}  {r['rate']:.4e} particle-steps/s  "
+        print(f"force_mode={r['force_mode']} build_lanes={r['build_lanes']}  {r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
-    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate", "force_staged", "build_lanes") if k in best}))
+    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate", "force_mode", "build_lanes") if k in best}))
 
 
 if __name__ == "__main__":

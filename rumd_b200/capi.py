@@ -17,10 +17,11 @@ LIB_PATH = os.path.join(_HERE, "librumd_b200.so")
 B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_OVERFLOW = range(6)
 CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
 # kernel variants (b2md_engine_set_variant)
-VARIANT_FORCE_STAGED, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM = 0, 1, 2
+VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP = 0, 1, 2, 3
+FORCE_STREAMED, FORCE_STAGED, FORCE_WINDOW = 0, 1, 2
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",
-              "target_T", "max_nbrs", "actual_max_nbrs", "mean_nbrs"]
+              "target_T", "max_nbrs", "actual_max_nbrs", "mean_nbrs", "window_tiles", "tiles"]
 NSTAT = len(STAT_NAMES)
 NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
 
@@ -189,7 +190,7 @@ class Engine:
         check(lib().b2md_engine_set_graph_mode(self._h, int(bool(conditional))))
 
     def set_variant(self, which, value):
-        """which: VARIANT_FORCE_STAGED, VARIANT_BUILD_LANES or VARIANT_BUILD_SMEM."""
+        """which: VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM or VARIANT_WINDOW_CAP."""
         check(lib().b2md_engine_set_variant(self._h, int(which), int(value)))
 
     def get_variant(self, which):

@@ -129,7 +129,8 @@ struct b2md_engine {
   long long pcap = 0, ecap = 0, ccap = 0, qcap = 0, zcap = 0;
   int rcap = 0;
   // kernel variants (b2md_engine_set_variant)
-  bool force_staged = false;  // force kernel: list tile staged in shared memory
+  int force_mode = 0;          // force kernel: FM_STREAMED, FM_STAGED or FM_WINDOW
+  int win_cap = 2560;          // FM_WINDOW: window capacity in particles
   int build_lanes = 2;         // list build: lanes per particle
   bool build_smem = false;     // list build: tile assembled in shared memory
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
@@ -141,6 +142,7 @@ struct b2md_engine {
   unsigned *nn = nullptr, *order = nullptr;
   int *key = nullptr, *slot = nullptr;
   unsigned* nbl = nullptr;
+  unsigned short* wl = nullptr;  // window list (same layout as nbl)
   int *cnt = nullptr, *cstart = nullptr;
   float* par = nullptr;
   double* elog = nullptr;
@@ -150,6 +152,8 @@ struct b2md_engine {
   // tiles
   int ntiles = 0, tcap = 0, ngroups = 0, gcap = 0;
   int *tile_rep = nullptr, *tile_first = nullptr, *ctot = nullptr, *cpref = nullptr;
+  int4* wseg = nullptr;  // per-tile window segments
+  int2* wmeta = nullptr;  // per-tile (segments, particles)
   double *tpart = nullptr, *gpart = nullptr;
   unsigned* gctr = nullptr;
   unsigned* fctr = nullptr;
@@ -166,6 +170,8 @@ namespace {
 
 constexpr int kChunk = 32;
 constexpr int kMaxDynSmemBytes = 220 * 1024;  // dynamic shared memory a list-tile kernel may use
+// largest position window: fits the shared memory, and 16-bit window offsets
+constexpr int kMaxWindow = (kMaxDynSmemBytes - (int)(kParSmemFloats * sizeof(float))) / (int)sizeof(float4);
 
 template <class T>
 void dev_grow(b2md_engine* e, T*& p, long long old_n, long long new_n, bool zero_new) {
@@ -219,6 +225,7 @@ void grow_list(b2md_engine* e, long long need) {
   if (need <= e->ecap) return;
   long long nc = std::max(need, e->ecap + e->ecap / 2);
   dev_grow(e, e->nbl, e->ecap, nc, false);
+  dev_grow(e, e->wl, e->ecap, nc, false);
   e->ealloc.grow(nc);
   e->ecap = nc;
   invalidate_graphs(e);
@@ -278,18 +285,33 @@ EngArgs make_args(b2md_engine* e) {
   a.idx_rows = 0;
   for (auto& h : e->reps)
     if (h.active) a.idx_rows = std::max(a.idx_rows, h.d.max_nbrs);
+  a.wl = e->wl;
+  a.wseg = e->wseg;
+  a.wmeta = e->wmeta;
+  a.win_on = e->force_mode == FM_WINDOW ? 1 : 0;
+  a.win_cap = e->win_cap;
   return a;
 }
 
-// Dynamic shared memory of k_force: pair table [+ staged list tile].
-size_t force_smem(const EngArgs& a, bool staged) {
-  return (size_t)kParSmemFloats * sizeof(float) + (staged ? (size_t)a.idx_rows * a.idx_pitch * sizeof(unsigned) : 0);
+// Dynamic shared memory of k_force: pair table [+ staged list tile | position window].
+size_t force_smem(const EngArgs& a, int mode) {
+  size_t extra = 0;
+  if (mode == FM_STAGED) extra = (size_t)a.idx_rows * a.idx_pitch * sizeof(unsigned);
+  if (mode == FM_WINDOW) extra = (size_t)a.win_cap * sizeof(float4);
+  return (size_t)kParSmemFloats * sizeof(float) + extra;
 }
 
-// Dynamic shared memory of k_rb_build: cut-off table [+ list tile].
+// Dynamic shared memory of k_rb_build: cut-off table [+ list tile] [+ window scratch].
 size_t build_smem(const b2md_engine* e, const EngArgs& a) {
   const int pb = e->pb;
-  return (size_t)kCs2Floats * sizeof(float) + (e->build_smem ? (size_t)a.idx_rows * (pb + 4) * sizeof(unsigned) : 0);
+  return (size_t)kCs2Floats * sizeof(float) + (e->build_smem ? (size_t)a.idx_rows * (pb + 4) * sizeof(unsigned) : 0) +
+         (a.win_on ? sizeof(WinTable) : 0);
+}
+
+// Marks every tile as having no position window (k_force then streams its
+// neighbours) until the next list build makes them.
+void drop_windows(b2md_engine* e) {
+  if (e->wmeta && e->tcap > 0) CK(cudaMemsetAsync(e->wmeta, 0xff, (size_t)e->tcap * sizeof(int2), e->stream));
 }
 
 // Re-lays out tiles and reduction groups over the active replicas and uploads
@@ -312,6 +334,8 @@ void relayout(b2md_engine* e) {
     dev_grow(e, e->ctot, e->tcap, nc, true);
     dev_grow(e, e->cpref, e->tcap, nc, true);
     dev_grow(e, e->tpart, (long long)e->tcap * kNPart, (long long)nc * kNPart, true);
+    dev_grow(e, e->wseg, (long long)e->tcap * kWinSeg, (long long)nc * kWinSeg, false);
+    dev_grow(e, e->wmeta, e->tcap, nc, false);
     e->tcap = nc;
   }
   if (G > e->gcap) {
@@ -339,6 +363,7 @@ void relayout(b2md_engine* e) {
   CK(cudaStreamSynchronize(e->stream));
   e->ntiles = T;
   e->ngroups = G;
+  drop_windows(e);  // tiles changed: no window until the next list build
   invalidate_graphs(e);
 }
 
@@ -483,6 +508,7 @@ void place_list(b2md_engine* e, HostRep& h, int max_nbrs) {
   h.d.nbl0 = off;
   h.d.max_nbrs = max_nbrs;
   h.d.nbl_stride = h.np;
+  drop_windows(e);  // window list entries live at the old place
 }
 
 // ---- launches ----
@@ -498,17 +524,29 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   k_rb_scatter<<<T, e->pb, 0, s>>>(a);
   k_rb_fix<<<T, e->pb, 0, s>>>(a);
   k_rb_permute<<<T, e->pb, 0, s>>>(a);
+  if (a.win_on) k_rb_window<<<T, e->pb, sizeof(WinScratch), s>>>(a);
   // list build: build_lanes lanes per particle (fewer when pb*lanes would
   // exceed a block), the list either assembled in shared memory or stored
   // straight to global memory
+  if (e->build_lanes == 32 && !a.win_on) {
+    // one warp per cell, candidates staged in shared memory
+    const size_t cw = (size_t)kCs2Floats * sizeof(float) + (size_t)kCwWarps * kCwCand * (sizeof(float4) + sizeof(int));
+    k_rb_build_cw<<<T, kCwWarps * 32, cw, s>>>(a);
+    return;
+  }
   const size_t smem = build_smem(e, a);
   if (smem > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
   const int lanes = std::min(e->build_lanes, kMaxBlock / e->pb);
 #define LB(LPV)                                                                    \
   if (lanes >= LPV) {                                                              \
-    if (e->build_smem) k_rb_build<LPV, true><<<T, e->pb * LPV, smem, s>>>(a);     \
-    else k_rb_build<LPV, false><<<T, e->pb * LPV, smem, s>>>(a);                  \
+    if (a.win_on) {                                                                \
+      if (e->build_smem) k_rb_build<LPV, true, true><<<T, e->pb * LPV, smem, s>>>(a); \
+      else k_rb_build<LPV, false, true><<<T, e->pb * LPV, smem, s>>>(a);             \
+    } else {                                                                       \
+      if (e->build_smem) k_rb_build<LPV, true, false><<<T, e->pb * LPV, smem, s>>>(a); \
+      else k_rb_build<LPV, false, false><<<T, e->pb * LPV, smem, s>>>(a);             \
+    }                                                                              \
     return;                                                                        \
   }
   LB(8) LB(4) LB(2) LB(1)
@@ -517,27 +555,29 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
 
 typedef void (*ForceFn)(EngArgs, int, cudaGraphConditionalHandle);
 
-template <bool STAGED>
+template <int MODE>
 ForceFn force_fn_var(int tp, bool fused, bool stress) {
-#define SEL(TPV)                                                                          \
-  if (tp == TPV) {                                                                        \
-    if (fused) return k_force<TPV, true, false, STAGED>;                                  \
-    return stress ? k_force<TPV, false, true, STAGED> : k_force<TPV, false, false, STAGED>; \
+#define SEL(TPV)                                                                      \
+  if (tp == TPV) {                                                                    \
+    if (fused) return k_force<TPV, true, false, MODE>;                                \
+    return stress ? k_force<TPV, false, true, MODE> : k_force<TPV, false, false, MODE>; \
   }
   SEL(1) SEL(2) SEL(4) SEL(8)
 #undef SEL
   return nullptr;
 }
 
-ForceFn force_fn_raw(int tp, bool fused, bool stress, bool staged) {
-  return staged ? force_fn_var<true>(tp, fused, stress) : force_fn_var<false>(tp, fused, stress);
+ForceFn force_fn_raw(int tp, bool fused, bool stress, int mode) {
+  if (mode == FM_STAGED) return force_fn_var<FM_STAGED>(tp, fused, stress);
+  if (mode == FM_WINDOW) return force_fn_var<FM_WINDOW>(tp, fused, stress);
+  return force_fn_var<FM_STREAMED>(tp, fused, stress);
 }
 
 // The force kernel for (tp, fused, stress), allowed to use the dynamic
 // shared memory the staged list tile `a` needs.
 ForceFn force_fn(const b2md_engine* e, bool fused, bool stress, const EngArgs& a) {
-  ForceFn fn = force_fn_raw(e->tp, fused, stress, e->force_staged);
-  if (force_smem(a, e->force_staged) > kMaxDynSmemBytes)
+  ForceFn fn = force_fn_raw(e->tp, fused, stress, e->force_mode);
+  if (force_smem(a, e->force_mode) > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
   return fn;
 }
@@ -548,21 +588,30 @@ void init_func_attrs(int device) {
   static unsigned long long done_mask = 0ull;  // one bit per device
   const unsigned long long bit = 1ull << (device & 63);
   if (done_mask & bit) return;
-  const void* builds[] = {(const void*)k_rb_build<1, true>, (const void*)k_rb_build<2, true>,
-                          (const void*)k_rb_build<4, true>, (const void*)k_rb_build<8, true>};
+  const void* builds[] = {
+      (const void*)k_rb_build<1, true, false>,  (const void*)k_rb_build<2, true, false>,
+      (const void*)k_rb_build<4, true, false>,  (const void*)k_rb_build<8, true, false>,
+      (const void*)k_rb_build<1, false, false>, (const void*)k_rb_build<2, false, false>,
+      (const void*)k_rb_build<4, false, false>, (const void*)k_rb_build<8, false, false>,
+      (const void*)k_rb_build<1, true, true>,   (const void*)k_rb_build<2, true, true>,
+      (const void*)k_rb_build<4, true, true>,   (const void*)k_rb_build<8, true, true>,
+      (const void*)k_rb_build<1, false, true>,  (const void*)k_rb_build<2, false, true>,
+      (const void*)k_rb_build<4, false, true>,  (const void*)k_rb_build<8, false, true>};
   for (const void* f : builds)
     CK(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
-  for (int tp : {1, 2, 4, 8})
-    for (int v = 0; v < 3; ++v)
-      CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2, true),
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
+  CK(cudaFuncSetAttribute((const void*)k_rb_build_cw, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
+  for (int mode : {FM_STAGED, FM_WINDOW})
+    for (int tp : {1, 2, 4, 8})
+      for (int v = 0; v < 3; ++v)
+        CK(cudaFuncSetAttribute((const void*)force_fn_raw(tp, v == 0, v == 2, mode),
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemBytes));
   done_mask |= bit;
 }
 
 void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
   if (e->ntiles == 0) return;
   ForceFn fn = force_fn(e, fused, stress, a);
-  fn<<<e->ntiles, e->pb * e->tp, force_smem(a, e->force_staged), s>>>(a, 0, cudaGraphConditionalHandle{});
+  fn<<<e->ntiles, e->pb * e->tp, force_smem(a, e->force_mode), s>>>(a, 0, cudaGraphConditionalHandle{});
 }
 
 void check_launch() { CK(cudaGetLastError()); }
@@ -572,7 +621,7 @@ void build_graph(b2md_engine* e, int which, int K) {
   EngArgs a = make_args(e);
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
-  const size_t smem = force_smem(a, e->force_staged);
+  const size_t smem = force_smem(a, e->force_mode);
   ForceFn fstep = force_fn(e, true, false, a);
   if (e->cond_mode) {
     std::vector<cudaGraphConditionalHandle> hs(K);
@@ -796,7 +845,7 @@ int b2md_engine_destroy(b2md_engine* e) {
   void* ptrs[] = {e->r[0], e->r[1], e->v[0], e->v[1], e->im[0], e->im[1], e->uidx[0], e->uidx[1], e->f, e->w,
                   e->sts, e->last_r, e->nn, e->order, e->key, e->slot, e->nbl, e->cnt, e->cstart, e->par, e->elog,
                   e->rep, e->st, e->rctr, e->tile_rep, e->tile_first, e->ctot, e->cpref, e->tpart, e->gpart,
-                  e->gctr, e->fctr, e->any_rebuild};
+                  e->gctr, e->fctr, e->any_rebuild, e->wl, e->wseg, e->wmeta};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -834,13 +883,27 @@ int b2md_engine_set_graph_mode(b2md_engine* e, int conditional) {
 int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
   if (!e) return fail(B2MD_ERR_ARG, "null engine");
   switch (which) {
-    case B2MD_VARIANT_FORCE_STAGED:
-      if (value != 0 && value != 1) return fail(B2MD_ERR_ARG, "force_staged must be 0 or 1");
-      e->force_staged = value != 0;
+    case B2MD_VARIANT_FORCE_MODE:
+      if (value < FM_STREAMED || value > FM_WINDOW) return fail(B2MD_ERR_ARG, "force mode must be 0, 1 or 2");
+      if (value == FM_WINDOW && e->force_mode != FM_WINDOW) {
+        // windows of earlier builds may be stale: none until the next list build
+        int rc = guarded([&] { drop_windows(e); });
+        if (rc) return rc;
+      }
+      e->force_mode = value;
+      break;
+    case B2MD_VARIANT_WINDOW_CAP:
+      if (value < 256 || value > kMaxWindow)
+        return fail(B2MD_ERR_ARG, "window capacity must be 256..%d particles (got %d)", kMaxWindow, value);
+      if (value != e->win_cap) {
+        int rc = guarded([&] { drop_windows(e); });
+        if (rc) return rc;
+      }
+      e->win_cap = value;
       break;
     case B2MD_VARIANT_BUILD_LANES:
-      if (value != 1 && value != 2 && value != 4 && value != 8)
-        return fail(B2MD_ERR_ARG, "build lanes must be 1, 2, 4 or 8 (got %d)", value);
+      if (value != 1 && value != 2 && value != 4 && value != 8 && value != 32)
+        return fail(B2MD_ERR_ARG, "build lanes must be 1, 2, 4, 8 or 32 (one warp per cell) (got %d)", value);
       e->build_lanes = value;
       break;
     case B2MD_VARIANT_BUILD_SMEM:
@@ -857,7 +920,8 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
 int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
   if (!e || !value) return fail(B2MD_ERR_ARG, "null argument");
   switch (which) {
-    case B2MD_VARIANT_FORCE_STAGED: *value = e->force_staged ? 1 : 0; break;
+    case B2MD_VARIANT_FORCE_MODE: *value = e->force_mode; break;
+    case B2MD_VARIANT_WINDOW_CAP: *value = e->win_cap; break;
     case B2MD_VARIANT_BUILD_LANES: *value = e->build_lanes; break;
     case B2MD_VARIANT_BUILD_SMEM: *value = e->build_smem ? 1 : 0; break;
     default: return fail(B2MD_ERR_ARG, "unknown variant %d", which);
@@ -1157,6 +1221,17 @@ int b2md_replica_stats(b2md_engine* e, int id, double* out) {
     double tot = 0;
     for (unsigned c : nn) tot += c;
     out[B2MD_STAT_MEAN_NBRS] = tot / h.n;
+    // tiles whose neighbours k_force reads from a position window
+    int wt = 0;
+    if (e->force_mode == FM_WINDOW && h.d.ntiles > 0) {
+      std::vector<int2> wm(h.d.ntiles);
+      CK(cudaMemcpyAsync(wm.data(), e->wmeta + h.d.tile0, h.d.ntiles * sizeof(int2), cudaMemcpyDeviceToHost,
+                         e->stream));
+      CK(cudaStreamSynchronize(e->stream));
+      for (const int2& m : wm) wt += m.x >= 0;
+    }
+    out[B2MD_STAT_WINDOW_TILES] = wt;
+    out[B2MD_STAT_TILES] = h.d.ntiles;
   });
 }
 
@@ -1305,7 +1380,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     long long nl = 2;
-    const size_t smem = force_smem(a, e->force_staged);
+    const size_t smem = force_smem(a, e->force_mode);
     ForceFn fstep = force_fn(e, true, false, a);
     std::vector<cudaEvent_t> ev(2 * nsteps);
     for (auto& x : ev) CK(cudaEventCreate(&x));
@@ -1319,7 +1394,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
       CK(cudaStreamSynchronize(e->stream));
       if (*h_any) {
         launch_rebuild(e, e->stream, a);
-        nl += 9;
+        nl += e->force_mode == FM_WINDOW ? 10 : 9;
       }
       CK(cudaEventRecord(ev[2 * k], e->stream));
       fstep<<<e->ntiles, e->pb * e->tp, smem, e->stream>>>(a, 0, cudaGraphConditionalHandle{});
@@ -1340,7 +1415,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     calc_f(e, false);
     CK(cudaStreamSynchronize(e->stream));
     *step_kernel_ms = tot;
-    *launches = nl + 10;
+    *launches = nl + (e->force_mode == FM_WINDOW ? 11 : 10);
   });
 }
 

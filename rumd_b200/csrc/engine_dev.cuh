@@ -9,7 +9,13 @@
 //     f, w, sts float4 as RUMD (ParticleData.h:41-46); last_r float4; nn uint
 //   list pool: nbl[nbl0 + k*stride + slot]  (column-major per replica, like RUMD's
 //     nbl[k*nvp + i], NeighborList.cu:1293, so a warp's k-th entries are one sector run)
+//   window list: wl[nbl0 + k*stride + slot] (uint16), the same entries as nbl
+//     written as offsets into the tile's position window (see below)
 //   cell pools: cnt[cell0 + c], start[cell0 + c] (chunk-local exclusive prefix)
+//   per-tile position window: wseg[tile*kWinSeg + s] = (first slot, length,
+//     window offset, 0) for the slot segments that hold every listed
+//     neighbour of the tile's particles, sorted by slot; wmeta[tile] =
+//     (segments, window particles), or (-1, -1) when the tile has none.
 //   per-tile / per-group FP64 partial sums for deterministic two-level reductions.
 //
 // A "tile" is pb consecutive slots of one replica; one CUDA block processes one
@@ -27,6 +33,8 @@ constexpr int kNumParam = 12;   // RUMD NumParam (rumd_base.h)
 constexpr int kNPart = 8;       // FP64 partial sums per tile
 constexpr int kGroup = 32;      // tiles per reduction group
 constexpr int kMaxBlock = 512;  // pb*tp limit (launch bounds)
+constexpr int kWinSeg = 128;    // slot segments per tile position window
+constexpr int kWinBase = 4;     // cell rows (y, z) a tile may span for a window
 
 enum { P_PE = 0, P_W, P_KE2, P_KET, P_PX, P_PY, P_PZ, P_M };
 enum { CUT_NS = 0, CUT_SP = 1, CUT_SF = 2 };
@@ -106,6 +114,11 @@ struct EngArgs {
   int nrep;
   int idx_pitch;  // k_force: shared-memory row pitch of the staged list tile (pb + bank padding)
   int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
+  unsigned short* wl;  // window list (force mode 2)
+  int4* wseg;          // per-tile window segments
+  int2* wmeta;         // per-tile (segments, particles)
+  int win_on;          // list builds also build the windows
+  int win_cap;         // window capacity in particles (shared memory of k_force)
 };
 
 }  // namespace b2md

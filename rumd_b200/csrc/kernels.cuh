@@ -242,6 +242,12 @@ __device__ __forceinline__ unsigned ld_stream(const unsigned* p) {
   return v;
 }
 
+__device__ __forceinline__ unsigned ld_stream_u16(const unsigned short* p) {
+  unsigned short v;
+  asm volatile("ld.global.nc.L1::no_allocate.u16 %0, [%1];" : "=h"(v) : "l"(p));
+  return v;
+}
+
 // List-entry readers for force_loop: entry k of the particle's column.
 // Staged: the tile's list copied to shared memory (row pitch `pitch`).
 struct IdxStaged {
@@ -255,42 +261,85 @@ struct IdxStreamed {
   size_t stride;
   __device__ __forceinline__ unsigned operator()(unsigned k) const { return ld_stream(p + k * stride); }
 };
+// Window: the 16-bit window list (offsets into the tile's position window).
+struct IdxWindow {
+  const unsigned short* p;
+  size_t stride;
+  __device__ __forceinline__ unsigned operator()(unsigned k) const { return ld_stream_u16(p + k * stride); }
+};
+
+// Neighbour-position readers: gathered from global memory (through L1), or
+// from the tile's position window in shared memory.
+struct PosGlobal {
+  const float4* __restrict__ p;
+  __device__ __forceinline__ float4 operator()(unsigned j) const { return __ldg(p + j); }
+};
+struct PosWindow {
+  const float4* p;
+  __device__ __forceinline__ float4 operator()(unsigned j) const { return p[j]; }
+};
+
+// Neighbour positions in flight per thread in force_loop.
+constexpr int kForceUnroll = 4;
 
 // The neighbour loop of one thread: entries k = lane_t, lane_t + TP, ... of
-// the particle's list column, four gathers in flight.
-template <int TP, bool STRESS, bool WRAP, class Idx>
-__device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, unsigned lane_t, unsigned nn,
-                                           const float4* __restrict__ rc, const float4& ri, const float* prow,
-                                           float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
+// the particle's list column, kForceUnroll neighbour positions in flight.
+template <int TP, bool STRESS, bool WRAP, class Idx, class Pos>
+__device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos& pos, unsigned lane_t, unsigned nn,
+                                           const float4& ri, const float* prow, float Lx, float Ly, float Lz,
+                                           float iLx, float iLy, float iLz) {
+  constexpr int U = kForceUnroll;
   unsigned k = lane_t;
-  for (; k + 3 * TP < nn; k += 4 * TP) {
-    const unsigned j0 = idx(k), j1 = idx(k + TP), j2 = idx(k + 2 * TP), j3 = idx(k + 3 * TP);
-    const float4 r0 = __ldg(rc + j0), r1 = __ldg(rc + j1), r2 = __ldg(rc + j2), r3 = __ldg(rc + j3);
-    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+  for (; k + (U - 1) * TP < nn; k += U * TP) {
+    unsigned j[U];
+    float4 rj[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) j[u] = idx(k + u * TP);
+#pragma unroll
+    for (int u = 0; u < U; ++u) rj[u] = pos(j[u]);
+#pragma unroll
+    for (int u = 0; u < U; ++u) lj_pair<STRESS, WRAP>(A, ri, rj[u], prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
   for (; k < nn; k += TP) {
-    const float4 r0 = __ldg(rc + idx(k));
+    const float4 r0 = pos(idx(k));
     lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
 }
 
-// Shared memory of k_force: [packed pair table, kParSmemFloats] [index tile
-// when STAGED]
+template <int TP, bool STRESS, class Idx, class Pos>
+__device__ __forceinline__ void force_loop_any(bool fast, PairAcc& A, const Idx& idx, const Pos& pos,
+                                               unsigned lane_t, unsigned nn, const float4& ri, const float* prow,
+                                               float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
+  if (fast)
+    force_loop<TP, STRESS, false>(A, idx, pos, lane_t, nn, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+  else
+    force_loop<TP, STRESS, true>(A, idx, pos, lane_t, nn, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+}
+
+// Shared memory of k_force: [packed pair table, kParSmemFloats]
+// [MODE 1: list tile | MODE 2: position window, win_cap float4]
 constexpr int kParSmemFloats = kMaxTypes * kMaxTypes * kParStride;
 constexpr unsigned kWaitPolls = 1u << 22;
 
-// One tile of pb particles per block, tp threads per particle.
-// STAGED = true copies the tile's list rows to shared memory with TMA bulk
-// copies before the pair loop; STAGED = false streams the list entries from
-// global memory inside the loop and leaves the shared memory to L1.
-template <int TP, bool FUSED, bool STRESS, bool STAGED>
+enum { FM_STREAMED = 0, FM_STAGED = 1, FM_WINDOW = 2 };
+
+// One tile of pb particles per block, tp threads per particle.  MODE selects
+// how the neighbours are read:
+//   FM_STREAMED  list entries and neighbour positions read from global memory
+//                inside the loop (positions through L1);
+//   FM_STAGED    the tile's list rows copied to shared memory first (TMA bulk
+//                copies), positions gathered from global memory;
+//   FM_WINDOW    the tile's position window (every slot segment holding a
+//                listed neighbour of the tile) copied to shared memory with one
+//                TMA bulk copy per segment, and the 16-bit window list read
+//                from global memory: every neighbour position comes from shared
+//                memory.  Tiles without a window (wmeta < 0) stream.
+template <int TP, bool FUSED, bool STRESS, int MODE>
 __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cudaGraphConditionalHandle h) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
+  float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
   __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
   __shared__ double s_scr[kMaxBlock];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
@@ -305,14 +354,20 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     const int pb = blockDim.x / TP;
     const int first = a.tile_first[tile];
     const int pitch = a.idx_pitch;
-    if (STAGED) {
-      // 1. rows of the list this tile needs: the largest neighbour count in it
+    const int rb = S->rbuf;
+    const float4* __restrict__ rc = a.r[rb] + R.p0;
+    const int2 wm = MODE == FM_WINDOW ? a.wmeta[tile] : make_int2(-1, -1);
+    const bool use_bar = MODE == FM_STAGED || (MODE == FM_WINDOW && wm.x >= 0);
+    if (use_bar) {
       if (threadIdx.x == 0) {
         s_rows = 0u;
         mbar_init(&s_bar, 1);
         mbar_fence_init();
       }
       __syncthreads();
+    }
+    if (MODE == FM_STAGED) {
+      // 1. rows of the list this tile needs: the largest neighbour count in it
       {
         unsigned c = (threadIdx.x < pb && first + (int)threadIdx.x < R.n) ? a.nn[R.p0 + first + threadIdx.x] : 0u;
 #pragma unroll
@@ -330,6 +385,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
         for (unsigned r = threadIdx.x; r < rows; r += 32)
           bulk_g2s(s_idx + r * pitch, src + (size_t)r * R.nbl_stride, width * 4u, &s_bar);
       }
+    } else if (MODE == FM_WINDOW && wm.x >= 0) {
+      // 1-2. one TMA bulk copy per window segment (16-byte aligned float4 runs)
+      if (threadIdx.x < 32) {
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, (unsigned)wm.y * 16u);
+        __syncwarp();
+        const int4* seg = a.wseg + (size_t)tile * kWinSeg;
+        for (int sgi = threadIdx.x; sgi < wm.x; sgi += 32) {
+          const int4 sg = seg[sgi];
+          bulk_g2s(s_win + sg.z, rc + sg.x, (unsigned)sg.y * 16u, &s_bar);
+        }
+      }
     }
     // 3. meanwhile: pair table and this particle's data
     const int nt = R.ntypes;
@@ -337,14 +403,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     const int lp = threadIdx.x / TP, lane_t = threadIdx.x % TP;
     const int i = first + lp;
     const bool valid = i < R.n;
-    const int rb = S->rbuf;
-    const float4* __restrict__ rc = a.r[rb] + R.p0;
     const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
     const float4 ri = valid ? rc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const int ti = valid ? __float_as_int(ri.w) : 0;
     const float* prow = s_par + ti * nt * kParStride;
     const unsigned nn = valid ? a.nn[R.p0 + i] : 0u;
+    const size_t lstride = (size_t)R.nbl_stride;
+    const unsigned* lcol = a.nbl + R.nbl0 + i;
+    const unsigned short* wcol = a.wl + R.nbl0 + i;
     // A particle farther than rc_max + 2 skin from every face of the box has
     // all its listed neighbours (within rc + skin at the build, each moved at
     // most skin/2 since) inside the box at their minimum image, so the
@@ -353,15 +420,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     const bool inner = fabsf(ri.x) < R.ilim[0] && fabsf(ri.y) < R.ilim[1] && fabsf(ri.z) < R.ilim[2];
     const bool fast = __all_sync(0xffffffffu, !valid || inner);
     PairAcc A;
-    if (STAGED) {
-      // 4. bounded wait for the index tile (also publishes the pair table)
+    if (use_bar) {
+      // 4. bounded wait for the copies (the barrier also publishes the pair table)
       const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
       if (ok) {
-        const IdxStaged idx{s_idx + lp, pitch};
-        if (fast)
-          force_loop<TP, STRESS, false>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+        if (MODE == FM_STAGED)
+          force_loop_any<TP, STRESS>(fast, A, IdxStaged{s_idx + lp, pitch}, PosGlobal{rc}, lane_t, nn, ri, prow,
+                                     Lx, Ly, Lz, iLx, iLy, iLz);
         else
-          force_loop<TP, STRESS, true>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+          force_loop_any<TP, STRESS>(fast, A, IdxWindow{wcol, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
+                                     Lx, Ly, Lz, iLx, iLy, iLz);
       } else {
         // the copies did not land in time: record it for the host and wait
         // (bounded) for them before this block's shared memory is released
@@ -370,13 +438,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     } else {
       __syncthreads();  // the pair table
-      const IdxStreamed idx{a.nbl + R.nbl0 + i, (size_t)R.nbl_stride};
-      if (fast)
-        force_loop<TP, STRESS, false>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-      else
-        force_loop<TP, STRESS, true>(A, idx, lane_t, nn, rc, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+      force_loop_any<TP, STRESS>(fast, A, IdxStreamed{lcol, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
+                                 Lz, iLx, iLy, iLz);
     }
-
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
     float sxx = A.sxx, syy = A.syy, szz = A.szz, syz = A.syz, sxz = A.sxz, sxy = A.sxy;
     if (TP > 1) {
@@ -760,14 +824,247 @@ __global__ void k_rb_permute(EngArgs a) {
 //     column-major row of the tile is one contiguous slot run).
 constexpr int kCs2Floats = kMaxTypes * kMaxTypes;
 
+// Position window of a tile (built with the list, read by k_force FM_WINDOW).
+// The tile's particles are consecutive in cell-key order, so they lie in at
+// most a few cell rows (y, z) -- its base rows -- each over an x-interval
+// [xa, xb] of cells.  Every listed neighbour of a particle lies in the 25 rows
+// (y+dy, z+dz), |dy|,|dz| <= 2, at x-cells within 2 of its own.  The window is
+// the union, per neighbour row, of the x-intervals [xa-2, xb+2] (modulo the
+// row length): a few slot segments (cells of one row are consecutive keys,
+// hence consecutive slots).  Segments are kept sorted by first slot and
+// numbered into the window in that order; a list entry j then becomes the
+// window offset j + (offset - first slot) of its segment.
+struct WinScratch {
+  int rowid[kMaxBlock];  // base row y + z*ny of each particle of the tile
+  int cx[kMaxBlock];     // x-cell of each particle
+  int brow[kWinBase], bxa[kWinBase], bxb[kWinBase];
+  int erow[25 * kWinBase];        // neighbour row of entry (base row, dz, dy)
+  int eiv[25 * kWinBase][4];      // its x-cells as <= 2 linear intervals
+  int em[25 * kWinBase];          // merged intervals (row leaders only)
+  int eseg[25 * kWinBase];        // first segment number of a leader
+  int ems[25 * kWinBase][8];      // <= 4 merged intervals [c0, c1)
+  int ustart[kWinSeg], ulen[kWinSeg];
+  int sstart[kWinSeg], slen[kWinSeg], soff[kWinSeg];
+  int nseg, W;  // nseg < 0: the tile has no window
+};
+
+// Builds the tile's window into w (and wseg / wmeta).  Called by the whole
+// block after rowid / cx of its np particles are written; warp 0 works.
+__device__ void tile_window(const EngArgs& a, const RepDev& R, int tile, int np, WinScratch* w) {
+  if (threadIdx.x >= 32) return;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x;
+  const unsigned lt = (1u << lane) - 1u;
+  const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
+  bool bad = false;
+  // W1: base rows = runs of equal rowid (x rises within a run)
+  int nb = 0, nend = 0;
+  for (int c0 = 0; c0 < np; c0 += 32) {
+    const int p = c0 + lane;
+    const bool in = p < np;
+    const bool st = in && (p == 0 || w->rowid[p] != w->rowid[p - 1]);
+    const bool en = in && (p == np - 1 || w->rowid[p] != w->rowid[p + 1]);
+    const unsigned ms = __ballot_sync(FULL, st), me = __ballot_sync(FULL, en);
+    const int rs = nb + __popc(ms & lt), re = nend + __popc(me & lt);
+    if (st && rs < kWinBase) {
+      w->brow[rs] = w->rowid[p];
+      w->bxa[rs] = w->cx[p];
+    }
+    if (en && re < kWinBase) w->bxb[re] = w->cx[p];
+    nb += __popc(ms);
+    nend += __popc(me);
+  }
+  if (nb > kWinBase || nb == 0) bad = true;
+  __syncwarp();
+  const int ne = bad ? 0 : 25 * nb;
+  // W2: entries (base row, dz, dy) -> neighbour row and x-intervals
+  for (int e = lane; e < ne; e += 32) {
+    const int k = e / 25, d = e % 25;
+    const int dz = d / 5 - 2, dy = d % 5 - 2;
+    const int by = w->brow[k] % ny, bz = w->brow[k] / ny;
+    int y = by + dy;
+    y += ((y < 0) - (y >= ny)) * ny;
+    int z = bz + dz;
+    z += ((z < 0) - (z >= nz)) * nz;
+    w->erow[e] = y + z * ny;
+    const int len = w->bxb[k] - w->bxa[k] + 5;
+    int a0 = 0, b0 = nx, a1 = 0, b1 = 0;
+    if (len < nx) {
+      int s0 = w->bxa[k] - 2;
+      if (s0 < 0) s0 += nx;
+      a0 = s0;
+      if (s0 + len <= nx) {
+        b0 = s0 + len;
+      } else {
+        b0 = nx;
+        b1 = s0 + len - nx;
+      }
+    }
+    w->eiv[e][0] = a0; w->eiv[e][1] = b0; w->eiv[e][2] = a1; w->eiv[e][3] = b1;
+  }
+  __syncwarp();
+  // W3: the first entry of each distinct row merges the row's intervals
+  int badm = 0;
+  for (int e = lane; e < ne; e += 32) {
+    const int row = w->erow[e];
+    bool leader = true;
+    for (int e2 = 0; e2 < e; ++e2)
+      if (w->erow[e2] == row) { leader = false; break; }
+    int m = 0;
+    if (leader) {
+      int ia[2 * kWinBase], ib[2 * kWinBase], c = 0;
+      for (int e2 = e; e2 < ne; ++e2) {
+        if (w->erow[e2] != row) continue;
+        for (int hh = 0; hh < 2; ++hh) {
+          const int x0 = w->eiv[e2][2 * hh], x1 = w->eiv[e2][2 * hh + 1];
+          if (x1 > x0 && c < 2 * kWinBase) {
+            int t = c++;
+            while (t > 0 && ia[t - 1] > x0) { ia[t] = ia[t - 1]; ib[t] = ib[t - 1]; --t; }
+            ia[t] = x0; ib[t] = x1;
+          }
+        }
+      }
+      for (int t = 0; t < c; ++t) {
+        if (m > 0 && ia[t] <= w->ems[e][2 * m - 1]) {
+          w->ems[e][2 * m - 1] = max(w->ems[e][2 * m - 1], ib[t]);
+        } else if (m < 4) {
+          w->ems[e][2 * m] = ia[t];
+          w->ems[e][2 * m + 1] = ib[t];
+          ++m;
+        } else {
+          badm = 1;
+        }
+      }
+    }
+    w->em[e] = m;
+  }
+  bad = bad || __any_sync(FULL, badm);
+  __syncwarp();
+  // W4: segment numbers, and slot ranges from the cell starts
+  int S = 0;
+  for (int c0 = 0; c0 < ne; c0 += 32) {
+    const int e = c0 + lane;
+    const int m = e < ne ? w->em[e] : 0;
+    int incl = m;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (e < ne) w->eseg[e] = S + incl - m;
+    S += __shfl_sync(FULL, incl, 31);
+  }
+  if (S > kWinSeg) bad = true;
+  __syncwarp();
+  const int* __restrict__ cbeg = a.cstart + R.cell0;  // absolute first slot (k_rb_fix)
+  const int* __restrict__ ccnt = a.cnt + R.cell0;
+  if (!bad)
+    for (int e = lane; e < ne; e += 32) {
+      const int m = w->em[e], row = w->erow[e], b = w->eseg[e];
+      for (int t = 0; t < m; ++t) {
+        const int k0 = row * nx + w->ems[e][2 * t], k1 = row * nx + w->ems[e][2 * t + 1] - 1;
+        const int s0 = cbeg[k0], s1 = cbeg[k1] + ccnt[k1];
+        w->ustart[b + t] = s0;
+        w->ulen[b + t] = s1 - s0;
+      }
+    }
+  __syncwarp();
+  // W5: non-empty segments in slot order (disjoint, so ranks by counting)
+  int nseg = 0;
+  if (!bad) {
+    int cnt = 0;
+    for (int sg = lane; sg < S; sg += 32) {
+      if (w->ulen[sg] <= 0) continue;
+      ++cnt;
+      const int st = w->ustart[sg];
+      int r = 0;
+      for (int t = 0; t < S; ++t) r += (w->ulen[t] > 0) && (w->ustart[t] < st);
+      w->sstart[r] = st;
+      w->slen[r] = w->ulen[sg];
+    }
+    nseg = __reduce_add_sync(FULL, cnt);
+  }
+  __syncwarp();
+  // W6: window offsets (exclusive prefix of the lengths in slot order)
+  int W = 0;
+  for (int c0 = 0; c0 < nseg; c0 += 32) {
+    const int sg = c0 + lane;
+    const int len = sg < nseg ? w->slen[sg] : 0;
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (sg < nseg) w->soff[sg] = W + incl - len;
+    W += __shfl_sync(FULL, incl, 31);
+  }
+  if (W > a.win_cap) bad = true;
+  if (!bad)
+    for (int sg = lane; sg < nseg; sg += 32)
+      a.wseg[(size_t)tile * kWinSeg + sg] = make_int4(w->sstart[sg], w->slen[sg], w->soff[sg], 0);
+  if (lane == 0) {
+    w->nseg = bad ? -1 : nseg;
+    w->W = bad ? -1 : W;
+    a.wmeta[tile] = make_int2(w->nseg, w->W);
+  }
+}
+
+// The tile's window segments as the list build reads them (shared memory).
+struct WinTable {
+  int sstart[kWinSeg], slen[kWinSeg], soff[kWinSeg];
+  int nseg;
+};
+
+// (6b) the position window of every tile (after the sort, before the list
+//      build): one block per tile, pb threads
+__global__ void __launch_bounds__(kMaxBlock) k_rb_window(EngArgs a) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  WinScratch* w = reinterpret_cast<WinScratch*>(s_dyn);
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!a.win_on || !rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  if (R.nb_method != NB_CELLS) {
+    if (threadIdx.x == 0) a.wmeta[tile] = make_int2(-1, -1);  // no window for all pairs
+    return;
+  }
+  const int first = a.tile_first[tile];
+  const int np = min((int)blockDim.x, R.n - first);
+  if ((int)threadIdx.x < np) {
+    const float4 r = a.r[a.st[rep].rbuf][(size_t)R.p0 + first + threadIdx.x];
+    const int cx = cell_coord(r.x, R.invL[0], R.nc[0]);
+    const int cy = cell_coord(r.y, R.invL[1], R.nc[1]);
+    const int cz = cell_coord(r.z, R.invL[2], R.nc[2]);
+    w->rowid[threadIdx.x] = cy + cz * R.nc[1];
+    w->cx[threadIdx.x] = cx;
+  }
+  __syncthreads();
+  tile_window(a, R, tile, np, w);
+}
+
+// Window offset delta of the non-empty slot range [b, e) of one neighbour
+// row part, which lies in one window segment by construction; a range that
+// does not sets *bad (the tile then gets no window, so k_force never reads
+// outside the staged window).
+__device__ __forceinline__ int window_delta(const WinTable* w, int b, int e, int* bad) {
+  int lo = 0, hi = w->nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (w->sstart[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  if (w->nseg <= 0 || b < w->sstart[lo] || e > w->sstart[lo] + w->slen[lo]) *bad = 1;
+  return w->soff[lo] - w->sstart[lo];
+}
+
 //     SMEM_LIST = false writes the entries straight to the global list (one
 //     lane per particle needs no shared-memory tile and keeps occupancy high).
-template <int LP, bool SMEM_LIST>
+template <int LP, bool SMEM_LIST, bool WIN>
 __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   float* s_cs2 = reinterpret_cast<float*>(s_dyn);
   unsigned* s_list = reinterpret_cast<unsigned*>(s_dyn + kCs2Floats * sizeof(float));
-  __shared__ int s_max;
+  __shared__ int s_max, s_winbad;
   const int tile = blockIdx.x, rep = a.tile_rep[tile];
   if (!rb_active(a, rep)) return;
   const RepDev& R = a.rep[rep];
@@ -776,7 +1073,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   const int pb = blockDim.x / LP;
   const int lpitch = pb + 4;  // rows 16 bytes apart: a group's LP rows fall in different banks
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
-  if (threadIdx.x == 0) s_max = 0;
+  if (threadIdx.x == 0) {
+    s_max = 0;
+    s_winbad = 0;
+  }
   __syncthreads();
   const int lp = threadIdx.x / LP, q = threadIdx.x % LP;
   const unsigned lane = threadIdx.x & 31u;
@@ -792,10 +1092,34 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   const float* cs2 = s_cs2 + (valid ? __float_as_int(ri.w) : 0) * nt;
   const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
   const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+  // this particle's list column, held in registers: the list stores below
+  // cannot alias the replica table as far as the compiler can tell, so
+  // reading R.nbl0 / R.nbl_stride in the loop would reload them after every store
+  unsigned* __restrict__ col = a.nbl + R.nbl0 + i;
+  unsigned short* __restrict__ wcol = a.wl + R.nbl0 + i;
+  const size_t lstride = (size_t)R.nbl_stride;
+  WinTable* ws = reinterpret_cast<WinTable*>(
+      s_dyn + kCs2Floats * sizeof(float) + (SMEM_LIST ? (size_t)a.idx_rows * lpitch * sizeof(unsigned) : 0));
+  bool win_ok = false;
+  if (WIN) {
+    // the tile's window segments (k_rb_window), sorted by first slot
+    const int2 wm = a.wmeta[tile];
+    const int ns = wm.x >= 0 ? min(wm.x, kWinSeg) : -1;
+    for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+      const int4 sg = a.wseg[(size_t)tile * kWinSeg + k];
+      ws->sstart[k] = sg.x;
+      ws->slen[k] = sg.y;
+      ws->soff[k] = sg.z;
+    }
+    if (threadIdx.x == 0) ws->nseg = ns;
+    __syncthreads();
+    win_ok = ws->nseg > 0;
+  }
   int count = 0;
   // appends the accepted candidates of slots [b, e); every lane of the warp
-  // calls it (invalid groups with an empty range)
-  auto seg = [&](int b, int e, bool wrap) {
+  // calls it (invalid groups with an empty range).  With a window, entry j is
+  // also written to the window list as j + delta.
+  auto seg = [&](int b, int e, bool wrap, int delta) {
     int rounds = e > b ? (e - b + LP - 1) / LP : 0;
     rounds = __reduce_max_sync(0xffffffffu, rounds);
     for (int r = 0; r < rounds; ++r) {
@@ -816,7 +1140,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
         const int pos = count + __popc(g & below);
         if (pos < maxn) {
           if (SMEM_LIST) s_list[pos * lpitch + lp] = (unsigned)j;
-          else a.nbl[R.nbl0 + (size_t)pos * R.nbl_stride + i] = (unsigned)j;
+          else col[(size_t)pos * lstride] = (unsigned)j;
+          if (WIN && win_ok) wcol[(size_t)pos * lstride] = (unsigned short)(j + delta);
         }
       }
       count += __popc(g);
@@ -861,12 +1186,14 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
             e1 = cbeg[cb] + ccnt[cb];
           }
         }
-        seg(b0, e0, wrap);
-        seg(b1, e1, wrap);
+        const int d0 = WIN && win_ok && e0 > b0 ? window_delta(ws, b0, e0, &s_winbad) : 0;
+        const int d1 = WIN && win_ok && e1 > b1 ? window_delta(ws, b1, e1, &s_winbad) : 0;
+        seg(b0, e0, wrap, d0);
+        seg(b1, e1, wrap, d1);
       }
     }
   } else {
-    seg(0, valid ? R.n : 0, true);  // all pairs (calculateNBL_N2 criterion), ascending j
+    seg(0, valid ? R.n : 0, true, 0);  // all pairs (calculateNBL_N2 criterion), ascending j
   }
   if (valid && q == 0) {
     a.nn[(size_t)R.p0 + i] = (unsigned)min(count, maxn);
@@ -876,6 +1203,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   // write the tile's rows [0, rows) of the list: slots [first, first+width)
   if (SMEM_LIST) fence_async_shared();
   __syncthreads();
+  if (WIN && win_ok && threadIdx.x == 0 && s_winbad) a.wmeta[tile] = make_int2(-1, -1);
   if (SMEM_LIST && threadIdx.x < 32) {
     const int rows = min(s_max, maxn);
     const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
@@ -894,6 +1222,170 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
     unsigned c = atomicAdd(&a.rctr[rep], 1u);
     s_last = (c == (unsigned)(R.ntiles - 1));
     if (s_last) {
+      a.rctr[rep] = 0u;
+      S->rebuild = 0;
+      S->nrebuilds += 1;
+    }
+  }
+}
+
+// (7') The same list with one warp per cell.  The particles of a cell share
+//      their 25 neighbour row parts, so the warp stages the candidates' slots
+//      and positions in shared memory once (kCwCand at a time) and tests each
+//      particle of the cell against 32 consecutive candidates per round;
+//      ballot + prefix count append the accepted ones in candidate order, the
+//      reference's order.  Every lane does useful work in every round but the
+//      last of a particle.  All-pairs replicas use one part [0, n) for the
+//      whole tile.
+constexpr int kCwWarps = 4;   // warps per block
+constexpr int kCwCand = 512;  // staged candidates per warp
+
+__global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  float* s_cs2 = reinterpret_cast<float*>(s_dyn);
+  float4* s_pos = reinterpret_cast<float4*>(s_dyn + kCs2Floats * sizeof(float));  // [warp][kCwCand]
+  int* s_slot = reinterpret_cast<int*>(s_pos + kCwWarps * kCwCand);                 // [warp][kCwCand]
+  __shared__ int s_max;
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  const int nt = R.ntypes;
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
+  if (threadIdx.x == 0) s_max = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned lt = (1u << lane) - 1u;
+  const int first = a.tile_first[tile];
+  const int last = (tile + 1 < R.tile0 + R.ntiles) ? a.tile_first[tile + 1] : R.n;
+  const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
+  const int maxn = R.max_nbrs;
+  const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
+  const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+  const size_t lstride = (size_t)R.nbl_stride;
+  unsigned* __restrict__ lbase = a.nbl + R.nbl0;
+  float4* wpos = s_pos + warp * kCwCand;
+  int* wslot = s_slot + warp * kCwCand;
+  const bool cells = R.nb_method == NB_CELLS;
+  const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
+  const int* __restrict__ cbeg = a.cstart + R.cell0;  // absolute first slot (k_rb_fix)
+  const int* __restrict__ ccnt = a.cnt + R.cell0;
+  // units of work: the cells from the first to the last particle's (keys
+  // ascend along the slots), or one unit for all pairs
+  int k0 = 0, k1 = 0;
+  if (cells && last > first) {
+    const float4 rf = rc[first], rl = rc[last - 1];
+    k0 = cell_coord(rf.x, iLx, nx) + cell_coord(rf.y, iLy, ny) * nx + cell_coord(rf.z, iLz, nz) * nx * ny;
+    k1 = cell_coord(rl.x, iLx, nx) + cell_coord(rl.y, iLy, ny) * nx + cell_coord(rl.z, iLz, nz) * nx * ny;
+  }
+  int wmax = 0;
+  for (int c = k0 + warp; c <= k1; c += kCwWarps) {
+    const int p0 = cells ? max(cbeg[c], first) : first;
+    const int p1 = cells ? min(cbeg[c] + ccnt[c], last) : last;
+    if (p0 >= p1) continue;  // no particle of this tile in the cell
+    // lane r < 25: row (dz, dy) = (r/5 - 2, r%5 - 2) as one or two slot parts
+    int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
+    bool wrap = true;
+    if (cells) {
+      const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+      // no wrapped cell among the 5x5x5 and at least 7 cells a side: the
+      // minimum-image step is exactly the identity
+      wrap = !(nx >= 7 && ny >= 7 && nz >= 7 && cx >= 2 && cx < nx - 2 && cy >= 2 && cy < ny - 2 && cz >= 2 &&
+               cz < nz - 2);
+      if (lane < 25) {
+        const int dz = lane / 5 - 2, dy = lane % 5 - 2;
+        int oz = cz + dz;
+        oz += ((oz < 0) - (oz >= nz)) * nz;
+        int oy = cy + dy;
+        oy += ((oy < 0) - (oy >= ny)) * ny;
+        const int row = oy * nx + oz * nx * ny;
+        const int lo = cx - 2, hi = cx + 2;
+        if (lo >= 0 && hi < nx) {
+          b0 = cbeg[row + lo];
+          e0 = cbeg[row + hi] + ccnt[row + hi];
+        } else {
+          const int cw = row + nx - 1;
+          const int ca = lo < 0 ? row + nx + lo : row + lo;
+          const int cb = lo < 0 ? row + hi : row + hi - nx;
+          b0 = cbeg[ca];
+          e0 = cbeg[cw] + ccnt[cw];
+          b1 = cbeg[row];
+          e1 = cbeg[cb] + ccnt[cb];
+        }
+      }
+    } else if (lane == 0) {
+      e0 = R.n;
+    }
+    const int l0 = e0 - b0, len = l0 + (e1 - b1);
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int off = incl - len;                  // this lane's first candidate number
+    const int M = __shfl_sync(FULL, incl, 31);   // candidates of the unit
+    for (int pg = p0; pg < p1; pg += 32) {
+      const int pe = min(p1, pg + 32);
+      int cnt_reg = 0;  // lane k: count of particle pg + k
+      for (int ch = 0; ch < M; ch += kCwCand) {
+        const int mc = min(kCwCand, M - ch);
+        __syncwarp();
+        // candidate numbers [ch, ch + mc): each lane writes its own parts
+        for (int v = max(off, ch); v < min(off + l0, ch + mc); ++v) wslot[v - ch] = b0 + (v - off);
+        for (int v = max(off + l0, ch); v < min(off + len, ch + mc); ++v) wslot[v - ch] = b1 + (v - off - l0);
+        __syncwarp();
+        for (int v = lane; v < mc; v += 32) wpos[v] = __ldg(rc + wslot[v]);
+        __syncwarp();
+        for (int p = pg; p < pe; ++p) {
+          const float4 ri = rc[p];
+          const float* cs2 = s_cs2 + __float_as_int(ri.w) * nt;
+          unsigned* __restrict__ col = lbase + p;
+          int count = __shfl_sync(FULL, cnt_reg, p - pg);
+          for (int v0 = 0; v0 < mc; v0 += 32) {
+            const int v = v0 + lane;
+            bool in = false;
+            int j = 0;
+            if (v < mc) {
+              j = wslot[v];
+              const float4 rj = wpos[v];
+              float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
+              if (wrap) {
+                dx = mi_comp(dx, Lx, iLx);
+                dy = mi_comp(dy, Ly, iLy);
+                dz = mi_comp(dz, Lz, iLz);
+              }
+              in = (j != p) && dist2_ref(dx, dy, dz) < cs2[__float_as_int(rj.w)];
+            }
+            const unsigned g = __ballot_sync(FULL, in);
+            if (in) {
+              const int pos = count + __popc(g & lt);
+              if (pos < maxn) col[(size_t)pos * lstride] = (unsigned)j;
+            }
+            count += __popc(g);
+          }
+          if (lane == p - pg) cnt_reg = count;
+        }
+      }
+      if (pg + lane < pe) {
+        const int p = pg + lane;
+        a.nn[(size_t)R.p0 + p] = (unsigned)min(cnt_reg, maxn);
+        a.last_r[(size_t)R.p0 + p] = rc[p];
+        wmax = max(wmax, cnt_reg);
+      }
+    }
+  }
+  wmax = __reduce_max_sync(FULL, wmax);
+  if (lane == 0) atomicMax(&s_max, wmax);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int s_max_v = s_max;
+    atomicMax(&S->actual_max_nbrs, s_max_v);
+    if (s_max_v > R.max_nbrs) atomicExch(&S->overflow, 1);
+    __threadfence();
+    const unsigned cdone = atomicAdd(&a.rctr[rep], 1u);
+    if (cdone == (unsigned)(R.ntiles - 1)) {
       a.rctr[rep] = 0u;
       S->rebuild = 0;
       S->nrebuilds += 1;

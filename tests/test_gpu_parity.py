@@ -206,12 +206,14 @@ def test_neighbour_list_and_permutation_bit_exact(capi, oracle, ka_params, n):
     e.close()
 
 
-def test_n2_and_sort_methods_give_same_sets(capi, oracle, ka_params):
+@pytest.mark.parametrize("lanes", [2, 32])
+def test_n2_and_sort_methods_give_same_sets(capi, oracle, ka_params, lanes):
     n = 5000
     m = melted_ka(capi, ka_params, n, steps=100, seed=7)
     sets = []
     for method in ("sort", "n2"):
         e = new_engine(capi)
+        e.set_variant(capi.VARIANT_BUILD_LANES, lanes)
         rid = e.add(m["pos4"], m["box"], ka_params, 2, cutoff="SF", vel4=m["vel4"])
         e.set_nb_method(rid, method)
         e.calc_f()
@@ -288,8 +290,9 @@ def test_fused_run_equals_separate_calcf_integrate(capi, ka_params):
     assert s1["xi"] == s2["xi"]
 
 
-VARIANTS = [  # (force_staged, build_lanes, build_smem)
-    (1, 8, 1), (0, 8, 1), (1, 1, 0), (0, 1, 0), (0, 2, 0), (0, 4, 0), (0, 8, 0), (0, 1, 1)]
+VARIANTS = [  # (force_mode, build_lanes, build_smem)
+    (1, 8, 1), (0, 8, 1), (1, 1, 0), (0, 1, 0), (0, 2, 0), (0, 4, 0), (0, 8, 0), (0, 1, 1),
+    (2, 2, 0), (2, 8, 1), (2, 1, 0), (2, 4, 0), (0, 32, 0), (1, 32, 0), (2, 32, 0)]
 
 
 @pytest.mark.parametrize("tp", [1, 4])
@@ -303,7 +306,7 @@ def test_kernel_variants_give_identical_lists_and_trajectories(capi, oracle, ka_
     res = []
     for fs, lanes, bs in VARIANTS:
         e = new_engine(capi, pb=64, tp=tp)
-        e.set_variant(capi.VARIANT_FORCE_STAGED, fs)
+        e.set_variant(capi.VARIANT_FORCE_MODE, fs)
         e.set_variant(capi.VARIANT_BUILD_LANES, lanes)
         e.set_variant(capi.VARIANT_BUILD_SMEM, bs)
         assert e.get_variant(capi.VARIANT_BUILD_LANES) == lanes
@@ -315,6 +318,9 @@ def test_kernel_variants_give_identical_lists_and_trajectories(capi, oracle, ka_
             assert gc[i] == counts[s]
             assert np.array_equal(gl[i, : gc[i]], old[nbl[s, : counts[s]]])
         f0 = e.get(rid, "force", n)
+        if fs == 2:  # the window path is taken, not the streamed fallback
+            st0 = e.stats(rid)
+            assert st0["window_tiles"] == st0["tiles"] > 0
         e.run(200)
         res.append((f0, e.get(rid, "pos", n), e.get(rid, "vel", n), e.stats(rid)))
         e.close()
