@@ -142,12 +142,18 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *   B2MD_VARIANT_WINDOW_CAP    mode 2: window capacity in particles (shared
  *                              memory of the force kernel, 16 bytes each);
  *                              tiles with larger windows stream.
+ *   B2MD_VARIANT_SM_TILES      mode 0: 1 = the force kernel runs as many
+ *                              blocks as fit on the GPU, and each block claims
+ *                              tiles from its SM's share of the tile range,
+ *                              so each SM works on neighbouring tiles whose
+ *                              neighbours share its L1; 0 = one block per tile.
  * No reference counterpart beyond Sample::SetPB_TP (Sample.h:96). */
 enum {
   B2MD_VARIANT_FORCE_MODE = 0,
   B2MD_VARIANT_BUILD_LANES = 1,
   B2MD_VARIANT_BUILD_SMEM = 2,
-  B2MD_VARIANT_WINDOW_CAP = 3
+  B2MD_VARIANT_WINDOW_CAP = 3,
+  B2MD_VARIANT_SM_TILES = 4
 };
 B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
 B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);

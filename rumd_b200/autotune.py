@@ -12,6 +12,8 @@ and, in a second stage at the winning shape, the kernel variants
                 window staged (2) in shared memory
   build_lanes   lanes per particle in the list build: 1, 2, 4, 8, or 32 (one
                 warp per cell)
+  sm_tiles      streamed mode: blocks claim tiles from their SM's region (1)
+                or one block per tile (0)
 Each candidate is timed on the device (CUDA events around a short run of the
 real workload, after a warm-up run).  As in RUMD's test mode
 (Autotune.py:929-937), every candidate's potential energy after its run must
@@ -26,7 +28,10 @@ import os
 DEFAULT_PB = (32, 64, 128)
 DEFAULT_TP = (1, 2, 4, 8)
 DEFAULT_SKIN = (0.2, 0.3, 0.4, 0.5)
-VARIANTS = tuple(itertools.product((0, 1, 2), (1, 2, 4, 8, 32)))  # (force_mode, build_lanes)
+VARIANT_KEYS = ("force_mode", "build_lanes", "sm_tiles")
+# kernel-variant candidates: (force_mode, sm_tiles) x build_lanes
+VARIANTS = tuple(dict(force_mode=fm, sm_tiles=st, build_lanes=bl)
+                 for (fm, st), bl in itertools.product(((0, 0), (0, 1), (1, 0), (2, 0)), (1, 2, 4, 8, 32)))
 
 
 def candidates(pbs=DEFAULT_PB, tps=DEFAULT_TP, skins=DEFAULT_SKIN, max_block=512):
@@ -54,18 +59,18 @@ def search(cands, measure, pe_tol=0.005):
 
 def search_variants(shape, measure, variants=VARIANTS, pe_tol=0.005):
     """Second stage: the kernel variants at a fixed (pb, tp, skin).
-    measure(pb, tp, skin, force_mode=, build_lanes=) -> (rate, pe)."""
+    measure(pb, tp, skin, **variant) -> (rate, pe)."""
     table = []
     ref_pe = None
     best = None
-    for fs, bl in variants:
-        rate, pe = measure(shape["pb"], shape["tp"], shape["skin"], force_mode=fs, build_lanes=bl)
+    for var in variants:
+        rate, pe = measure(shape["pb"], shape["tp"], shape["skin"], **var)
         ok = True
         if ref_pe is None:
             ref_pe = pe
         elif abs(pe - ref_pe) > pe_tol:
             ok = False
-        table.append({"force_mode": fs, "build_lanes": bl, "rate": rate, "pe": pe, "ok": ok})
+        table.append(dict(var, rate=rate, pe=pe, ok=ok))
         if ok and (best is None or rate > best["rate"]):
             best = table[-1]
     return best, table
@@ -75,9 +80,11 @@ def apply(engine, entry):
     """Sets a tuned entry's launch shape and kernel variants on an engine."""
     from . import capi
     engine.set_launch(entry["pb"], entry["tp"])
-    if "force_mode" in entry:
-        engine.set_variant(capi.VARIANT_FORCE_MODE, entry["force_mode"])
-        engine.set_variant(capi.VARIANT_BUILD_LANES, entry["build_lanes"])
+    codes = {"force_mode": capi.VARIANT_FORCE_MODE, "build_lanes": capi.VARIANT_BUILD_LANES,
+             "sm_tiles": capi.VARIANT_SM_TILES}
+    for k, code in codes.items():
+        if k in entry:
+            engine.set_variant(code, entry[k])
 
 
 def signature(replicas):
@@ -99,8 +106,8 @@ class Autotune:
 
     def tune(self, replicas, measure, force=False, variants=False):
         """Stage 1 over (pb, tp, skin); with variants=True, stage 2 over the
-        kernel variants at the winning shape (measure then takes
-        force_mode= and build_lanes= keywords)."""
+        kernel variants at the winning shape (measure then takes the
+        VARIANT_KEYS as keywords)."""
         key = signature(replicas)
         cache = self._load()
         if key in cache and not force:
@@ -109,8 +116,8 @@ class Autotune:
         entry = {"pb": best["pb"], "tp": best["tp"], "skin": best["skin"], "rate": best["rate"], "table": table}
         if variants:
             vbest, vtable = search_variants(entry, measure)
-            entry.update(force_mode=vbest["force_mode"], build_lanes=vbest["build_lanes"],
-                         rate=max(entry["rate"], vbest["rate"]), variant_table=vtable)
+            entry.update({k: vbest[k] for k in VARIANT_KEYS if k in vbest})
+            entry.update(rate=max(entry["rate"], vbest["rate"]), variant_table=vtable)
         cache[key] = entry
         with open(self.cache_path, "w") as fh:
             json.dump(cache, fh, indent=1)
@@ -140,12 +147,14 @@ def device_measure(capi, replicas, device=0, steps=300, warmup=100):
     replicas: list of dicts with pos4, vel4, box, params, ntypes, T, n, density."""
     import torch
 
-    def measure(pb, tp, skin, force_mode=None, build_lanes=None):
+    def measure(pb, tp, skin, force_mode=None, build_lanes=None, sm_tiles=None):
         e = capi.Engine(device=device, max_replicas=len(replicas), pb=pb, tp=tp)
         if force_mode is not None:
             e.set_variant(capi.VARIANT_FORCE_MODE, force_mode)
         if build_lanes is not None:
             e.set_variant(capi.VARIANT_BUILD_LANES, build_lanes)
+        if sm_tiles is not None:
+            e.set_variant(capi.VARIANT_SM_TILES, sm_tiles)
         ids = [e.add(r["pos4"], r["box"], r["params"], r["ntypes"], cutoff="SF", skin=skin, T=r["T"],
                      vel4=r["vel4"]) for r in replicas]
         e.calc_f()  # invariance check on the common starting configuration
@@ -190,9 +199,10 @@ def main(argv=None):
         print(f"pb={r['pb']:4d} tp={r['tp']} skin={r['skin']:.2f}  {r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
     for r in best.get("variant_table", []):
-        print(f"force_mode={r['force_mode']} build_lanes={r['build_lanes']}  {r['rate']:.4e} particle-steps/s  "
+        print(f"force_mode={r['force_mode']} sm_tiles={r['sm_tiles']} build_lanes={r['build_lanes']}  "
+              f"{r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
-    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate", "force_mode", "build_lanes") if k in best}))
+    print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate") + VARIANT_KEYS if k in best}))
 
 
 if __name__ == "__main__":

@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "librumd_b200.so")
 B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_OVERFLOW = range(6)
 CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
 # kernel variants (b2md_engine_set_variant)
-VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP = 0, 1, 2, 3
+VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP, VARIANT_SM_TILES = 0, 1, 2, 3, 4
 FORCE_STREAMED, FORCE_STAGED, FORCE_WINDOW = 0, 1, 2
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",

@@ -130,8 +130,11 @@ struct b2md_engine {
   int rcap = 0;
   // kernel variants (b2md_engine_set_variant)
   int force_mode = 0;          // force kernel: FM_STREAMED, FM_STAGED or FM_WINDOW
+  bool sm_tiles = false;       // FM_STREAMED: blocks claim tiles from their SM's region
+  int nsm = 0;                 // streaming multiprocessors of the device
+  unsigned* smctr = nullptr;   // SM-region claim counters (nsm + 1)
   int win_cap = 2560;          // FM_WINDOW: window capacity in particles
-  int build_lanes = 2;         // list build: lanes per particle
+  int build_lanes = 32;        // list build: lanes per particle (32: one warp per cell)
   bool build_smem = false;     // list build: tile assembled in shared memory
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
   float4* r[2] = {nullptr, nullptr};
@@ -289,6 +292,8 @@ EngArgs make_args(b2md_engine* e) {
   a.wseg = e->wseg;
   a.wmeta = e->wmeta;
   a.win_on = e->force_mode == FM_WINDOW ? 1 : 0;
+  a.nreg = (e->sm_tiles && e->force_mode == FM_STREAMED) ? e->nsm : 0;
+  a.smctr = e->smctr;
   a.win_cap = e->win_cap;
   return a;
 }
@@ -608,10 +613,20 @@ void init_func_attrs(int device) {
   done_mask |= bit;
 }
 
+// Grid of k_force: one block per tile, or with SM tiles as many blocks as
+// fit on the GPU at once (never more than the tiles).
+int force_grid(const b2md_engine* e, const EngArgs& a, ForceFn fn, size_t smem) {
+  if (a.nreg <= 0) return e->ntiles;
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, e->pb * e->tp, smem));
+  return std::max(1, std::min(e->ntiles, std::max(per_sm, 1) * e->nsm));
+}
+
 void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
   if (e->ntiles == 0) return;
   ForceFn fn = force_fn(e, fused, stress, a);
-  fn<<<e->ntiles, e->pb * e->tp, force_smem(a, e->force_mode), s>>>(a, 0, cudaGraphConditionalHandle{});
+  const size_t smem = force_smem(a, e->force_mode);
+  fn<<<force_grid(e, a, fn, smem), e->pb * e->tp, smem, s>>>(a, 0, cudaGraphConditionalHandle{});
 }
 
 void check_launch() { CK(cudaGetLastError()); }
@@ -654,7 +669,7 @@ void build_graph(b2md_engine* e, int which, int K) {
       cudaKernelNodeParams kp = {};
       void* args[] = {&a, &has_next, &hn};
       kp.func = (void*)fstep;
-      kp.gridDim = dim3(e->ntiles);
+      kp.gridDim = dim3(force_grid(e, a, fstep, smem));
       kp.blockDim = dim3(e->pb * e->tp);
       kp.sharedMemBytes = (unsigned)smem;
       kp.kernelParams = args;
@@ -667,7 +682,7 @@ void build_graph(b2md_engine* e, int which, int K) {
     CK(cudaStreamBeginCapture(e->cap_stream, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < K; ++k) {
       launch_rebuild(e, e->cap_stream, a);
-      fstep<<<e->ntiles, e->pb * e->tp, smem, e->cap_stream>>>(a, 0, cudaGraphConditionalHandle{});
+      fstep<<<force_grid(e, a, fstep, smem), e->pb * e->tp, smem, e->cap_stream>>>(a, 0, cudaGraphConditionalHandle{});
     }
     CK(cudaStreamEndCapture(e->cap_stream, &captured));
     CK(cudaGraphDestroy(g));
@@ -822,6 +837,9 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
     grow_reps(e, std::max(max_replicas, 1));
     init_func_attrs(device);
     CK(cudaMalloc(&e->fctr, sizeof(unsigned)));
+    CK(cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaMalloc(&e->smctr, (e->nsm + 1) * sizeof(unsigned)));
+    CK(cudaMemsetAsync(e->smctr, 0, (e->nsm + 1) * sizeof(unsigned), e->stream));
     // [0]: "a replica needs a rebuild" raised by the step kernel;
     // [1]: the same decision read by the host in b2md_run_timed
     CK(cudaMalloc(&e->any_rebuild, 2 * sizeof(int)));
@@ -845,7 +863,7 @@ int b2md_engine_destroy(b2md_engine* e) {
   void* ptrs[] = {e->r[0], e->r[1], e->v[0], e->v[1], e->im[0], e->im[1], e->uidx[0], e->uidx[1], e->f, e->w,
                   e->sts, e->last_r, e->nn, e->order, e->key, e->slot, e->nbl, e->cnt, e->cstart, e->par, e->elog,
                   e->rep, e->st, e->rctr, e->tile_rep, e->tile_first, e->ctot, e->cpref, e->tpart, e->gpart,
-                  e->gctr, e->fctr, e->any_rebuild, e->wl, e->wseg, e->wmeta};
+                  e->gctr, e->fctr, e->any_rebuild, e->wl, e->wseg, e->wmeta, e->smctr};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->stream) cudaStreamDestroy(e->stream);
@@ -892,6 +910,10 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
       }
       e->force_mode = value;
       break;
+    case B2MD_VARIANT_SM_TILES:
+      if (value != 0 && value != 1) return fail(B2MD_ERR_ARG, "sm_tiles must be 0 or 1");
+      e->sm_tiles = value != 0;
+      break;
     case B2MD_VARIANT_WINDOW_CAP:
       if (value < 256 || value > kMaxWindow)
         return fail(B2MD_ERR_ARG, "window capacity must be 256..%d particles (got %d)", kMaxWindow, value);
@@ -921,6 +943,7 @@ int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
   if (!e || !value) return fail(B2MD_ERR_ARG, "null argument");
   switch (which) {
     case B2MD_VARIANT_FORCE_MODE: *value = e->force_mode; break;
+    case B2MD_VARIANT_SM_TILES: *value = e->sm_tiles ? 1 : 0; break;
     case B2MD_VARIANT_WINDOW_CAP: *value = e->win_cap; break;
     case B2MD_VARIANT_BUILD_LANES: *value = e->build_lanes; break;
     case B2MD_VARIANT_BUILD_SMEM: *value = e->build_smem ? 1 : 0; break;
@@ -1397,7 +1420,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
         nl += e->force_mode == FM_WINDOW ? 10 : 9;
       }
       CK(cudaEventRecord(ev[2 * k], e->stream));
-      fstep<<<e->ntiles, e->pb * e->tp, smem, e->stream>>>(a, 0, cudaGraphConditionalHandle{});
+      fstep<<<force_grid(e, a, fstep, smem), e->pb * e->tp, smem, e->stream>>>(a, 0, cudaGraphConditionalHandle{});
       CK(cudaEventRecord(ev[2 * k + 1], e->stream));
       nl += 2;
     }

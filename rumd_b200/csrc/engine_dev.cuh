@@ -119,6 +119,8 @@ struct EngArgs {
   int2* wmeta;         // per-tile (segments, particles)
   int win_on;          // list builds also build the windows
   int win_cap;         // window capacity in particles (shared memory of k_force)
+  int nreg;            // SM regions for k_force tile claiming (0 = one tile per block)
+  unsigned* smctr;     // per-region claim counters [nreg] + tiles claimed [nreg]
 };
 
 }  // namespace b2md

@@ -101,7 +101,8 @@ __device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int l
 }
 
 // Last block of the whole grid: publishes "any replica needs a rebuild" to
-// the next conditional graph node (or nothing when launched eagerly).
+// the next conditional graph node (or nothing when launched eagerly), and
+// clears the SM-region tile counters (every block has made its last claim).
 __device__ __forceinline__ void grid_final(const EngArgs& a, int has_cond, cudaGraphConditionalHandle h) {
   if (threadIdx.x == 0) {
     __threadfence();
@@ -110,9 +111,71 @@ __device__ __forceinline__ void grid_final(const EngArgs& a, int has_cond, cudaG
       __threadfence();
       int any = atomicExch(a.any_rebuild, 0);
       *a.fctr = 0u;
+      for (int k = 0; k <= a.nreg && a.nreg > 0; ++k) a.smctr[k] = 0u;
       if (has_cond) cudaGraphSetConditional(h, any ? 1u : 0u);
     }
   }
+}
+
+// First tile of SM region r (regions split [0, ntiles) evenly).
+__device__ __forceinline__ int region_first(const EngArgs& a, int r) {
+  return (int)(((long long)r * a.ntiles) / a.nreg);
+}
+
+// Called by warp 0; returns (in every lane) a tile no other block has
+// claimed, or -1 when every tile is claimed.  A block first claims from its
+// own SM's region (smctr[r] counts claim attempts there; the first
+// region-size ones succeed); when that is used up and smctr[nreg] (tiles
+// claimed so far) shows tiles left, the warp scans the other regions, 32 at
+// a time, and claims from one with tiles left.  Every claim is a single
+// atomic; nothing waits on another block.
+__device__ int claim_tile(const EngArgs& a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const int nreg = a.nreg;
+  unsigned* ctr = a.smctr;
+  unsigned smid;
+  asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+  const int r0 = (int)(smid % (unsigned)nreg);
+  int tile = -1;
+  if (lane == 0) {
+    const int lo = region_first(a, r0), size = region_first(a, r0 + 1) - lo;
+    if (size > 0) {
+      const unsigned t = atomicAdd(&ctr[r0], 1u);
+      if (t < (unsigned)size) tile = lo + (int)t;
+    }
+  }
+  tile = __shfl_sync(FULL, tile, 0);
+  if (tile < 0) {
+    const unsigned done = __shfl_sync(FULL, lane == 0 ? *(volatile unsigned*)&ctr[nreg] : 0u, 0);
+    if (done < (unsigned)a.ntiles) {
+      for (int base = 1; base < nreg && tile < 0; base += 32) {
+        const int q = base + lane;
+        int r = -1, lo = 0, size = 0;
+        if (q < nreg) {
+          r = (r0 + q) % nreg;
+          lo = region_first(a, r);
+          size = region_first(a, r + 1) - lo;
+          if (*(volatile unsigned*)&ctr[r] >= (unsigned)size) r = -1;
+        }
+        unsigned m = __ballot_sync(FULL, r >= 0);
+        while (m && tile < 0) {
+          const int src = __ffs(m) - 1;
+          m &= m - 1;
+          const int rr = __shfl_sync(FULL, r, src), rlo = __shfl_sync(FULL, lo, src);
+          const int rsize = __shfl_sync(FULL, size, src);
+          int got = -1;
+          if (lane == 0) {
+            const unsigned t = atomicAdd(&ctr[rr], 1u);
+            if (t < (unsigned)rsize) got = rlo + (int)t;
+          }
+          tile = __shfl_sync(FULL, got, 0);
+        }
+      }
+    }
+  }
+  if (tile >= 0 && lane == 0) atomicAdd(&ctr[nreg], 1u);
+  return tile;
 }
 
 // Nose-Hoover leap-frog for one particle (integrateNVTAlgorithm,
@@ -279,8 +342,10 @@ struct PosWindow {
   __device__ __forceinline__ float4 operator()(unsigned j) const { return p[j]; }
 };
 
-// Neighbour positions in flight per thread in force_loop.
+// Neighbour positions in flight per thread in force_loop, and whether the
+// next group's list entries are loaded one group ahead.
 constexpr int kForceUnroll = 4;
+constexpr bool kForcePipeline = false;
 
 // The neighbour loop of one thread: entries k = lane_t, lane_t + TP, ... of
 // the particle's list column, kForceUnroll neighbour positions in flight.
@@ -290,15 +355,36 @@ __device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos
                                            float iLx, float iLy, float iLz) {
   constexpr int U = kForceUnroll;
   unsigned k = lane_t;
-  for (; k + (U - 1) * TP < nn; k += U * TP) {
-    unsigned j[U];
-    float4 rj[U];
+  if (kForcePipeline) {
+    // the next group's list entries are loaded while this group's positions
+    // are gathered and summed
+    unsigned jn[U];
+    if (k + (U - 1) * TP < nn) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) j[u] = idx(k + u * TP);
+      for (int u = 0; u < U; ++u) jn[u] = idx(k + u * TP);
+    }
+    for (; k + (U - 1) * TP < nn; k += U * TP) {
+      float4 rj[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) rj[u] = pos(j[u]);
+      for (int u = 0; u < U; ++u) rj[u] = pos(jn[u]);
+      if (k + U * TP + (U - 1) * TP < nn) {
 #pragma unroll
-    for (int u = 0; u < U; ++u) lj_pair<STRESS, WRAP>(A, ri, rj[u], prow, Lx, Ly, Lz, iLx, iLy, iLz);
+        for (int u = 0; u < U; ++u) jn[u] = idx(k + U * TP + u * TP);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) lj_pair<STRESS, WRAP>(A, ri, rj[u], prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    }
+  } else {
+    for (; k + (U - 1) * TP < nn; k += U * TP) {
+      unsigned j[U];
+      float4 rj[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) j[u] = idx(k + u * TP);
+#pragma unroll
+      for (int u = 0; u < U; ++u) rj[u] = pos(j[u]);
+#pragma unroll
+      for (int u = 0; u < U; ++u) lj_pair<STRESS, WRAP>(A, ri, rj[u], prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    }
   }
   for (; k < nn; k += TP) {
     const float4 r0 = pos(idx(k));
@@ -345,7 +431,23 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
   __shared__ double s_blk[kNPart], s_tot[kNPart];
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ unsigned s_rows;
-  const int tile = blockIdx.x;
+  __shared__ int s_tile;
+  // SM tiles (streamed mode): a grid of at most as many blocks as fit at once;
+  // each block claims tiles from its SM's region of the tile range, so the
+  // tiles an SM processes are neighbours in space and share its L1
+  const bool sm_tiles = MODE == FM_STREAMED && a.nreg > 0;
+  int tile = blockIdx.x;
+  for (;;) {
+  if (sm_tiles) {
+    __syncthreads();  // the previous tile is done with shared memory
+    if (threadIdx.x < 32) {
+      const int t = claim_tile(a);
+      if (threadIdx.x == 0) s_tile = t;
+    }
+    __syncthreads();
+    tile = s_tile;
+    if (tile < 0) break;
+  }
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
@@ -502,6 +604,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     }
   }
+  if (!sm_tiles) break;
+  }  // tiles
   grid_final(a, has_cond, h);
 }
 
@@ -1159,19 +1263,43 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
     const bool inner = nx >= 7 && ny >= 7 && nz >= 7 && cx >= 2 && cx < nx - 2 && cy >= 2 && cy < ny - 2 &&
                        cz >= 2 && cz < nz - 2;
     const bool wrap = !__all_sync(0xffffffffu, !valid || inner);
+    // Cells farther from the particle than its largest list radius hold no
+    // neighbour: rows (dz, dy) out of reach are skipped and each row's x-range
+    // is trimmed at its ends, which leaves the list (and its order) unchanged.
+    // The reach is the largest (rc + skin) of the particle's type plus 0.01;
+    // the gaps are the exact distances from the particle to the cell faces.
+    float reach2 = 0.f;
+    for (int k = 0; k < nt; ++k) reach2 = fmaxf(reach2, cs2[k]);
+    reach2 = sqrtf(reach2) + 0.01f;
+    reach2 *= reach2;
+    const float wx = Lx / nx, wy = Ly / ny, wz = Lz / nz;
+    auto gap = [](float x, int c, int d, float w, float half) -> float {
+      if (d > 0) return fmaxf(0.f, fmaf((float)(c + d), w, -half) - x);
+      if (d < 0) return fmaxf(0.f, x - fmaf((float)(c + d + 1), w, -half));
+      return 0.f;
+    };
     for (int dz = -2; dz <= 2; ++dz) {
       int oz = cz + dz;
       oz += ((oz < 0) - (oz >= nz)) * nz;
+      const float gz = gap(ri.z, cz, dz, wz, 0.5f * Lz);
       for (int dy = -2; dy <= 2; ++dy) {
         int oy = cy + dy;
         oy += ((oy < 0) - (oy >= ny)) * ny;
-        // the five cells cx-2..cx+2 of this row are consecutive keys, so
+        const float gy = gap(ri.y, cy, dy, wy, 0.5f * Ly);
+        const float gyz2 = fmaf(gy, gy, gz * gz);
+        // the cells cx+dxl..cx+dxh of this row are consecutive keys, so
         // their particles are one slot range (two when the row wraps); the
-        // scan order dx = -2..2, ascending slot, is the reference's
+        // scan order dx ascending, ascending slot, is the reference's
+        int dxl = -2, dxh = 2;
+        while (dxl < 0 && fmaf(gap(ri.x, cx, dxl, wx, 0.5f * Lx), gap(ri.x, cx, dxl, wx, 0.5f * Lx), gyz2) >= reach2)
+          ++dxl;
+        while (dxh > 0 && fmaf(gap(ri.x, cx, dxh, wx, 0.5f * Lx), gap(ri.x, cx, dxh, wx, 0.5f * Lx), gyz2) >= reach2)
+          --dxh;
+        const bool reach = gyz2 < reach2;
         const int row = oy * nx + oz * nx * ny;
-        const int lo = cx - 2, hi = cx + 2;
+        const int lo = cx + dxl, hi = cx + dxh;
         int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
-        if (valid) {
+        if (valid && reach) {
           if (lo >= 0 && hi < nx) {
             const int c1 = row + hi;
             b0 = cbeg[row + lo];
@@ -1238,7 +1366,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
 //      last of a particle.  All-pairs replicas use one part [0, n) for the
 //      whole tile.
 constexpr int kCwWarps = 4;   // warps per block
-constexpr int kCwCand = 512;  // staged candidates per warp
+constexpr int kCwCand = 256;  // staged candidates per warp
 
 __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
   constexpr unsigned FULL = 0xffffffffu;

@@ -42,7 +42,7 @@ def test_cache_round_trip(tmp_path):
 def test_variant_stage_picks_fastest_and_is_cached(tmp_path):
     from rumd_b200 import autotune
 
-    def measure(pb, tp, skin, force_mode=None, build_lanes=None):
+    def measure(pb, tp, skin, force_mode=None, build_lanes=None, sm_tiles=None):
         if force_mode is None:
             return float(pb * tp), -5.0
         # streamed index loads and two build lanes fastest; staged with one lane breaks pe

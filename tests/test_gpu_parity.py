@@ -290,9 +290,10 @@ def test_fused_run_equals_separate_calcf_integrate(capi, ka_params):
     assert s1["xi"] == s2["xi"]
 
 
-VARIANTS = [  # (force_mode, build_lanes, build_smem)
-    (1, 8, 1), (0, 8, 1), (1, 1, 0), (0, 1, 0), (0, 2, 0), (0, 4, 0), (0, 8, 0), (0, 1, 1),
-    (2, 2, 0), (2, 8, 1), (2, 1, 0), (2, 4, 0), (0, 32, 0), (1, 32, 0), (2, 32, 0)]
+VARIANTS = [  # (force_mode, build_lanes, build_smem, sm_tiles)
+    (1, 8, 1, 0), (0, 8, 1, 0), (1, 1, 0, 0), (0, 1, 0, 0), (0, 2, 0, 0), (0, 4, 0, 0), (0, 8, 0, 0),
+    (0, 1, 1, 0), (2, 2, 0, 0), (2, 8, 1, 0), (2, 1, 0, 0), (2, 4, 0, 0), (0, 32, 0, 0), (1, 32, 0, 0),
+    (2, 32, 0, 0), (0, 32, 0, 1), (0, 2, 0, 1), (2, 32, 0, 1)]
 
 
 @pytest.mark.parametrize("tp", [1, 4])
@@ -304,11 +305,12 @@ def test_kernel_variants_give_identical_lists_and_trajectories(capi, oracle, ka_
     nc, old, counts, nbl, ov = oracle_sorted_list(oracle, m["pos4"], m["box"], ka_params, 2, 0.3, 400)
     assert not ov
     res = []
-    for fs, lanes, bs in VARIANTS:
+    for fs, lanes, bs, smt in VARIANTS:
         e = new_engine(capi, pb=64, tp=tp)
         e.set_variant(capi.VARIANT_FORCE_MODE, fs)
         e.set_variant(capi.VARIANT_BUILD_LANES, lanes)
         e.set_variant(capi.VARIANT_BUILD_SMEM, bs)
+        e.set_variant(capi.VARIANT_SM_TILES, smt)
         assert e.get_variant(capi.VARIANT_BUILD_LANES) == lanes
         rid = e.add(m["pos4"], m["box"], ka_params, 2, cutoff="SF", dt=0.005, T=0.9, vel4=m["vel4"])
         e.calc_f()
