@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--tp", type=int, default=2)
     p.add_argument("--batch-steps", type=int, default=2000)
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--served-jobs", type=int, default=48, help="jobs in the served stream (0: skip)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--force-mode", type=int, default=None, help="kernel variant: 0 streamed, 1 staged, 2 window")
     p.add_argument("--build-lanes", type=int, default=None, help="kernel variant: list-build lanes per particle")
@@ -312,6 +313,37 @@ def batched(capi, device, pb, tp, steps, seed=0):
             "speedup_vs_sequential": rate_b / rate_s}
 
 
+def served(capi, device, pb, tp, njobs, seed=0):
+    """Continuous batching: a seeded Poisson stream (50 jobs/s) of KA/LJ jobs,
+    N log-uniform in [256, 32768], steps log-uniform in [1e3, 1e5], admitted
+    against a 150 GB budget and advanced together (rumd_b200.serving).
+    Latencies are wall-clock from arrival to the job's last step; against the
+    plain one-job-at-a-time loop on a sample of the same jobs."""
+    from rumd_b200 import serving
+    jobs = serving.poisson_stream(njobs, rate=50.0, seed=seed)
+    e = new_engine(capi, device=device, pb=pb, tp=tp)
+    srv = serving.MDServer(e, hbm_budget=150e9, chunk_steps=500, dt=DT, skin=SKIN, tau=TAU)
+    srv.serve(jobs)
+    e.close()
+    summ = serving.latency_summary(jobs)
+    sample = [serving.Job(**{k: getattr(j, k) for k in ("id", "kind", "n", "T", "steps", "seed")}, arrival=0.0)
+              for j in jobs[::8]]
+    t0 = time.perf_counter()
+    serving.serve_one_at_a_time(lambda: new_engine(capi, device=device, pb=pb, tp=tp), sample, dt=DT, skin=SKIN,
+                                tau=TAU)
+    t_one = time.perf_counter() - t0
+    one_rate = sum(j.n * j.steps for j in sample) / t_one
+    return {"value": summ["throughput"], "unit": "particle-steps/s", "jobs": summ["jobs"],
+            "p50_latency_s": summ["p50_s"], "p99_latency_s": summ["p99_s"], "makespan_s": summ["makespan_s"],
+            "particle_steps": summ["particle_steps"], "hbm_max_used_bytes": srv.max_used,
+            "one_at_a_time_value": one_rate,
+            "one_at_a_time_sample": f"{len(sample)} of the {njobs} jobs run alone back to back (wall clock)",
+            "speedup_vs_one_at_a_time": summ["throughput"] / one_rate,
+            "stream": "Poisson 50 jobs/s, KA (rho 1.2) or LJ (rho 0.8442) 50/50, N 256-32768 and steps 1e3-1e5 "
+                      "log-uniform, T 0.5-2.0, seed 0; throughput = particle-steps / (last completion - first "
+                      "arrival)"}
+
+
 def config_block(args, world, engine=None):
     variants = {}
     if engine is not None:
@@ -434,6 +466,8 @@ def main():
             extra["cpu_baseline"] = cpu_baseline_sample(e, rid, box, params)
         if not args.no_batched:
             extra["batched"] = batched(capi, device, args.pb, args.tp, args.batch_steps)
+        if args.served_jobs > 0:
+            extra["served"] = served(capi, device, args.pb, args.tp, args.served_jobs)
     e.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
