@@ -7,7 +7,9 @@ NVT (tau=0.2), dt=0.005, skin 0.3, shifted-force cut-off 2.5 sigma_ij, FP32
 forces with FP64 reductions.  A "step" is one MD time step (momentum reset,
 neighbour-list check/rebuild, forces, integration).  The line also carries the
 batched form (256 mixed-size KA replicas in one launch sequence) against
-sequential plain runs of a sample of the same replicas.
+sequential plain runs of a sample of the same replicas, and the served form
+(a Poisson stream of KA/LJ jobs through the continuous-batching server, with
+p50/p99 job latency) against the one-job-at-a-time loop.
 
   python bench.py [--gpus N --steps K --warmup W]        # this implementation
   python bench.py --impl reference ...                   # reference CPU path
@@ -51,6 +53,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--force-mode", type=int, default=None, help="kernel variant: 0 streamed, 1 staged, 2 window")
     p.add_argument("--build-lanes", type=int, default=None, help="kernel variant: list-build lanes per particle")
+    p.add_argument("--sm-tiles", type=int, default=None, help="kernel variant: 1 = SM-region tile claiming")
     p.add_argument("--profile-launches", action="store_true",
                    help="small plain run only (for the ncu launch list)")
     return p.parse_args()
@@ -230,9 +233,9 @@ def time_run(capi, e, steps, device):
     return t0.elapsed_time(t1) / 1e3
 
 
-def launches_in_run(steps, rebuilds, per_rebuild=9):
-    # per step: fused kernel; per graph launch: gate; per rebuild: 9 kernels
-    # (10 with position windows); run start: steps + momentum; run end:
+def launches_in_run(steps, rebuilds, per_rebuild=8):
+    # per step: fused kernel; per graph launch: gate; per rebuild: 8 kernels
+    # (9 with position windows); run start: steps + momentum; run end:
     # rebuild sequence + force kernel
     graph_launches = steps // 32 + steps % 32
     return int(steps + graph_launches + per_rebuild * rebuilds + 2 + per_rebuild + 1)
@@ -402,6 +405,7 @@ def main():
     capi.lib()
     KERNEL_VARIANTS[capi.VARIANT_FORCE_MODE] = args.force_mode
     KERNEL_VARIANTS[capi.VARIANT_BUILD_LANES] = args.build_lanes
+    KERNEL_VARIANTS[capi.VARIANT_SM_TILES] = args.sm_tiles
     device = local
     if args.profile_launches:
         # Same workload driven with eager launches only (b2md_run_timed): the
@@ -458,7 +462,7 @@ def main():
                 "step_share_of_run": per_launch_s * args.steps / t}
     extra = {}
     cfg = config_block(args, world, e)
-    per_rebuild = 10 if cfg.get("force_mode") == capi.FORCE_WINDOW else 9
+    per_rebuild = 9 if cfg.get("force_mode") == capi.FORCE_WINDOW else 8
     if rank == 0:
         pos4, vel4, im3 = e.get(rid, "pos", N_PLAIN), e.get(rid, "vel", N_PLAIN), e.get(rid, "images", N_PLAIN)
         e2e = e2e_run(capi, device, args.pb, args.tp, pos4, vel4, im3, box, params, args.steps)

@@ -517,11 +517,13 @@ void place_list(b2md_engine* e, HostRep& h, int max_nbrs) {
 }
 
 // ---- launches ----
+// Kernels in one rebuild sequence (launch_rebuild).
+int rebuild_launches(const b2md_engine* e) { return e->force_mode == FM_WINDOW ? 9 : 8; }
+
 void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   const int T = e->ntiles;
   const int R = (int)e->reps.size();
   if (T == 0) return;
-  k_rb_begin<<<(R + 127) / 128, 128, 0, s>>>(a);
   k_rb_clear<<<T, e->pb, 0, s>>>(a);
   k_rb_count<<<T, e->pb, 0, s>>>(a);
   k_rb_scan_local<<<T, e->pb, 0, s>>>(a);
@@ -1417,7 +1419,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
       CK(cudaStreamSynchronize(e->stream));
       if (*h_any) {
         launch_rebuild(e, e->stream, a);
-        nl += e->force_mode == FM_WINDOW ? 10 : 9;
+        nl += rebuild_launches(e);
       }
       CK(cudaEventRecord(ev[2 * k], e->stream));
       fstep<<<force_grid(e, a, fstep, smem), e->pb * e->tp, smem, e->stream>>>(a, 0, cudaGraphConditionalHandle{});
@@ -1438,7 +1440,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     calc_f(e, false);
     CK(cudaStreamSynchronize(e->stream));
     *step_kernel_ms = tot;
-    *launches = nl + (e->force_mode == FM_WINDOW ? 11 : 10);
+    *launches = nl + rebuild_launches(e) + 1;
   });
 }
 

@@ -740,6 +740,8 @@ __global__ void k_rb_clear(EngArgs a) {
   const int tile = blockIdx.x, rep = a.tile_rep[tile];
   if (!rb_active(a, rep)) return;
   const RepDev& R = a.rep[rep];
+  // the replica's first tile also resets the per-build maximum list length
+  if (tile == R.tile0 && threadIdx.x == 0) a.st[rep].actual_max_nbrs = 0;
   if (R.nb_method != NB_CELLS) return;
   const int ch = cell_chunk(R), lt = tile - R.tile0;
   const int c0 = lt * ch, c1 = min(R.ncell, c0 + ch);
@@ -1521,11 +1523,5 @@ __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
   }
 }
 
-// Resets the per-build maximum before a rebuild sequence.
-__global__ void k_rb_begin(EngArgs a) {
-  const int rep = blockIdx.x * blockDim.x + threadIdx.x;
-  if (rep >= a.nrep) return;
-  if (a.rep[rep].active && a.st[rep].rebuild && !a.st[rep].overflow) a.st[rep].actual_max_nbrs = 0;
-}
 
 }  // namespace b2md
