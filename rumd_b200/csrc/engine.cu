@@ -616,12 +616,14 @@ void init_func_attrs(int device) {
 }
 
 // Grid of k_force: one block per tile, or with SM tiles as many blocks as
-// fit on the GPU at once (never more than the tiles).
+// fit on the GPU at once -- all SMs then hold the same number of blocks, so
+// each SM's region of tiles is worked by its own blocks (blocks that find no
+// tile left exit at once).
 int force_grid(const b2md_engine* e, const EngArgs& a, ForceFn fn, size_t smem) {
   if (a.nreg <= 0) return e->ntiles;
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fn, e->pb * e->tp, smem));
-  return std::max(1, std::min(e->ntiles, std::max(per_sm, 1) * e->nsm));
+  return std::max(1, std::max(per_sm, 1) * e->nsm);
 }
 
 void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
