@@ -282,9 +282,8 @@ EngArgs make_args(b2md_engine* e) {
   a.gctr = e->gctr; a.rctr = e->rctr; a.fctr = e->fctr; a.any_rebuild = e->any_rebuild; a.elog = e->elog;
   a.ntiles = e->ntiles;
   a.nrep = (int)e->reps.size();
-  // staged list tile: pb columns + padding so that the tp rows a warp reads
-  // at once fall in different shared-memory banks
-  a.idx_pitch = e->pb + (e->tp > 1 ? 32 / e->tp : 0);
+  // staged list tile (force mode 1): pb slots per block of 8 entries
+  a.idx_pitch = e->pb;
   a.idx_rows = 0;
   for (auto& h : e->reps)
     if (h.active) a.idx_rows = std::max(a.idx_rows, h.d.max_nbrs);
@@ -301,7 +300,7 @@ EngArgs make_args(b2md_engine* e) {
 // Dynamic shared memory of k_force: pair table [+ staged list tile | position window].
 size_t force_smem(const EngArgs& a, int mode) {
   size_t extra = 0;
-  if (mode == FM_STAGED) extra = (size_t)a.idx_rows * a.idx_pitch * sizeof(unsigned);
+  if (mode == FM_STAGED) extra = (size_t)list_rows(a.idx_rows) * a.idx_pitch * sizeof(unsigned);
   if (mode == FM_WINDOW) extra = (size_t)a.win_cap * sizeof(float4);
   return (size_t)kParSmemFloats * sizeof(float) + extra;
 }
@@ -309,7 +308,7 @@ size_t force_smem(const EngArgs& a, int mode) {
 // Dynamic shared memory of k_rb_build: cut-off table [+ list tile] [+ window scratch].
 size_t build_smem(const b2md_engine* e, const EngArgs& a) {
   const int pb = e->pb;
-  return (size_t)kCs2Floats * sizeof(float) + (e->build_smem ? (size_t)a.idx_rows * (pb + 4) * sizeof(unsigned) : 0) +
+  return (size_t)kCs2Floats * sizeof(float) + (e->build_smem ? (size_t)list_rows(a.idx_rows) * pb * sizeof(unsigned) : 0) +
          (a.win_on ? sizeof(WinTable) : 0);
 }
 
@@ -500,7 +499,7 @@ void place_params(b2md_engine* e, HostRep& h) {
 }
 
 void place_list(b2md_engine* e, HostRep& h, int max_nbrs) {
-  long long len = (long long)max_nbrs * h.np;
+  long long len = (long long)list_rows(max_nbrs) * h.np;
   if (h.nbl0 >= 0) e->ealloc.release(h.nbl0, h.nbl_len);
   long long off = e->ealloc.alloc(len, 32);
   if (off < 0) {
@@ -1472,7 +1471,7 @@ int b2md_nbl_export(b2md_engine* e, int id, unsigned* counts, unsigned* nbl, int
     HostRep& h = get_rep(e, id);
     CK(cudaSetDevice(e->device));
     RepState s = read_state(e, id);
-    std::vector<unsigned> ids(h.n), nn(h.n), lst((size_t)h.d.max_nbrs * h.np);
+    std::vector<unsigned> ids(h.n), nn(h.n), lst((size_t)list_rows(h.d.max_nbrs) * h.np);
     CK(cudaMemcpyAsync(ids.data(), e->uidx[s.abuf] + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
     CK(cudaMemcpyAsync(nn.data(), e->nn + h.p0, h.n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
     CK(cudaMemcpyAsync(lst.data(), e->nbl + h.nbl0, lst.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
@@ -1481,7 +1480,7 @@ int b2md_nbl_export(b2md_engine* e, int id, unsigned* counts, unsigned* nbl, int
       unsigned i = ids[sl];
       unsigned c = std::min<unsigned>(nn[sl], (unsigned)max_nbrs);
       counts[i] = nn[sl];
-      for (unsigned k = 0; k < c; ++k) nbl[(size_t)i * max_nbrs + k] = ids[lst[(size_t)k * h.np + sl]];
+      for (unsigned k = 0; k < c; ++k) nbl[(size_t)i * max_nbrs + k] = ids[lst[lpos(k, (unsigned)sl, h.np)]];
     }
   });
 }

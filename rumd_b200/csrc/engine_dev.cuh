@@ -7,10 +7,14 @@
 //     im[2]   int4    images               (abuf)
 //     uidx[2] uint    original particle id (abuf)  == d_unsorted_index (ParticleData.h:56)
 //     f, w, sts float4 as RUMD (ParticleData.h:41-46); last_r float4; nn uint
-//   list pool: nbl[nbl0 + k*stride + slot]  (column-major per replica, like RUMD's
-//     nbl[k*nvp + i], NeighborList.cu:1293, so a warp's k-th entries are one sector run)
-//   window list: wl[nbl0 + k*stride + slot] (uint16), the same entries as nbl
-//     written as offsets into the tile's position window (see below)
+//   list pool: entry k of slot i at nbl[nbl0 + lpos(k, i, stride)]: blocks of
+//     8 entries, block b of all slots one run (RUMD's nbl[k*nvp + i],
+//     NeighborList.cu:1293, with 8 consecutive entries of a slot packed into
+//     one 32-byte sector: the list build writes a sector per 8 entries and a
+//     thread of the force kernel reads 4 entries with one 16-byte load, while
+//     a warp's loads of one block still cover consecutive sectors)
+//   window list: wl[nbl0 + lpos(k, i, stride)] (uint16), the same entries as
+//     nbl written as offsets into the tile's position window (see below)
 //   cell pools: cnt[cell0 + c], start[cell0 + c] (chunk-local exclusive prefix)
 //   per-tile position window: wseg[tile*kWinSeg + s] = (first slot, length,
 //     window offset, 0) for the slot segments that hold every listed
@@ -35,6 +39,13 @@ constexpr int kGroup = 32;      // tiles per reduction group
 constexpr int kMaxBlock = 512;  // pb*tp limit (launch bounds)
 constexpr int kWinSeg = 128;    // slot segments per tile position window
 constexpr int kWinBase = 4;     // cell rows (y, z) a tile may span for a window
+
+// Place of list entry k of slot i in a replica's list (stride = its slots).
+__host__ __device__ __forceinline__ size_t lpos(unsigned k, unsigned i, size_t stride) {
+  return (size_t)(k >> 3) * (stride << 3) + ((size_t)i << 3) + (k & 7u);
+}
+// List rows allocated for a capacity of max_nbrs entries (whole blocks of 8).
+__host__ __device__ __forceinline__ int list_rows(int max_nbrs) { return (max_nbrs + 7) & ~7; }
 
 enum { P_PE = 0, P_W, P_KE2, P_KET, P_PX, P_PY, P_PZ, P_M };
 enum { CUT_NS = 0, CUT_SP = 1, CUT_SF = 2 };
@@ -112,7 +123,7 @@ struct EngArgs {
   double* elog;
   int ntiles;
   int nrep;
-  int idx_pitch;  // k_force: shared-memory row pitch of the staged list tile (pb + bank padding)
+  int idx_pitch;  // k_force: slots per staged list block (pb)
   int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
   unsigned short* wl;  // window list (force mode 2)
   int4* wseg;          // per-tile window segments

@@ -311,24 +311,106 @@ __device__ __forceinline__ unsigned ld_stream_u16(const unsigned short* p) {
   return v;
 }
 
-// List-entry readers for force_loop: entry k of the particle's column.
-// Staged: the tile's list copied to shared memory (row pitch `pitch`).
+__device__ __forceinline__ uint4 ld_stream_v4(const unsigned* p) {
+  uint4 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+
+__device__ __forceinline__ uint2 ld_stream_v2(const unsigned* p) {
+  uint2 v;
+  asm volatile("ld.global.nc.L1::no_allocate.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+  return v;
+}
+
+// The list entries one of a particle's TP lanes handles: with E = 8/TP, lane
+// t takes entries 8m + E t + (0 .. E-1) of every block m of 8, so its q-th
+// entry is lane_entry(q).  Four consecutive q (q a multiple of 4) are one
+// 16-byte run of a block when E >= 4, two 8-byte runs when E = 2, and four
+// single entries when E = 1.
+template <int TP>
+__device__ __forceinline__ unsigned lane_entry(unsigned q, unsigned t) {
+  constexpr unsigned E = 8 / TP;
+  return 8u * (q / E) + E * t + q % E;
+}
+
+// The number of this lane's entries below nn.
+template <int TP>
+__device__ __forceinline__ unsigned lane_count(unsigned nn, unsigned t) {
+  constexpr int E = 8 / TP;
+  const int rem = (int)(nn & 7u) - E * (int)t;
+  return (nn >> 3) * (unsigned)E + (unsigned)min(E, max(0, rem));
+}
+
+// List-entry readers for force_loop: one(k) is entry k of the particle;
+// group<TP>(q, t) is lane t's entries q .. q+3 (q a multiple of 4).
+// Streamed: read from the global list inside the loop, past L1.
+struct IdxStreamed {
+  const unsigned* base;  // the replica's list
+  unsigned i;            // the particle's slot
+  size_t stride;
+  __device__ __forceinline__ unsigned one(unsigned k) const { return ld_stream(base + lpos(k, i, stride)); }
+  template <int TP>
+  __device__ __forceinline__ uint4 group(unsigned q, unsigned t) const {
+    constexpr unsigned E = 8 / TP;
+    if (E >= 4) return ld_stream_v4(base + lpos(lane_entry<TP>(q, t), i, stride));
+    if (E == 2) {
+      const uint2 a = ld_stream_v2(base + lpos(lane_entry<TP>(q, t), i, stride));
+      const uint2 b = ld_stream_v2(base + lpos(lane_entry<TP>(q + 2, t), i, stride));
+      return make_uint4(a.x, a.y, b.x, b.y);
+    }
+    return make_uint4(one(lane_entry<TP>(q, t)), one(lane_entry<TP>(q + 1, t)), one(lane_entry<TP>(q + 2, t)),
+                      one(lane_entry<TP>(q + 3, t)));
+  }
+};
+// Staged: the tile's list blocks copied to shared memory, block b of slot lp
+// at p[(b * pb + lp) * 8]; p points at this particle's first block.
 struct IdxStaged {
   const unsigned* p;
-  int pitch;
-  __device__ __forceinline__ unsigned operator()(unsigned k) const { return p[k * pitch]; }
+  int bstride;  // pb * 8
+  __device__ __forceinline__ unsigned one(unsigned k) const { return p[(k >> 3) * bstride + (k & 7u)]; }
+  template <int TP>
+  __device__ __forceinline__ uint4 group(unsigned q, unsigned t) const {
+    constexpr unsigned E = 8 / TP;
+    if (E >= 4) {
+      const unsigned k = lane_entry<TP>(q, t);
+      return *reinterpret_cast<const uint4*>(p + (k >> 3) * bstride + (k & 7u));
+    }
+    if (E == 2) {
+      const unsigned k0 = lane_entry<TP>(q, t), k1 = lane_entry<TP>(q + 2, t);
+      const uint2 a = *reinterpret_cast<const uint2*>(p + (k0 >> 3) * bstride + (k0 & 7u));
+      const uint2 b = *reinterpret_cast<const uint2*>(p + (k1 >> 3) * bstride + (k1 & 7u));
+      return make_uint4(a.x, a.y, b.x, b.y);
+    }
+    return make_uint4(one(lane_entry<TP>(q, t)), one(lane_entry<TP>(q + 1, t)), one(lane_entry<TP>(q + 2, t)),
+                      one(lane_entry<TP>(q + 3, t)));
+  }
 };
-// Streamed: read from the global list inside the loop (ld_stream).
-struct IdxStreamed {
-  const unsigned* p;
-  size_t stride;
-  __device__ __forceinline__ unsigned operator()(unsigned k) const { return ld_stream(p + k * stride); }
-};
-// Window: the 16-bit window list (offsets into the tile's position window).
+// Window: the 16-bit window list (offsets into the tile's position window),
+// in the list's layout.
 struct IdxWindow {
-  const unsigned short* p;
+  const unsigned short* base;
+  unsigned i;
   size_t stride;
-  __device__ __forceinline__ unsigned operator()(unsigned k) const { return ld_stream_u16(p + k * stride); }
+  __device__ __forceinline__ unsigned one(unsigned k) const { return ld_stream_u16(base + lpos(k, i, stride)); }
+  template <int TP>
+  __device__ __forceinline__ uint4 group(unsigned q, unsigned t) const {
+    constexpr unsigned E = 8 / TP;
+    if (E >= 4) {
+      // four 16-bit entries = 8 bytes
+      const uint2 w = ld_stream_v2(reinterpret_cast<const unsigned*>(base + lpos(lane_entry<TP>(q, t), i, stride)));
+      return make_uint4(w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16);
+    }
+    if (E == 2) {
+      const unsigned a = ld_stream(reinterpret_cast<const unsigned*>(base + lpos(lane_entry<TP>(q, t), i, stride)));
+      const unsigned b =
+          ld_stream(reinterpret_cast<const unsigned*>(base + lpos(lane_entry<TP>(q + 2, t), i, stride)));
+      return make_uint4(a & 0xffffu, a >> 16, b & 0xffffu, b >> 16);
+    }
+    return make_uint4(one(lane_entry<TP>(q, t)), one(lane_entry<TP>(q + 1, t)), one(lane_entry<TP>(q + 2, t)),
+                      one(lane_entry<TP>(q + 3, t)));
+  }
 };
 
 // Neighbour-position readers: gathered from global memory (through L1), or
@@ -342,52 +424,25 @@ struct PosWindow {
   __device__ __forceinline__ float4 operator()(unsigned j) const { return p[j]; }
 };
 
-// Neighbour positions in flight per thread in force_loop, and whether the
-// next group's list entries are loaded one group ahead.
-constexpr int kForceUnroll = 4;
-constexpr bool kForcePipeline = false;
-
-// The neighbour loop of one thread: entries k = lane_t, lane_t + TP, ... of
-// the particle's list column, kForceUnroll neighbour positions in flight.
+// The neighbour loop of one thread: its entries (lane_entry) in groups of
+// four -- one vector load of list entries, four neighbour positions in
+// flight -- then the remaining ones singly.  Only entries below nn are read.
 template <int TP, bool STRESS, bool WRAP, class Idx, class Pos>
 __device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos& pos, unsigned lane_t, unsigned nn,
                                            const float4& ri, const float* prow, float Lx, float Ly, float Lz,
                                            float iLx, float iLy, float iLz) {
-  constexpr int U = kForceUnroll;
-  unsigned k = lane_t;
-  if (kForcePipeline) {
-    // the next group's list entries are loaded while this group's positions
-    // are gathered and summed
-    unsigned jn[U];
-    if (k + (U - 1) * TP < nn) {
-#pragma unroll
-      for (int u = 0; u < U; ++u) jn[u] = idx(k + u * TP);
-    }
-    for (; k + (U - 1) * TP < nn; k += U * TP) {
-      float4 rj[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) rj[u] = pos(jn[u]);
-      if (k + U * TP + (U - 1) * TP < nn) {
-#pragma unroll
-        for (int u = 0; u < U; ++u) jn[u] = idx(k + U * TP + u * TP);
-      }
-#pragma unroll
-      for (int u = 0; u < U; ++u) lj_pair<STRESS, WRAP>(A, ri, rj[u], prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    }
-  } else {
-    for (; k + (U - 1) * TP < nn; k += U * TP) {
-      unsigned j[U];
-      float4 rj[U];
-#pragma unroll
-      for (int u = 0; u < U; ++u) j[u] = idx(k + u * TP);
-#pragma unroll
-      for (int u = 0; u < U; ++u) rj[u] = pos(j[u]);
-#pragma unroll
-      for (int u = 0; u < U; ++u) lj_pair<STRESS, WRAP>(A, ri, rj[u], prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    }
+  const unsigned cnt = lane_count<TP>(nn, lane_t);
+  unsigned q = 0;
+  for (; q + 4 <= cnt; q += 4) {
+    const uint4 j = idx.template group<TP>(q, lane_t);
+    const float4 r0 = pos(j.x), r1 = pos(j.y), r2 = pos(j.z), r3 = pos(j.w);
+    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
-  for (; k < nn; k += TP) {
-    const float4 r0 = pos(idx(k));
+  for (; q < cnt; ++q) {
+    const float4 r0 = pos(idx.one(lane_entry<TP>(q, lane_t)));
     lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
 }
@@ -478,14 +533,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
       __syncthreads();
       const unsigned rows = min(s_rows, (unsigned)a.idx_rows);
-      // 2. one TMA bulk copy per list row: slots [first, first+width) of rows 0..rows-1
+      // 2. one TMA bulk copy per list block of 8 entries: slots [first, first+width)
+      //    of blocks 0 .. ceil(rows/8)-1, each a contiguous run of width*32 bytes
       if (threadIdx.x < 32) {
         const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
-        if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, rows * width * 4u);
+        const unsigned nblk = (rows + 7u) >> 3;
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, nblk * width * 32u);
         __syncwarp();
-        const unsigned* src = a.nbl + R.nbl0 + first;
-        for (unsigned r = threadIdx.x; r < rows; r += 32)
-          bulk_g2s(s_idx + r * pitch, src + (size_t)r * R.nbl_stride, width * 4u, &s_bar);
+        const unsigned* src = a.nbl + R.nbl0 + (size_t)first * 8;
+        for (unsigned b = threadIdx.x; b < nblk; b += 32)
+          bulk_g2s(s_idx + b * pitch * 8, src + (size_t)b * R.nbl_stride * 8, width * 32u, &s_bar);
       }
     } else if (MODE == FM_WINDOW && wm.x >= 0) {
       // 1-2. one TMA bulk copy per window segment (16-byte aligned float4 runs)
@@ -512,8 +569,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     const float* prow = s_par + ti * nt * kParStride;
     const unsigned nn = valid ? a.nn[R.p0 + i] : 0u;
     const size_t lstride = (size_t)R.nbl_stride;
-    const unsigned* lcol = a.nbl + R.nbl0 + i;
-    const unsigned short* wcol = a.wl + R.nbl0 + i;
+    const unsigned* lbase = a.nbl + R.nbl0;
+    const unsigned short* wbase = a.wl + R.nbl0;
     // A particle farther than rc_max + 2 skin from every face of the box has
     // all its listed neighbours (within rc + skin at the build, each moved at
     // most skin/2 since) inside the box at their minimum image, so the
@@ -527,10 +584,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
       if (ok) {
         if (MODE == FM_STAGED)
-          force_loop_any<TP, STRESS>(fast, A, IdxStaged{s_idx + lp, pitch}, PosGlobal{rc}, lane_t, nn, ri, prow,
+          force_loop_any<TP, STRESS>(fast, A, IdxStaged{s_idx + lp * 8, pitch * 8}, PosGlobal{rc}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
         else
-          force_loop_any<TP, STRESS>(fast, A, IdxWindow{wcol, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
+          force_loop_any<TP, STRESS>(fast, A, IdxWindow{wbase, (unsigned)i, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
       } else {
         // the copies did not land in time: record it for the host and wait
@@ -540,7 +597,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     } else {
       __syncthreads();  // the pair table
-      force_loop_any<TP, STRESS>(fast, A, IdxStreamed{lcol, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
+      force_loop_any<TP, STRESS>(fast, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
                                  Lz, iLx, iLy, iLz);
     }
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
@@ -1177,7 +1234,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   RepState* S = a.st + rep;
   const int nt = R.ntypes;
   const int pb = blockDim.x / LP;
-  const int lpitch = pb + 4;  // rows 16 bytes apart: a group's LP rows fall in different banks
+  // shared-memory list tile: block b (8 entries) of slot lp at s_list[(b * pb + lp) * 8]
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
   if (threadIdx.x == 0) {
     s_max = 0;
@@ -1201,11 +1258,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   // this particle's list column, held in registers: the list stores below
   // cannot alias the replica table as far as the compiler can tell, so
   // reading R.nbl0 / R.nbl_stride in the loop would reload them after every store
-  unsigned* __restrict__ col = a.nbl + R.nbl0 + i;
-  unsigned short* __restrict__ wcol = a.wl + R.nbl0 + i;
+  unsigned* __restrict__ lbase = a.nbl + R.nbl0;
+  unsigned short* __restrict__ wbase = a.wl + R.nbl0;
   const size_t lstride = (size_t)R.nbl_stride;
   WinTable* ws = reinterpret_cast<WinTable*>(
-      s_dyn + kCs2Floats * sizeof(float) + (SMEM_LIST ? (size_t)a.idx_rows * lpitch * sizeof(unsigned) : 0));
+      s_dyn + kCs2Floats * sizeof(float) + (SMEM_LIST ? (size_t)list_rows(a.idx_rows) * pb * sizeof(unsigned) : 0));
   bool win_ok = false;
   if (WIN) {
     // the tile's window segments (k_rb_window), sorted by first slot
@@ -1245,9 +1302,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
       if (in) {
         const int pos = count + __popc(g & below);
         if (pos < maxn) {
-          if (SMEM_LIST) s_list[pos * lpitch + lp] = (unsigned)j;
-          else col[(size_t)pos * lstride] = (unsigned)j;
-          if (WIN && win_ok) wcol[(size_t)pos * lstride] = (unsigned short)(j + delta);
+          if (SMEM_LIST) s_list[((pos >> 3) * pb + lp) * 8 + (pos & 7)] = (unsigned)j;
+          else lbase[lpos((unsigned)pos, (unsigned)i, lstride)] = (unsigned)j;
+          if (WIN && win_ok) wbase[lpos((unsigned)pos, (unsigned)i, lstride)] = (unsigned short)(j + delta);
         }
       }
       count += __popc(g);
@@ -1335,11 +1392,11 @@ __global__ void __launch_bounds__(kMaxBlock) k_rb_build(EngArgs a) {
   __syncthreads();
   if (WIN && win_ok && threadIdx.x == 0 && s_winbad) a.wmeta[tile] = make_int2(-1, -1);
   if (SMEM_LIST && threadIdx.x < 32) {
-    const int rows = min(s_max, maxn);
+    const int nblk = (min(s_max, maxn) + 7) >> 3;
     const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
-    unsigned* dst = a.nbl + R.nbl0 + first;
-    for (int r = threadIdx.x; r < rows; r += 32)
-      bulk_s2g(dst + (size_t)r * R.nbl_stride, s_list + r * lpitch, width * 4u);
+    unsigned* dst = a.nbl + R.nbl0 + (size_t)first * 8;
+    for (int b = threadIdx.x; b < nblk; b += 32)
+      bulk_s2g(dst + (size_t)b * R.nbl_stride * 8, s_list + b * pb * 8, width * 32u);
     bulk_commit();
     bulk_wait_all();
   }
@@ -1471,7 +1528,7 @@ __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
         for (int p = pg; p < pe; ++p) {
           const float4 ri = rc[p];
           const float* cs2 = s_cs2 + __float_as_int(ri.w) * nt;
-          unsigned* __restrict__ col = lbase + p;
+
           int count = __shfl_sync(FULL, cnt_reg, p - pg);
           for (int v0 = 0; v0 < mc; v0 += 32) {
             const int v = v0 + lane;
@@ -1491,7 +1548,7 @@ __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
             const unsigned g = __ballot_sync(FULL, in);
             if (in) {
               const int pos = count + __popc(g & lt);
-              if (pos < maxn) col[(size_t)pos * lstride] = (unsigned)j;
+              if (pos < maxn) lbase[lpos((unsigned)pos, (unsigned)p, lstride)] = (unsigned)j;
             }
             count += __popc(g);
           }
