@@ -56,6 +56,8 @@ def parse():
     p.add_argument("--sm-tiles", type=int, default=None, help="kernel variant: 1 = SM-region tile claiming")
     p.add_argument("--profile-launches", action="store_true",
                    help="small plain run only (for the ncu launch list)")
+    p.add_argument("--lj1m", action="store_true",
+                   help="only the HBM-scale plain workload: single-component LJ, N=1,048,576 (one JSON line)")
     return p.parse_args()
 
 
@@ -347,6 +349,43 @@ def served(capi, device, pb, tp, njobs, seed=0):
                       "arrival)"}
 
 
+def lj_hbm_scale(capi, device, args):
+    """The HBM-scale plain configuration: single-component LJ (SF rc = 2.5),
+    N = 1,048,576 (4 x 64^3 FCC), density 0.8442, T = 0.722, NVT tau = 0.2,
+    dt = 0.004, skin 0.3.  The list (about 320 MB) no longer fits in L2, so the
+    force kernel's bytes come from HBM.  Prints one JSON line (not the
+    headline)."""
+    from rumd_b200 import initconf as I
+    n = 1048576
+    c = I.lj_config(n, density=0.8442, T=2.0, seed=3)
+    params = I.lj_params(1, I.LJ)
+    e = new_engine(capi, device=device, pb=args.pb, tp=args.tp)
+    rid = e.add(c["pos4"], c["box"], params, 1, cutoff="SF", skin=SKIN, dt=0.004, T=2.0, tau=TAU, vel4=c["vel4"])
+    e.run(500)
+    e.set_integrator(rid, 0.004, 0.722, TAU)
+    e.run(1000)
+    steps = max(args.steps, 1)
+    r0 = e.stats(rid)["rebuilds"]
+    flush_l2(device)
+    t = time_run(capi, e, steps, device)
+    rebuilds = e.stats(rid)["rebuilds"] - r0
+    kms, _ = e.run_timed(200)
+    st = e.stats(rid)
+    per_launch_s = kms / 200 / 1e3
+    bytes_alg = n * (168.0 + 4.0 * st["mean_nbrs"])
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_alg / per_launch_s / 1e9
+    print(json.dumps({"workload": "single-component LJ, N=1048576, rho=0.8442, T=0.722, NVT tau=0.2, dt=0.004, "
+                                  "skin 0.3, SF rc=2.5 (plain method, HBM scale)",
+                      "value": n * steps / t, "unit": "particle-steps/s", "steps": steps,
+                      "ms_per_step": t / steps * 1e3, "rebuilds": rebuilds, "pb": args.pb, "tp": args.tp,
+                      "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                   "frac": achieved / peak, "peak_source": peak_kind,
+                                   "kernel_ms": per_launch_s * 1e3, "bytes_per_launch_alg": bytes_alg,
+                                   "mean_list_length": st["mean_nbrs"]}}), flush=True)
+    e.close()
+
+
 def config_block(args, world, engine=None):
     variants = {}
     if engine is not None:
@@ -407,6 +446,10 @@ def main():
     KERNEL_VARIANTS[capi.VARIANT_BUILD_LANES] = args.build_lanes
     KERNEL_VARIANTS[capi.VARIANT_SM_TILES] = args.sm_tiles
     device = local
+    if args.lj1m:
+        lj_hbm_scale(capi, device, args)
+        dist.close()
+        return
     if args.profile_launches:
         # Same workload driven with eager launches only (b2md_run_timed): the
         # kernels and their order are those of the graphs, but ncu sees plain

@@ -1525,34 +1525,52 @@ __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
         __syncwarp();
         for (int v = lane; v < mc; v += 32) wpos[v] = __ldg(rc + wslot[v]);
         __syncwarp();
-        for (int p = pg; p < pe; ++p) {
-          const float4 ri = rc[p];
-          const float* cs2 = s_cs2 + __float_as_int(ri.w) * nt;
-
-          int count = __shfl_sync(FULL, cnt_reg, p - pg);
+        // two particles at a time: each staged candidate is read once and
+        // tested against both (the second is a copy of the first when the
+        // cell has an odd count; its results are discarded)
+        for (int p = pg; p < pe; p += 2) {
+          const bool two = p + 1 < pe;
+          const int p1 = two ? p + 1 : p;
+          const float4 ra = rc[p], rb = rc[p1];
+          const float* cs2a = s_cs2 + __float_as_int(ra.w) * nt;
+          const float* cs2b = s_cs2 + __float_as_int(rb.w) * nt;
+          int ca = __shfl_sync(FULL, cnt_reg, p - pg);
+          int cb = __shfl_sync(FULL, cnt_reg, p1 - pg);
           for (int v0 = 0; v0 < mc; v0 += 32) {
             const int v = v0 + lane;
-            bool in = false;
+            bool ina = false, inb = false;
             int j = 0;
             if (v < mc) {
               j = wslot[v];
               const float4 rj = wpos[v];
-              float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
+              const int tj = __float_as_int(rj.w);
+              float ax = ra.x - rj.x, ay = ra.y - rj.y, az = ra.z - rj.z;
+              float bx = rb.x - rj.x, by = rb.y - rj.y, bz = rb.z - rj.z;
               if (wrap) {
-                dx = mi_comp(dx, Lx, iLx);
-                dy = mi_comp(dy, Ly, iLy);
-                dz = mi_comp(dz, Lz, iLz);
+                ax = mi_comp(ax, Lx, iLx);
+                ay = mi_comp(ay, Ly, iLy);
+                az = mi_comp(az, Lz, iLz);
+                bx = mi_comp(bx, Lx, iLx);
+                by = mi_comp(by, Ly, iLy);
+                bz = mi_comp(bz, Lz, iLz);
               }
-              in = (j != p) && dist2_ref(dx, dy, dz) < cs2[__float_as_int(rj.w)];
+              ina = (j != p) && dist2_ref(ax, ay, az) < cs2a[tj];
+              inb = two && (j != p1) && dist2_ref(bx, by, bz) < cs2b[tj];
             }
-            const unsigned g = __ballot_sync(FULL, in);
-            if (in) {
-              const int pos = count + __popc(g & lt);
+            const unsigned ga = __ballot_sync(FULL, ina), gb = __ballot_sync(FULL, inb);
+            if (ina) {
+              const int pos = ca + __popc(ga & lt);
               if (pos < maxn) lbase[lpos((unsigned)pos, (unsigned)p, lstride)] = (unsigned)j;
             }
-            count += __popc(g);
+            if (inb) {
+              const int pos = cb + __popc(gb & lt);
+              if (pos < maxn) lbase[lpos((unsigned)pos, (unsigned)p1, lstride)] = (unsigned)j;
+            }
+            ca += __popc(ga);
+            cb += __popc(gb);
           }
-          if (lane == p - pg) cnt_reg = count;
+          if (lane == p - pg) cnt_reg = ca;
+          if (two && lane == p1 - pg) cnt_reg = cb;
         }
       }
       if (pg + lane < pe) {
