@@ -365,6 +365,17 @@ def lj_hbm_scale(capi, device, args):
     e.set_integrator(rid, 0.004, 0.722, TAU)
     e.run(1000)
     steps = max(args.steps, 1)
+    if args.profile_launches:
+        # eager launches of `steps` steps between cudaProfilerStart/Stop (for ncu)
+        import torch
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.start()
+        ms, nl = e.run_timed(steps)
+        torch.cuda.synchronize(device)
+        torch.cuda.profiler.stop()
+        print(json.dumps({"profile_steps": steps, "step_kernel_ms_avg": ms / steps, "launches": nl}), flush=True)
+        e.close()
+        return
     r0 = e.stats(rid)["rebuilds"]
     flush_l2(device)
     t = time_run(capi, e, steps, device)

@@ -142,6 +142,10 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *   B2MD_VARIANT_WINDOW_CAP    mode 2: window capacity in particles (shared
  *                              memory of the force kernel, 16 bytes each);
  *                              tiles with larger windows stream.
+ *   B2MD_VARIANT_WINDOW_LIST_ROWS  mode 2: rows (multiple of 8) of the 16-bit
+ *                              window list copied to shared memory with the
+ *                              window; a tile whose longest list is longer
+ *                              reads its list from global memory.  0: never.
  *   B2MD_VARIANT_SM_TILES      mode 0: 1 = the force kernel runs as many
  *                              blocks as fit on the GPU, and each block claims
  *                              tiles from its SM's share of the tile range,
@@ -153,7 +157,8 @@ enum {
   B2MD_VARIANT_BUILD_LANES = 1,
   B2MD_VARIANT_BUILD_SMEM = 2,
   B2MD_VARIANT_WINDOW_CAP = 3,
-  B2MD_VARIANT_SM_TILES = 4
+  B2MD_VARIANT_SM_TILES = 4,
+  B2MD_VARIANT_WINDOW_LIST_ROWS = 5
 };
 B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
 B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);

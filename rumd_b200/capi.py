@@ -18,6 +18,7 @@ B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_O
 CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
 # kernel variants (b2md_engine_set_variant)
 VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP, VARIANT_SM_TILES = 0, 1, 2, 3, 4
+VARIANT_WINDOW_LIST_ROWS = 5
 FORCE_STREAMED, FORCE_STAGED, FORCE_WINDOW = 0, 1, 2
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",

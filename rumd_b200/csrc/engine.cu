@@ -134,6 +134,7 @@ struct b2md_engine {
   int nsm = 0;                 // streaming multiprocessors of the device
   unsigned* smctr = nullptr;   // SM-region claim counters (nsm + 1)
   int win_cap = 2560;          // FM_WINDOW: window capacity in particles
+  int wl_rows_cap = 128;       // FM_WINDOW: window-list rows staged in shared memory (0 = stream)
   int build_lanes = 32;        // list build: lanes per particle (32: one warp per cell)
   bool build_smem = false;     // list build: tile assembled in shared memory
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
@@ -294,6 +295,7 @@ EngArgs make_args(b2md_engine* e) {
   a.nreg = (e->sm_tiles && e->force_mode == FM_STREAMED) ? e->nsm : 0;
   a.smctr = e->smctr;
   a.win_cap = e->win_cap;
+  a.wl_rows = e->force_mode == FM_WINDOW ? std::min(list_rows(a.idx_rows), e->wl_rows_cap & ~7) : 0;
   return a;
 }
 
@@ -301,7 +303,8 @@ EngArgs make_args(b2md_engine* e) {
 size_t force_smem(const EngArgs& a, int mode) {
   size_t extra = 0;
   if (mode == FM_STAGED) extra = (size_t)list_rows(a.idx_rows) * a.idx_pitch * sizeof(unsigned);
-  if (mode == FM_WINDOW) extra = (size_t)a.win_cap * sizeof(float4);
+  if (mode == FM_WINDOW)
+    extra = (size_t)a.win_cap * sizeof(float4) + (size_t)a.wl_rows * a.idx_pitch * sizeof(unsigned short);
   return (size_t)kParSmemFloats * sizeof(float) + extra;
 }
 
@@ -913,6 +916,11 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
       }
       e->force_mode = value;
       break;
+    case B2MD_VARIANT_WINDOW_LIST_ROWS:
+      if (value < 0 || value > 1024 || value % 8 != 0)
+        return fail(B2MD_ERR_ARG, "window-list rows must be a multiple of 8 in 0..1024 (got %d)", value);
+      e->wl_rows_cap = value;
+      break;
     case B2MD_VARIANT_SM_TILES:
       if (value != 0 && value != 1) return fail(B2MD_ERR_ARG, "sm_tiles must be 0 or 1");
       e->sm_tiles = value != 0;
@@ -947,6 +955,7 @@ int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
   switch (which) {
     case B2MD_VARIANT_FORCE_MODE: *value = e->force_mode; break;
     case B2MD_VARIANT_SM_TILES: *value = e->sm_tiles ? 1 : 0; break;
+    case B2MD_VARIANT_WINDOW_LIST_ROWS: *value = e->wl_rows_cap; break;
     case B2MD_VARIANT_WINDOW_CAP: *value = e->win_cap; break;
     case B2MD_VARIANT_BUILD_LANES: *value = e->build_lanes; break;
     case B2MD_VARIANT_BUILD_SMEM: *value = e->build_smem ? 1 : 0; break;

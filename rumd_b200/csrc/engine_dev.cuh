@@ -130,6 +130,7 @@ struct EngArgs {
   int2* wmeta;         // per-tile (segments, particles)
   int win_on;          // list builds also build the windows
   int win_cap;         // window capacity in particles (shared memory of k_force)
+  int wl_rows;         // window-list rows k_force stages in shared memory (multiple of 8; 0 = none)
   int nreg;            // SM regions for k_force tile claiming (0 = one tile per block)
   unsigned* smctr;     // per-region claim counters [nreg] + tiles claimed [nreg]
 };

@@ -413,6 +413,32 @@ struct IdxWindow {
   }
 };
 
+// Window, staged: the tile's 16-bit window-list blocks copied to shared
+// memory, block b of slot lp at p[(b * pb + lp) * 8]; p points at this
+// particle's first block.
+struct IdxWindowStaged {
+  const unsigned short* p;
+  int bstride;  // pb * 8
+  __device__ __forceinline__ unsigned one(unsigned k) const { return p[(k >> 3) * bstride + (k & 7u)]; }
+  template <int TP>
+  __device__ __forceinline__ uint4 group(unsigned q, unsigned t) const {
+    constexpr unsigned E = 8 / TP;
+    if (E >= 4) {
+      const unsigned k = lane_entry<TP>(q, t);
+      const uint2 w = *reinterpret_cast<const uint2*>(p + (k >> 3) * bstride + (k & 7u));
+      return make_uint4(w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16);
+    }
+    if (E == 2) {
+      const unsigned k0 = lane_entry<TP>(q, t), k1 = lane_entry<TP>(q + 2, t);
+      const unsigned a = *reinterpret_cast<const unsigned*>(p + (k0 >> 3) * bstride + (k0 & 7u));
+      const unsigned b = *reinterpret_cast<const unsigned*>(p + (k1 >> 3) * bstride + (k1 & 7u));
+      return make_uint4(a & 0xffffu, a >> 16, b & 0xffffu, b >> 16);
+    }
+    return make_uint4(one(lane_entry<TP>(q, t)), one(lane_entry<TP>(q + 1, t)), one(lane_entry<TP>(q + 2, t)),
+                      one(lane_entry<TP>(q + 3, t)));
+  }
+};
+
 // Neighbour-position readers: gathered from global memory (through L1), or
 // from the tile's position window in shared memory.
 struct PosGlobal {
@@ -481,6 +507,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
+  unsigned short* s_wl = reinterpret_cast<unsigned short*>(s_win + a.win_cap);  // mode 2: staged window list
   __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
   __shared__ double s_scr[kMaxBlock];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
@@ -523,7 +550,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
       __syncthreads();
     }
-    if (MODE == FM_STAGED) {
+    if (MODE == FM_STAGED || (MODE == FM_WINDOW && wm.x >= 0 && a.wl_rows > 0)) {
       // 1. rows of the list this tile needs: the largest neighbour count in it
       {
         unsigned c = (threadIdx.x < pb && first + (int)threadIdx.x < R.n) ? a.nn[R.p0 + first + threadIdx.x] : 0u;
@@ -532,6 +559,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
         if ((threadIdx.x & 31) == 0 && c) atomicMax(&s_rows, c);
       }
       __syncthreads();
+    }
+    bool wl_staged = false;
+    if (MODE == FM_STAGED) {
       const unsigned rows = min(s_rows, (unsigned)a.idx_rows);
       // 2. one TMA bulk copy per list block of 8 entries: slots [first, first+width)
       //    of blocks 0 .. ceil(rows/8)-1, each a contiguous run of width*32 bytes
@@ -545,15 +575,24 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
           bulk_g2s(s_idx + b * pitch * 8, src + (size_t)b * R.nbl_stride * 8, width * 32u, &s_bar);
       }
     } else if (MODE == FM_WINDOW && wm.x >= 0) {
-      // 1-2. one TMA bulk copy per window segment (16-byte aligned float4 runs)
+      // 1-2. one TMA bulk copy per window segment (16-byte aligned float4 runs),
+      //      and, when the tile's list fits the staged rows, one per block of 8
+      //      window-list entries (width*16 bytes)
+      const unsigned wrows = a.wl_rows > 0 ? s_rows : 0u;
+      wl_staged = a.wl_rows > 0 && wrows <= (unsigned)a.wl_rows;
       if (threadIdx.x < 32) {
-        if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, (unsigned)wm.y * 16u);
+        const unsigned width = (unsigned)min(pb, R.nbl_stride - first);
+        const unsigned nblk = wl_staged ? (wrows + 7u) >> 3 : 0u;
+        if (threadIdx.x == 0) mbar_arrive_expect_tx(&s_bar, (unsigned)wm.y * 16u + nblk * width * 16u);
         __syncwarp();
         const int4* seg = a.wseg + (size_t)tile * kWinSeg;
         for (int sgi = threadIdx.x; sgi < wm.x; sgi += 32) {
           const int4 sg = seg[sgi];
           bulk_g2s(s_win + sg.z, rc + sg.x, (unsigned)sg.y * 16u, &s_bar);
         }
+        const unsigned short* src = a.wl + R.nbl0 + (size_t)first * 8;
+        for (unsigned b = threadIdx.x; b < nblk; b += 32)
+          bulk_g2s(s_wl + b * pitch * 8, src + (size_t)b * R.nbl_stride * 8, width * 16u, &s_bar);
       }
     }
     // 3. meanwhile: pair table and this particle's data
@@ -586,6 +625,9 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
         if (MODE == FM_STAGED)
           force_loop_any<TP, STRESS>(fast, A, IdxStaged{s_idx + lp * 8, pitch * 8}, PosGlobal{rc}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
+        else if (wl_staged)
+          force_loop_any<TP, STRESS>(fast, A, IdxWindowStaged{s_wl + lp * 8, pitch * 8}, PosWindow{s_win}, lane_t, nn,
+                                     ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
         else
           force_loop_any<TP, STRESS>(fast, A, IdxWindow{wbase, (unsigned)i, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
