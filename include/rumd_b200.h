@@ -51,6 +51,13 @@ extern "C" {
 #define B2MD_CUTOFF_SP 1
 #define B2MD_CUTOFF_SF 2
 
+/* pair functions: which RUMD class the parameter table rows belong to */
+#define B2MD_POT_LJ_12_6 0            /* Pot_LJ_12_6 / Pot_IPL_12_6: p0 rc, p1 A12, p2 A6 */
+#define B2MD_POT_LJ_12_6_SMOOTH_2_4 1 /* Pot_LJ_12_6_smooth_2_4 (PairPotential.h:218-256):
+                                         p0 rc, p1 1/sigma^2, p2 4 eps, p3 c2, p4 c4 */
+#define B2MD_POT_IPL_N 2              /* Pot_IPL_n (PairPotential.h:603-637):
+                                         p0 rc, p1 1/sigma^2, p2 eps, p3 n */
+
 /* fields for b2md_replica_get / b2md_replica_set */
 #define B2MD_FIELD_POS 0
 #define B2MD_FIELD_VEL 1
@@ -99,6 +106,7 @@ typedef struct {
   int max_nbrs;             /* list capacity per particle (0 = density estimate)   */
   int energy_interval;      /* log (pe, W, KE, xi) every k steps (0 = off)         */
   int energy_capacity;      /* number of log entries kept                          */
+  int potential;            /* B2MD_POT_* (0: LJ 12-6)                             */
 } b2md_replica_desc;
 
 /* Engine lifetime.  Replaces the allocation that RUMD spreads over
@@ -175,10 +183,11 @@ B2MD_API int b2md_replica_get(b2md_engine* e, int id, int field, void* out);
  * with reset_sorting, ParticleData.cu:333-355).  Setting positions forces a
  * neighbour-list rebuild before the next force evaluation. */
 B2MD_API int b2md_replica_set(b2md_engine* e, int id, int field, const void* in);
-/* Pair parameter table / cut-off method / skin (PairPotential::SetParams +
- * CopyParamsToGPU, PairPotential.cu:82-125; SetNbListSkin). */
+/* Pair parameter table / cut-off method / skin / pair function
+ * (PairPotential::SetParams + CopyParamsToGPU, PairPotential.cu:82-125;
+ * SetNbListSkin; Sample::SetPotential with another Pot_* class). */
 B2MD_API int b2md_replica_set_potential(b2md_engine* e, int id, int ntypes, const float* params,
-                               int cutoff_method, float skin);
+                               int cutoff_method, float skin, int potential);
 /* Integrator settings (IntegratorNVT::SetTimeStep, SetTargetTemperature,
  * SetRelaxationTime, SetThermostatState, SetThermostatOn*,
  * SetTemperatureChangePerTimeStep; IntegratorNVT.cu:132-190). */

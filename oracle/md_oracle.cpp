@@ -9,6 +9,8 @@
 // Parity anchors (reference paths are relative to the RUMD source tree):
 //   * Pot_LJ_12_6::SetParams            include/rumd/PairPotential.h:202-207
 //   * Pot_IPL_12_6::ComputeInteraction  include/rumd/PairPotential.h:161-168
+//   * Pot_LJ_12_6_smooth_2_4            include/rumd/PairPotential.h:218-256
+//   * Pot_IPL_n                         include/rumd/PairPotential.h:603-637
 //   * fij (NS/SP/SF cut-off handling)   include/rumd/PairPotential.h:1198-1244
 //   * shift constants p10/p11           src/PairPotential.cu:82-125
 //   * calculateDistance / wrap          include/rumd/SimulationBox.h:111-155
@@ -66,6 +68,21 @@ static float ipl_12_6_f32(float dist2, const float* p, float* u_acc) {
   return s;
 }
 
+// PairPotential::CopyParamsToGPU for one (i,j) row (src/PairPotential.cu:82-125):
+// p11 = u(rc), p10 = s(rc) rc from the float pair function, then the row is
+// stored at (i,j) and mirrored to (j,i) (assume_Newton3 defaults to true,
+// src/PairPotential.cu:55).
+static void store_row(int ntypes, float* params, int i, int j, float* row,
+                      float (*pair)(float, const float*, float*)) {
+  float u = 0.f, s = 0.f;
+  float Rcut = row[0];
+  if (Rcut > 0.0f) s = pair(Rcut * Rcut, row, &u);
+  row[NP - 1] = u;
+  row[NP - 2] = s * Rcut;
+  std::memcpy(&params[(i * ntypes + j) * NP], row, NP * sizeof(float));
+  if (i != j) std::memcpy(&params[(j * ntypes + i) * NP], row, NP * sizeof(float));
+}
+
 // Pot_LJ_12_6::SetParams + PairPotential::CopyParamsToGPU for one (i,j) pair,
 // mirrored to (j,i) (assume_Newton3 defaults to true, src/PairPotential.cu:55).
 ORC_API void orc_lj_set_params(int ntypes, float* params, int i, int j,
@@ -75,13 +92,54 @@ ORC_API void orc_lj_set_params(int ntypes, float* params, int i, int j,
   row[0] = rcut * sigma;
   row[1] = (float)(4. * epsilon * std::pow((double)sigma, 12.));
   row[2] = (float)(-4. * epsilon * std::pow((double)sigma, 6.));
-  float u = 0.f, s = 0.f;
-  float Rcut = row[0];
-  if (Rcut > 0.0f) s = ipl_12_6_f32(Rcut * Rcut, row, &u);
-  row[NP - 1] = u;
-  row[NP - 2] = s * Rcut;
-  std::memcpy(&params[(i * ntypes + j) * NP], row, sizeof(row));
-  if (i != j) std::memcpy(&params[(j * ntypes + i) * NP], row, sizeof(row));
+  store_row(ntypes, params, i, j, row, ipl_12_6_f32);
+}
+
+// Pot_LJ_12_6_smooth_2_4::ComputeInteraction, host float arithmetic
+// (include/rumd/PairPotential.h:248-255).
+static float smooth_2_4_f32(float dist2, const float* p, float* u_acc) {
+  float Dist2 = dist2 * p[1];
+  float invDist2 = 1.0f / Dist2;
+  float invDist6 = invDist2 * invDist2 * invDist2;
+  float s = p[2] * p[1] * (invDist2 * invDist6 * (12.f * invDist6 - 6.f) - 2.0f * p[3] - 4.0f * p[4] * Dist2);
+  *u_acc += p[2] * (invDist6 * (invDist6 - 1.0f) + p[3] * Dist2 + p[4] * Dist2 * Dist2);
+  return s;
+}
+
+// Pot_IPL_n::ComputeInteraction, host float arithmetic
+// (include/rumd/PairPotential.h:630-636).
+static float ipl_n_f32(float dist2, const float* p, float* u_acc) {
+  float invDist2 = 1.0f / (dist2 * p[1]);
+  float invDist_n = expf(logf(invDist2) * p[3] * 0.5f);
+  float s = p[1] * p[2] * p[3] * invDist_n * invDist2;
+  *u_acc += p[2] * invDist_n;
+  return s;
+}
+
+// Pot_LJ_12_6_smooth_2_4::SetParams (include/rumd/PairPotential.h:232-246):
+// c2, c4 from Rcut (in units of sigma) in double, stored as float.
+ORC_API void orc_smooth_set_params(int ntypes, float* params, int i, int j,
+                                   float sigma, float epsilon, float rcut) {
+  float row[NP];
+  std::memset(row, 0, sizeof(row));
+  row[0] = rcut * sigma;
+  row[1] = 1.0f / (sigma * sigma);
+  row[2] = 4.0f * epsilon;
+  row[3] = (float)(48. * std::pow((double)rcut, -14.0) - 15. * std::pow((double)rcut, -8.));
+  row[4] = (float)(6. * std::pow((double)rcut, -10.0) - 21. * std::pow((double)rcut, -16.));
+  store_row(ntypes, params, i, j, row, smooth_2_4_f32);
+}
+
+// Pot_IPL_n::SetParams (include/rumd/PairPotential.h:616-628).
+ORC_API void orc_ipl_n_set_params(int ntypes, float* params, int i, int j, float n,
+                                  float sigma, float epsilon, float rcut) {
+  float row[NP];
+  std::memset(row, 0, sizeof(row));
+  row[0] = rcut * sigma;
+  row[1] = 1.f / (sigma * sigma);
+  row[2] = epsilon;
+  row[3] = n;
+  store_row(ntypes, params, i, j, row, ipl_n_f32);
 }
 
 // ---------------------------------------------------------------------------
@@ -254,13 +312,40 @@ ORC_API unsigned orc_max_nbrs_estimate(unsigned n, float max_cut, float skin, do
 // Pair forces
 // ---------------------------------------------------------------------------
 
+enum { ORC_POT_LJ_12_6 = 0, ORC_POT_LJ_12_6_SMOOTH_2_4 = 1, ORC_POT_IPL_N = 2 };
+
+// The pair functions in double at squared distance d2 for a parameter row of
+// the reference layout: F = s d, energy u.
+//   LJ 12-6          Pot_IPL_12_6::ComputeInteraction  PairPotential.h:161-168
+//   LJ 12-6 smooth   Pot_LJ_12_6_smooth_2_4             PairPotential.h:248-255
+//   IPL n            Pot_IPL_n                          PairPotential.h:630-636
+static void pair_f64(int kind, double d2, const float* p, double* s, double* u) {
+  if (kind == ORC_POT_LJ_12_6) {
+    double i2 = 1. / d2, i6 = i2 * i2 * i2, a12 = p[1], a6 = p[2];
+    *s = i6 * i2 * (12. * a12 * i6 + 6. * a6);
+    *u = i6 * (a12 * i6 + a6);
+  } else if (kind == ORC_POT_LJ_12_6_SMOOTH_2_4) {
+    double is2 = p[1], a = p[2], c2 = p[3], c4 = p[4];
+    double D2 = d2 * is2, i2 = 1. / D2, i6 = i2 * i2 * i2;
+    *s = a * is2 * (i2 * i6 * (12. * i6 - 6.) - 2. * c2 - 4. * c4 * D2);
+    *u = a * (i6 * (i6 - 1.) + c2 * D2 + c4 * D2 * D2);
+  } else {
+    double is2 = p[1], eps = p[2], nn = p[3];
+    double i2 = 1. / (d2 * is2), tn = std::pow(i2, 0.5 * nn);
+    *s = is2 * eps * nn * tn * i2;
+    *u = eps * tn;
+  }
+}
+
 // FP64 pair sum over all j within Rcut (minimum image), every pair visited
 // from both sides as the reference's full list does.  u is halved per
 // particle (Calcf: f.w *= 0.5), w = sum d^2 s (w.w), forces F_i = sum s*d.
 // Uses a cell list with cells >= max cutoff, or all pairs for small boxes.
-ORC_API void orc_forces_f64(int n, const double* pos3, const int* type, const double* L,
-                            int ntypes, const float* params, int cutoff,
-                            double* f3, double* u, double* w) {
+// The cut-off terms (fij, PairPotential.h:1208-1221) use s(rc), u(rc) of the
+// same pair function in double.
+ORC_API void orc_forces_f64_pot(int n, const double* pos3, const int* type, const double* L,
+                                int ntypes, const float* params, int cutoff, int potential,
+                                double* f3, double* u, double* w) {
   double invL[3] = {1. / L[0], 1. / L[1], 1. / L[2]};
   double maxc = 0;
   for (int k = 0; k < ntypes * ntypes; ++k) maxc = std::max(maxc, (double)params[k * NP]);
@@ -304,14 +389,11 @@ ORC_API void orc_forces_f64(int n, const double* pos3, const int* type, const do
       const float* p = &params[(type[i] * ntypes + type[j]) * NP];
       double rc = p[0];
       if (d2 < rc * rc) {
-        double i2 = 1. / d2, i6 = i2 * i2 * i2;
-        double a12 = p[1], a6 = p[2];
-        double s = i6 * i2 * (12. * a12 * i6 + 6. * a6);
-        double uu = i6 * (a12 * i6 + a6);
+        double s, uu;
+        pair_f64(potential, d2, p, &s, &uu);
         if (cutoff != ORC_NS) {
-          double ic2 = 1. / (rc * rc), ic6 = ic2 * ic2 * ic2;
-          double uc = ic6 * (a12 * ic6 + a6);
-          double sc = ic6 * ic2 * (12. * a12 * ic6 + 6. * a6);
+          double sc, uc;
+          pair_f64(potential, rc * rc, p, &sc, &uc);
           if (cutoff == ORC_SP) {
             uu -= uc;
           } else {
@@ -339,6 +421,12 @@ ORC_API void orc_forces_f64(int n, const double* pos3, const int* type, const do
     f3[3 * i] = fx; f3[3 * i + 1] = fy; f3[3 * i + 2] = fz;
     u[i] = 0.5 * ui; w[i] = wi;
   }
+}
+
+ORC_API void orc_forces_f64(int n, const double* pos3, const int* type, const double* L,
+                            int ntypes, const float* params, int cutoff,
+                            double* f3, double* u, double* w) {
+  orc_forces_f64_pot(n, pos3, type, L, ntypes, params, cutoff, ORC_POT_LJ_12_6, f3, u, w);
 }
 
 // FP32 reference-arithmetic force sum over a row-major list (fij + Calcf with

@@ -48,6 +48,9 @@ def lib():
         L.orc_max_nbrs_estimate.argtypes = [u, f, f, d]
         L.orc_max_nbrs_estimate.restype = u
         L.orc_forces_f64.argtypes = [i, P, P, P, i, P, i, P, P, P]
+        L.orc_forces_f64_pot.argtypes = [i, P, P, P, i, P, i, i, P, P, P]
+        L.orc_smooth_set_params.argtypes = [i, P, i, i, f, f, f]
+        L.orc_ipl_n_set_params.argtypes = [i, P, i, i, f, f, f, f]
         L.orc_forces_f32.argtypes = [i, P, P, i, P, i, P, P, i, P, P]
         run_args = [i, P, P, P, P, i, P, i, f, f, d, d, P, i, i, i, i, P, P]
         L.orc_md_run_f32.argtypes = run_args
@@ -73,6 +76,24 @@ def lj_params(ntypes, table):
     params = np.zeros(ntypes * ntypes * NUM_PARAM, np.float32)
     for (i, j), (sig, eps, rc) in table.items():
         lib().orc_lj_set_params(ntypes, _p(params), i, j, sig, eps, rc)
+    return params
+
+
+def smooth_params(ntypes, table):
+    """Pot_LJ_12_6_smooth_2_4 table from {(i, j): (sigma, epsilon, rcut_in_sigma)}
+    (PairPotential.h:232-246 + CopyParamsToGPU)."""
+    params = np.zeros(ntypes * ntypes * NUM_PARAM, np.float32)
+    for (i, j), (sig, eps, rc) in table.items():
+        lib().orc_smooth_set_params(ntypes, _p(params), i, j, sig, eps, rc)
+    return params
+
+
+def ipl_n_params(ntypes, n, table):
+    """Pot_IPL_n table with exponent n from {(i, j): (sigma, epsilon, rcut_in_sigma)}
+    (PairPotential.h:616-628 + CopyParamsToGPU)."""
+    params = np.zeros(ntypes * ntypes * NUM_PARAM, np.float32)
+    for (i, j), (sig, eps, rc) in table.items():
+        lib().orc_ipl_n_set_params(ntypes, _p(params), i, j, n, sig, eps, rc)
     return params
 
 
@@ -144,14 +165,17 @@ def max_nbrs_estimate(n, max_cut, skin, volume):
     return int(lib().orc_max_nbrs_estimate(n, max_cut, skin, volume))
 
 
-def forces_f64(pos3, types, L, ntypes, params, cutoff):
+POTENTIAL = {"LJ_12_6": 0, "LJ_12_6_smooth_2_4": 1, "IPL_n": 2}
+
+
+def forces_f64(pos3, types, L, ntypes, params, cutoff, potential="LJ_12_6"):
     """FP64 pair sum; returns (f[n,3], u[n], w[n]) with u halved, w = sum d^2 s."""
     pos3 = np.ascontiguousarray(pos3, np.float64)
     types = np.ascontiguousarray(types, np.int32)
     n = len(pos3)
     f = np.zeros((n, 3)); u = np.zeros(n); w = np.zeros(n)
-    lib().orc_forces_f64(n, _p(pos3), _p(types), _p(np.asarray(L, np.float64)), ntypes,
-                         _p(params), cutoff, _p(f), _p(u), _p(w))
+    lib().orc_forces_f64_pot(n, _p(pos3), _p(types), _p(np.asarray(L, np.float64)), ntypes,
+                             _p(params), cutoff, POTENTIAL[potential], _p(f), _p(u), _p(w))
     return f, u, w
 
 

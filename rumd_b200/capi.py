@@ -16,6 +16,8 @@ LIB_PATH = os.path.join(_HERE, "librumd_b200.so")
 
 B2MD_OK, B2MD_ERR_ARG, B2MD_ERR_CUDA, B2MD_ERR_NOMEM, B2MD_ERR_STATE, B2MD_ERR_OVERFLOW = range(6)
 CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
+# pair functions (which RUMD Pot_* class the parameter rows belong to)
+POTENTIAL = {"LJ_12_6": 0, "LJ_12_6_smooth_2_4": 1, "IPL_n": 2}
 # kernel variants (b2md_engine_set_variant)
 VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP, VARIANT_SM_TILES = 0, 1, 2, 3, 4
 VARIANT_WINDOW_LIST_ROWS = 5
@@ -49,7 +51,7 @@ class ReplicaDesc(ctypes.Structure):
         ("tau", ctypes.c_double), ("dT_per_step", ctypes.c_double), ("xi", ctypes.c_double),
         ("thermostat_mask", ctypes.c_uint), ("reset_interval", ctypes.c_int),
         ("max_nbrs", ctypes.c_int), ("energy_interval", ctypes.c_int),
-        ("energy_capacity", ctypes.c_int),
+        ("energy_capacity", ctypes.c_int), ("potential", ctypes.c_int),
     ]
 
 
@@ -77,7 +79,7 @@ def lib():
             "b2md_replica_remove": [P, i],
             "b2md_replica_get": [P, i, i, P],
             "b2md_replica_set": [P, i, i, P],
-            "b2md_replica_set_potential": [P, i, i, P, i, f],
+            "b2md_replica_set_potential": [P, i, i, P, i, f, i],
             "b2md_replica_set_integrator": [P, i, f, d, d, d, u],
             "b2md_replica_set_xi": [P, i, d],
             "b2md_replica_set_reset_interval": [P, i, i],
@@ -206,7 +208,7 @@ class Engine:
 
     def add(self, pos4, box, params, ntypes, cutoff="SF", skin=0.3, dt=0.005, T=1.0, tau=0.2,
             vel4=None, im3=None, thermostat=True, xi=0.0, reset_interval=100, max_nbrs=0,
-            dT_per_step=0.0, energy_interval=0, energy_capacity=0, thermostat_mask=None):
+            dT_per_step=0.0, energy_interval=0, energy_capacity=0, thermostat_mask=None, potential="LJ_12_6"):
         pos4 = np.ascontiguousarray(pos4, np.float32)
         n = len(pos4)
         params = np.ascontiguousarray(params, np.float32)
@@ -224,6 +226,7 @@ class Engine:
         d.reset_interval = reset_interval
         d.max_nbrs = max_nbrs
         d.energy_interval, d.energy_capacity = energy_interval, energy_capacity
+        d.potential = POTENTIAL[potential] if isinstance(potential, str) else int(potential)
         v = None if vel4 is None else np.ascontiguousarray(vel4, np.float32)
         im = None if im3 is None else np.ascontiguousarray(im3, np.int32)
         rid = ctypes.c_int()
@@ -246,10 +249,11 @@ class Engine:
         arr = np.ascontiguousarray(arr, dt)
         check(lib().b2md_replica_set(self._h, rid, FIELD[field], _ptr(arr)))
 
-    def set_potential(self, rid, ntypes, params, cutoff, skin):
+    def set_potential(self, rid, ntypes, params, cutoff, skin, potential="LJ_12_6"):
         params = np.ascontiguousarray(params, np.float32)
         c = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
-        check(lib().b2md_replica_set_potential(self._h, rid, ntypes, _ptr(params), c, skin))
+        pk = POTENTIAL[potential] if isinstance(potential, str) else int(potential)
+        check(lib().b2md_replica_set_potential(self._h, rid, ntypes, _ptr(params), c, skin, pk))
 
     def set_integrator(self, rid, dt, T, tau, dT_per_step=0.0, thermostat_mask=0xFFFFFFFF):
         check(lib().b2md_replica_set_integrator(self._h, rid, dt, T, tau, dT_per_step, thermostat_mask))

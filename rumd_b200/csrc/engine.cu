@@ -411,10 +411,17 @@ void write_field(b2md_engine* e, int id, size_t off, const T& val) {
 
 // Packs a RUMD parameter table into the engine's per-pair rows and derives
 // the cell grid (NeighborList.cu:717-732).
-void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, float skin) {
+void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, float skin, int potential) {
   if (ntypes < 1 || ntypes > kMaxTypes) api_fail(B2MD_ERR_ARG, "ntypes must be 1..8");
   if (cutoff < 0 || cutoff > 2) api_fail(B2MD_ERR_ARG, "cutoff method must be NS, SP or SF");
+  if (potential < POT_LJ_12_6 || potential > POT_IPL_N)
+    api_fail(B2MD_ERR_ARG, "pair function must be LJ 12-6, LJ 12-6 smooth 2-4 or IPL n");
+  if (potential != POT_LJ_12_6)
+    for (int k = 0; k < ntypes * ntypes; ++k)
+      if (params[k * kNumParam] > 0.f && !(params[k * kNumParam + 1] > 0.f))
+        api_fail(B2MD_ERR_ARG, "pair parameter 1 (1/sigma^2) must be positive");
   if (!(skin >= 0.f)) api_fail(B2MD_ERR_ARG, "skin must be >= 0");
+  h.d.potential = potential;
   h.params.assign(params, params + ntypes * ntypes * kNumParam);
   h.d.ntypes = ntypes;
   h.d.cutoff = cutoff;
@@ -444,17 +451,39 @@ std::vector<float> pack_params(const HostRep& h) {
     float* q = &out[k * kParStride];
     float rc = p[0];
     const float sc = p[kNumParam - 2], uc = p[kNumParam - 1];  // s(rc)*rc, u(rc)
-    q[0] = rc * rc;
-    q[1] = p[1];
-    q[2] = p[2];
-    // fij's cut-off terms (PairPotential.h:1208-1221) as s -= c_s/r, u += c_ur r + c_u0
+    // fij's cut-off terms (PairPotential.h:1208-1221) as s -= c_s/r, u += c_s r + c_u0
     const bool sf = h.d.cutoff == CUT_SF, sp = h.d.cutoff == CUT_SP;
-    q[3] = sf ? sc : 0.f;
-    q[4] = sf ? -(sc * rc + uc) : (sp ? -uc : 0.f);
-    q[5] = sf ? sc : 0.f;
+    const float c_s = sf ? sc : 0.f;
+    const float c_u0 = sf ? -(sc * rc + uc) : (sp ? -uc : 0.f);
     float cs = rc + h.skin;  // calculateNBL_*: (params + skin)^2 in float
+    q[0] = rc * rc;
     q[6] = cs * cs;
-    q[7] = 0.f;
+    if (h.d.potential == POT_LJ_12_6) {
+      q[1] = p[1];
+      q[2] = p[2];
+      q[3] = c_s;
+      q[4] = c_u0;
+      q[5] = c_s;
+    } else if (h.d.potential == POT_LJ_12_6_SMOOTH_2_4) {
+      // u = 4eps [(s/r)^12 - (s/r)^6 + c2 (r/s)^2 + c4 (r/s)^4]: the r^2 and
+      // r^4 terms folded into b, c (force) and e, g (energy) per unit of d^2
+      const float is2 = p[1], a = p[2], c2 = p[3], c4 = p[4];
+      q[1] = rc > 0.f ? 1.f / is2 : 0.f;
+      q[2] = a;
+      q[3] = -2.f * c2 * a * is2;
+      q[4] = -4.f * c4 * a * is2 * is2;
+      q[5] = c2 * a * is2;
+      q[7] = c4 * a * is2 * is2;
+      q[8] = c_s;
+      q[9] = c_u0;
+    } else {  // POT_IPL_N: u = eps (sigma/r)^n
+      q[1] = rc > 0.f ? 1.f / p[1] : 0.f;
+      q[2] = p[2];
+      q[3] = 0.5f * p[3];
+      q[4] = p[3] * p[2];
+      q[8] = c_s;
+      q[9] = c_u0;
+    }
   }
   return out;
 }
@@ -991,7 +1020,7 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
       h.d.L[k] = d->box[k];
       h.d.invL[k] = 1.f / d->box[k];
     }
-    set_potential(h, d->ntypes, d->params, d->cutoff_method, d->skin);
+    set_potential(h, d->ntypes, d->params, d->cutoff_method, d->skin, d->potential);
     // types must be in range
     for (int i = 0; i < d->n; ++i) {
       int t;
@@ -1163,14 +1192,14 @@ int b2md_replica_set(b2md_engine* e, int id, int field, const void* in) {
 }
 
 int b2md_replica_set_potential(b2md_engine* e, int id, int ntypes, const float* params, int cutoff_method,
-                               float skin) {
+                               float skin, int potential) {
   if (!params) return fail(B2MD_ERR_ARG, "params is null");
   return guarded([&] {
     HostRep& h = get_rep(e, id);
     CK(cudaSetDevice(e->device));
     CK(cudaStreamSynchronize(e->stream));
     if (ntypes != h.d.ntypes) api_fail(B2MD_ERR_ARG, "number of types cannot change");
-    set_potential(h, ntypes, params, cutoff_method, skin);
+    set_potential(h, ntypes, params, cutoff_method, skin, potential);
     place_cells(e, h);
     place_params(e, h);
     int want = estimate_max_nbrs(h);
@@ -1225,7 +1254,7 @@ int b2md_replica_set_nb_method(b2md_engine* e, int id, int method) {
     CK(cudaStreamSynchronize(e->stream));
     h.nb_method_req = method;
     std::vector<float> params = h.params;
-    set_potential(h, h.d.ntypes, params.data(), h.d.cutoff, h.skin);
+    set_potential(h, h.d.ntypes, params.data(), h.d.cutoff, h.skin, h.d.potential);
     upload_rep(e, id);
     WRITE_STATE(e, id, rebuild, 1);
     invalidate_graphs(e);

@@ -32,7 +32,7 @@
 namespace b2md {
 
 constexpr int kMaxTypes = 8;
-constexpr int kParStride = 8;   // packed floats per type pair
+constexpr int kParStride = 12;  // packed floats per type pair
 constexpr int kNumParam = 12;   // RUMD NumParam (rumd_base.h)
 constexpr int kNPart = 8;       // FP64 partial sums per tile
 constexpr int kGroup = 32;      // tiles per reduction group
@@ -50,9 +50,18 @@ __host__ __device__ __forceinline__ int list_rows(int max_nbrs) { return (max_nb
 enum { P_PE = 0, P_W, P_KE2, P_KET, P_PX, P_PY, P_PZ, P_M };
 enum { CUT_NS = 0, CUT_SP = 1, CUT_SF = 2 };
 enum { NB_CELLS = 0, NB_N2 = 1 };
+// pair functions (the RUMD classes whose rows the parameter table holds)
+enum { POT_LJ_12_6 = 0, POT_LJ_12_6_SMOOTH_2_4 = 1, POT_IPL_N = 2 };
 
-// Packed pair row (8 floats): rc^2, A12, A6, c_s, c_u0, c_ur, (rc+skin)^2, 0.
-// The cut-off method is folded into c_s, c_u0, c_ur (see lj_pair).
+// Packed pair row (kParStride floats; slot 6 is (rc+skin)^2 for every pair
+// function, read by the list build).  The cut-off method is folded into c_s,
+// c_u0 (and c_ur):
+//   LJ 12-6:          rc^2, A12, A6, c_s, c_u0, c_ur, (rc+skin)^2, 0, ...
+//   LJ 12-6 smooth:   rc^2, sigma^2, 4 eps, b, c, e, (rc+skin)^2, g, c_s, c_u0
+//                     (b = -2 c2 4eps/sigma^2, c = -4 c4 4eps/sigma^4,
+//                      e = c2 4eps/sigma^2, g = c4 4eps/sigma^4)
+//   IPL n:            rc^2, sigma^2, eps, n/2, n eps, 0, (rc+skin)^2, 0, c_s, c_u0
+// (see lj_pair).
 struct RepDev {
   int n, p0, tile0, ntiles;
   int group0, ngroups;
@@ -73,7 +82,7 @@ struct RepDev {
   long long elog0;
   double dof;
   int active;
-  int pad_;
+  int potential;  // POT_*
 };
 
 struct RepState {

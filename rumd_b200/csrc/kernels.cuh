@@ -255,15 +255,20 @@ struct PairAcc {
   float sxx = 0.f, syy = 0.f, szz = 0.f, syz = 0.f, sxz = 0.f, sxy = 0.f;
 };
 
-// fij + Pot_IPL_12_6::ComputeInteraction (PairPotential.h:161-168, 1198-1244)
-// for one neighbour, without branches so that consecutive pairs interleave.
+// fij (PairPotential.h:1198-1244) for one neighbour, without branches so
+// that consecutive pairs interleave, for the pair function POT:
+//   POT_LJ_12_6            Pot_IPL_12_6 / Pot_LJ_12_6::ComputeInteraction
+//                          (PairPotential.h:161-168)
+//   POT_LJ_12_6_SMOOTH_2_4 Pot_LJ_12_6_smooth_2_4::ComputeInteraction
+//                          (PairPotential.h:248-255)
+//   POT_IPL_N              Pot_IPL_n::ComputeInteraction (PairPotential.h:630-636)
 // 1/r comes from one MUFU rsqrt refined by one Newton-Raphson step
 // (y <- y (3/2 - x y^2 / 2)); 1/r^2 = y^2.  The cut-off method is folded into
-// the packed pair row: s -= c_s / r and u += c_ur r + c_u0, which is
+// the packed pair row: s -= c_s / r and u += c_s r + c_u0, which is
 // s(rc) rc / r and s(rc) rc (r - rc) - u(rc) for SF, -u(rc) for SP, 0 for NS.
 // WRAP = false skips the minimum-image step; the caller uses it only when it
 // is exactly the identity (see k_force).
-template <bool STRESS, bool WRAP>
+template <bool STRESS, bool WRAP, int POT = POT_LJ_12_6>
 __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const float4& rj, const float* prow, float Lx,
                                         float Ly, float Lz, float iLx, float iLy, float iLz) {
   float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
@@ -274,16 +279,37 @@ __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const floa
   }
   const float d2 = dist2_ref(dx, dy, dz);
   const float* pp = prow + __float_as_int(rj.w) * kParStride;
-  const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, A12, A6, c_s
-  const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);  // c_u0, c_ur
   float y = rsqrt_approx(d2);
   y = y * __fmaf_rn(-0.5f * d2 * y, y, 1.5f);
   const float i2 = y * y;
-  const float i6 = i2 * i2 * i2;
-  const float t = q.y * i6;
-  float s = __fmaf_rn(-q.w, y, i6 * i2 * __fmaf_rn(12.f, t, 6.f * q.z));
-  float u = __fmaf_rn(i6, t + q.z, __fmaf_rn(q2.y, d2 * y, q2.x));
-  const bool in = d2 < q.x;
+  float s, u;
+  bool in;
+  if (POT == POT_LJ_12_6) {
+    const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, A12, A6, c_s
+    const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);  // c_u0, c_ur
+    const float i6 = i2 * i2 * i2;
+    const float t = q.y * i6;
+    s = __fmaf_rn(-q.w, y, i6 * i2 * __fmaf_rn(12.f, t, 6.f * q.z));
+    u = __fmaf_rn(i6, t + q.z, __fmaf_rn(q2.y, d2 * y, q2.x));
+    in = d2 < q.x;
+  } else if (POT == POT_LJ_12_6_SMOOTH_2_4) {
+    const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, sigma^2, 4 eps, b
+    const float4 q1 = *reinterpret_cast<const float4*>(pp + 4);  // c, e, -, g
+    const float2 q2 = *reinterpret_cast<const float2*>(pp + 8);  // c_s, c_u0
+    const float t2 = q.y * i2;  // (sigma / r)^2
+    const float t6 = t2 * t2 * t2;
+    s = __fmaf_rn(-q2.x, y, __fmaf_rn(q1.x, d2, __fmaf_rn(q.z * i2 * t6, __fmaf_rn(12.f, t6, -6.f), q.w)));
+    u = __fmaf_rn(q.z * t6, t6 - 1.f, __fmaf_rn(d2, __fmaf_rn(q1.w, d2, q1.y), __fmaf_rn(q2.x, d2 * y, q2.y)));
+    in = d2 < q.x;
+  } else {
+    const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, sigma^2, eps, n/2
+    const float ne = pp[4];                                       // n eps
+    const float2 q2 = *reinterpret_cast<const float2*>(pp + 8);  // c_s, c_u0
+    const float tn = expf(logf(q.y * i2) * q.w);                 // (sigma / r)^n
+    s = __fmaf_rn(-q2.x, y, ne * tn * i2);
+    u = __fmaf_rn(q.z, tn, __fmaf_rn(q2.x, d2 * y, q2.y));
+    in = d2 < q.x;
+  }
   s = in ? s : 0.f;
   u = in ? u : 0.f;
   A.fx = __fmaf_rn(dx, s, A.fx);
@@ -453,7 +479,7 @@ struct PosWindow {
 // The neighbour loop of one thread: its entries (lane_entry) in groups of
 // four -- one vector load of list entries, four neighbour positions in
 // flight -- then the remaining ones singly.  Only entries below nn are read.
-template <int TP, bool STRESS, bool WRAP, class Idx, class Pos>
+template <int TP, bool STRESS, bool WRAP, int POT, class Idx, class Pos>
 __device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos& pos, unsigned lane_t, unsigned nn,
                                            const float4& ri, const float* prow, float Lx, float Ly, float Lz,
                                            float iLx, float iLy, float iLz) {
@@ -462,25 +488,34 @@ __device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos
   for (; q + 4 <= cnt; q += 4) {
     const uint4 j = idx.template group<TP>(q, lane_t);
     const float4 r0 = pos(j.x), r1 = pos(j.y), r2 = pos(j.z), r3 = pos(j.w);
-    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-    lj_pair<STRESS, WRAP>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP, POT>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP, POT>(A, ri, r1, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP, POT>(A, ri, r2, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP, POT>(A, ri, r3, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
   for (; q < cnt; ++q) {
     const float4 r0 = pos(idx.one(lane_entry<TP>(q, lane_t)));
-    lj_pair<STRESS, WRAP>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+    lj_pair<STRESS, WRAP, POT>(A, ri, r0, prow, Lx, Ly, Lz, iLx, iLy, iLz);
   }
 }
 
+// The loop for the replica's pair function (block-uniform) and minimum-image need.
 template <int TP, bool STRESS, class Idx, class Pos>
-__device__ __forceinline__ void force_loop_any(bool fast, PairAcc& A, const Idx& idx, const Pos& pos,
+__device__ __forceinline__ void force_loop_any(bool fast, int pot, PairAcc& A, const Idx& idx, const Pos& pos,
                                                unsigned lane_t, unsigned nn, const float4& ri, const float* prow,
                                                float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
-  if (fast)
-    force_loop<TP, STRESS, false>(A, idx, pos, lane_t, nn, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
-  else
-    force_loop<TP, STRESS, true>(A, idx, pos, lane_t, nn, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
+#define FL(W, P) force_loop<TP, STRESS, W, P>(A, idx, pos, lane_t, nn, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz)
+  if (pot == POT_LJ_12_6) {
+    if (fast) FL(false, POT_LJ_12_6);
+    else FL(true, POT_LJ_12_6);
+  } else if (pot == POT_LJ_12_6_SMOOTH_2_4) {
+    if (fast) FL(false, POT_LJ_12_6_SMOOTH_2_4);
+    else FL(true, POT_LJ_12_6_SMOOTH_2_4);
+  } else {
+    if (fast) FL(false, POT_IPL_N);
+    else FL(true, POT_IPL_N);
+  }
+#undef FL
 }
 
 // Shared memory of k_force: [packed pair table, kParSmemFloats]
@@ -623,13 +658,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
       if (ok) {
         if (MODE == FM_STAGED)
-          force_loop_any<TP, STRESS>(fast, A, IdxStaged{s_idx + lp * 8, pitch * 8}, PosGlobal{rc}, lane_t, nn, ri, prow,
+          force_loop_any<TP, STRESS>(fast, R.potential, A, IdxStaged{s_idx + lp * 8, pitch * 8}, PosGlobal{rc}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
         else if (wl_staged)
-          force_loop_any<TP, STRESS>(fast, A, IdxWindowStaged{s_wl + lp * 8, pitch * 8}, PosWindow{s_win}, lane_t, nn,
+          force_loop_any<TP, STRESS>(fast, R.potential, A, IdxWindowStaged{s_wl + lp * 8, pitch * 8}, PosWindow{s_win}, lane_t, nn,
                                      ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
         else
-          force_loop_any<TP, STRESS>(fast, A, IdxWindow{wbase, (unsigned)i, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
+          force_loop_any<TP, STRESS>(fast, R.potential, A, IdxWindow{wbase, (unsigned)i, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
       } else {
         // the copies did not land in time: record it for the host and wait
@@ -639,7 +674,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     } else {
       __syncthreads();  // the pair table
-      force_loop_any<TP, STRESS>(fast, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
+      force_loop_any<TP, STRESS>(fast, R.potential, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
                                  Lz, iLx, iLy, iLz);
     }
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;

@@ -88,6 +88,15 @@ PYBIND11_MODULE(_rumd, m) {
       .def(py::init<PairPotential::CutoffMethod>(), py::arg("cutoff_method"))
       .def("SetParams", &Pot_LJ_12_6::SetParams, py::arg("i"), py::arg("j"), py::arg("Sigma"), py::arg("Epsilon"),
            py::arg("Rcut"));
+  py::class_<Pot_LJ_12_6_smooth_2_4, PairPotential>(m, "Pot_LJ_12_6_smooth_2_4")
+      .def(py::init<PairPotential::CutoffMethod>(), py::arg("cutoff_method"))
+      .def("SetParams", &Pot_LJ_12_6_smooth_2_4::SetParams, py::arg("i"), py::arg("j"), py::arg("Sigma"),
+           py::arg("Epsilon"), py::arg("Rcut"));
+  py::class_<Pot_IPL_n, PairPotential>(m, "Pot_IPL_n")
+      .def(py::init<float, PairPotential::CutoffMethod>(), py::arg("n"), py::arg("cutoff_method"))
+      .def("SetParams", &Pot_IPL_n::SetParams, py::arg("i"), py::arg("j"), py::arg("Sigma"), py::arg("Epsilon"),
+           py::arg("Rcut"))
+      .def("GetExponent", &Pot_IPL_n::GetExponent);
 
   py::class_<Integrator>(m, "Integrator")
       .def("Integrate", &Integrator::Integrate)

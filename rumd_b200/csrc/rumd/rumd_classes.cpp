@@ -87,6 +87,52 @@ void Pot_LJ_12_6::SetParams(unsigned i, unsigned j, float Sigma, float Epsilon, 
                           (float)(-4. * Epsilon * std::pow((double)Sigma, 6.)), Rcut * Sigma);
 }
 
+void Pot_LJ_12_6_smooth_2_4::SetParams(unsigned i, unsigned j, float Sigma, float Epsilon, float Rcut) {
+  // Pot_LJ_12_6_smooth_2_4::SetParams (PairPotential.h:232-246): c2, c4 in
+  // double from Rcut in units of sigma, stored as float
+  const float c2 = (float)(48. * std::pow((double)Rcut, -14.0) - 15. * std::pow((double)Rcut, -8.));
+  const float c4 = (float)(6. * std::pow((double)Rcut, -10.0) - 21. * std::pow((double)Rcut, -16.));
+  StoreParams(i, j, {Rcut * Sigma, 1.0f / (Sigma * Sigma), 4.0f * Epsilon, c2, c4});
+}
+
+float Pot_LJ_12_6_smooth_2_4::ComputeInteraction_CPU(float dist2, const float* param, float* u) const {
+  // Pot_LJ_12_6_smooth_2_4::ComputeInteraction on the host, float arithmetic
+  // (PairPotential.h:248-255), used for the shift constants
+  volatile float Dist2 = dist2 * param[1];
+  volatile float invDist2 = 1.0f / Dist2;
+  volatile float invDist6 = invDist2 * invDist2 * invDist2;
+  volatile float a = invDist2 * invDist6;
+  volatile float b = 12.f * invDist6 - 6.f;
+  volatile float c = 2.0f * param[3];
+  volatile float d = 4.0f * param[4] * Dist2;
+  volatile float s = param[2] * param[1] * (a * b - c - d);
+  volatile float e = invDist6 * (invDist6 - 1.0f);
+  volatile float g = param[3] * Dist2;
+  volatile float h = param[4] * Dist2 * Dist2;
+  *u += param[2] * (e + g + h);
+  return s;
+}
+
+Pot_IPL_n::Pot_IPL_n(float n_, CutoffMethod m) : PairPotential(m), n(n_) {
+  std::ostringstream ss;
+  ss << "potIPL_" << n_;
+  SetID_String(ss.str());
+}
+
+void Pot_IPL_n::SetParams(unsigned i, unsigned j, float Sigma, float Epsilon, float Rcut) {
+  // Pot_IPL_n::SetParams (PairPotential.h:616-628)
+  StoreParams(i, j, {Rcut * Sigma, 1.f / (Sigma * Sigma), Epsilon, n});
+}
+
+float Pot_IPL_n::ComputeInteraction_CPU(float dist2, const float* param, float* u) const {
+  // Pot_IPL_n::ComputeInteraction on the host (PairPotential.h:630-636)
+  volatile float invDist2 = 1.0f / (dist2 * param[1]);
+  volatile float invDist_n = std::exp(std::log(invDist2) * param[3] * 0.5f);
+  volatile float s = param[1] * param[2] * param[3] * invDist_n * invDist2;
+  *u += param[2] * invDist_n;
+  return s;
+}
+
 float PairPotential::GetPotentialParameter(unsigned t1, unsigned t2, unsigned k) const {
   auto it = params_map.find({t1, t2});
   if (it == params_map.end() || k >= it->second.size()) return 0.f;
@@ -408,6 +454,7 @@ void Sample::EnsureReplica() {
   d.thermostat_mask = nvt ? nvt->GetThermostatMask() : 0u;
   d.reset_interval = 0;
   d.max_nbrs = (int)pot->GetNeighborList().GetMaxNumNbrs();
+  d.potential = pot->PotentialKind();
   Check(b2md_replica_add(eng, &d, pos.data(), vel.data(), im.data(), &rid), "SetNumberOfParticles");
   int m = pot->GetNeighborList().MethodCode();
   if (m != -1) Check(b2md_replica_set_nb_method(eng, rid, m), "SetNB_Method");
@@ -433,7 +480,7 @@ void Sample::PotentialChanged() {
   if (!HasReplica() || !pot) return;
   std::vector<float> table = pot->ParamTable(GetNumberOfTypes());
   Check(b2md_replica_set_potential(eng, rid, (int)GetNumberOfTypes(), table.data(), pot->GetCutoffMethod(),
-                                   pot->GetNbListSkin()),
+                                   pot->GetNbListSkin(), pot->PotentialKind()),
         "SetPotential");
 }
 

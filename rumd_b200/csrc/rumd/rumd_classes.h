@@ -97,6 +97,8 @@ class PairPotential : public Potential {
   int GetCutoffMethod() const { return cutoffMethod; }
   unsigned GetActualMaxNumNbrs() const;
   void SetAssumeNewton3(bool v) { assume_Newton3 = v; }
+  // Which pair function the rows hold (B2MD_POT_*).
+  virtual int PotentialKind() const { return 0; }
   NeighborList& GetNeighborList() { return neighborList; }
   const NeighborList& GetNeighborList() const { return neighborList; }
 
@@ -128,6 +130,33 @@ class Pot_LJ_12_6 : public Pot_IPL_12_6 {
  public:
   explicit Pot_LJ_12_6(CutoffMethod m) : Pot_IPL_12_6(m) { SetID_String("potLJ_12_6"); }
   void SetParams(unsigned i, unsigned j, float Sigma, float Epsilon, float Rcut);
+};
+
+// v(r) = 4 eps ((sigma/r)^12 - (sigma/r)^6 + c2 (r/sigma)^2 + c4 (r/sigma)^4),
+// c2, c4 chosen so that the force and its derivative vanish at Rcut; the
+// constant c0 that would make v(Rcut) = 0 is left to the ShiftedPotential
+// cut-off (Pot_LJ_12_6_smooth_2_4, PairPotential.h:210-256).
+class Pot_LJ_12_6_smooth_2_4 : public PairPotential {
+ public:
+  explicit Pot_LJ_12_6_smooth_2_4(CutoffMethod m) : PairPotential(m) { SetID_String("potLJ_12_6_smooth_2_4"); }
+  void SetParams(unsigned i, unsigned j, float Sigma, float Epsilon, float Rcut);
+  int PotentialKind() const override { return 1; }
+
+ protected:
+  float ComputeInteraction_CPU(float dist2, const float* param, float* u) const override;
+};
+
+// v(r) = eps (sigma/r)^n (Pot_IPL_n, PairPotential.h:603-637).
+class Pot_IPL_n : public PairPotential {
+ public:
+  Pot_IPL_n(float n, CutoffMethod m);
+  void SetParams(unsigned i, unsigned j, float Sigma, float Epsilon, float Rcut);
+  int PotentialKind() const override { return 2; }
+  float GetExponent() const { return n; }
+
+ protected:
+  float ComputeInteraction_CPU(float dist2, const float* param, float* u) const override;
+  float n;
 };
 
 class Integrator {

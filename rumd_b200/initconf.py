@@ -11,8 +11,11 @@ Parameter tables reproduce Pot_LJ_12_6::SetParams (PairPotential.h:202-207)
 followed by PairPotential::CopyParamsToGPU (PairPotential.cu:82-125): A12 and
 A6 are evaluated in double and stored as float, the cut-off is Rcut*sigma in
 float, and the shift constants p10 = s(rc)*rc and p11 = u(rc) are computed
-with the FP32 Pot_IPL_12_6::ComputeInteraction arithmetic.
+with the FP32 Pot_IPL_12_6::ComputeInteraction arithmetic.  The tables of
+Pot_LJ_12_6_smooth_2_4 and Pot_IPL_n follow their SetParams the same way.
 """
+import math
+
 import numpy as np
 
 NUM_PARAM = 12
@@ -45,14 +48,87 @@ def lj_row(sigma, epsilon, rcut):
     return row
 
 
-def lj_params(ntypes, table):
-    """RUMD parameter table float32[ntypes*ntypes*12] from {(i,j): (sigma, eps, rcut/sigma)}."""
+def _shifts(row, pair):
+    """p11 = u(rc), p10 = s(rc)*rc from the float pair function (PairPotential.cu:82-125)."""
+    rc = row[0]
+    if rc > 0:
+        s, u = pair(rc * rc, row)
+        row[NUM_PARAM - 1] = u
+        row[NUM_PARAM - 2] = s * rc
+    return row
+
+
+def _smooth_2_4_f32(dist2, p):
+    # Pot_LJ_12_6_smooth_2_4::ComputeInteraction (PairPotential.h:248-255)
+    f = np.float32
+    d2 = f(dist2) * p[1]
+    i2 = f(1.0) / d2
+    i6 = i2 * i2 * i2
+    s = p[2] * p[1] * (i2 * i6 * (f(12.0) * i6 - f(6.0)) - f(2.0) * p[3] - f(4.0) * p[4] * d2)
+    u = f(0.0) + p[2] * (i6 * (i6 - f(1.0)) + p[3] * d2 + p[4] * d2 * d2)
+    return f(s), f(u)
+
+
+def _ipl_n_f32(dist2, p):
+    # Pot_IPL_n::ComputeInteraction (PairPotential.h:630-636); logf, expf as
+    # correctly rounded float functions
+    f = np.float32
+    i2 = f(1.0) / (f(dist2) * p[1])
+    tn = f(math.exp(float(f(math.log(float(i2))) * p[3] * f(0.5))))
+    s = p[1] * p[2] * p[3] * tn * i2
+    u = f(0.0) + p[2] * tn
+    return f(s), f(u)
+
+
+def smooth_row(sigma, epsilon, rcut):
+    """Pot_LJ_12_6_smooth_2_4::SetParams (PairPotential.h:232-246): c2, c4 in
+    double from rcut in units of sigma, stored as float."""
+    f = np.float32
+    row = np.zeros(NUM_PARAM, np.float32)
+    sigma, epsilon, rcut = f(sigma), f(epsilon), f(rcut)
+    row[0] = rcut * sigma
+    row[1] = f(1.0) / (sigma * sigma)
+    row[2] = f(4.0) * epsilon
+    x = float(rcut)
+    row[3] = f(48.0 * x ** -14.0 - 15.0 * x ** -8.0)
+    row[4] = f(6.0 * x ** -10.0 - 21.0 * x ** -16.0)
+    return _shifts(row, _smooth_2_4_f32)
+
+
+def ipl_n_row(n, sigma, epsilon, rcut):
+    """Pot_IPL_n::SetParams (PairPotential.h:616-628)."""
+    f = np.float32
+    row = np.zeros(NUM_PARAM, np.float32)
+    sigma, epsilon, rcut = f(sigma), f(epsilon), f(rcut)
+    row[0] = rcut * sigma
+    row[1] = f(1.0) / (sigma * sigma)
+    row[2] = epsilon
+    row[3] = f(n)
+    return _shifts(row, _ipl_n_f32)
+
+
+def _table(ntypes, table, row_of):
     p = np.zeros((ntypes, ntypes, NUM_PARAM), np.float32)
-    for (i, j), (sig, eps, rc) in table.items():
-        row = lj_row(sig, eps, rc)
+    for (i, j), args in table.items():
+        row = row_of(*args)
         p[i, j] = row
         p[j, i] = row
     return p.reshape(-1)
+
+
+def lj_params(ntypes, table):
+    """RUMD parameter table float32[ntypes*ntypes*12] from {(i,j): (sigma, eps, rcut/sigma)}."""
+    return _table(ntypes, table, lj_row)
+
+
+def smooth_params(ntypes, table):
+    """Pot_LJ_12_6_smooth_2_4 table from {(i,j): (sigma, eps, rcut/sigma)}."""
+    return _table(ntypes, table, smooth_row)
+
+
+def ipl_n_params(ntypes, n, table):
+    """Pot_IPL_n table with exponent n from {(i,j): (sigma, eps, rcut/sigma)}."""
+    return _table(ntypes, table, lambda sig, eps, rc: ipl_n_row(n, sig, eps, rc))
 
 
 def fcc_positions(n, density):

@@ -1,6 +1,7 @@
 """RUMD's Python surface for the LJ/NVT path: ``import rumd_b200.rumd as rumd``.
 
-The classes (Sample, Pot_LJ_12_6, Pot_IPL_12_6, IntegratorNVT, IntegratorNVE)
+The classes (Sample, Pot_LJ_12_6, Pot_IPL_12_6, Pot_LJ_12_6_smooth_2_4,
+Pot_IPL_n, IntegratorNVT, IntegratorNVE)
 are the C++ classes of ``_rumd`` (pybind11), named as RUMD's SWIG module names
 them (Swig/rumd.i, Potentials.i, Integrators.i); ``NoShift``,
 ``ShiftedPotential`` and ``ShiftedForce`` are the cut-off methods
@@ -30,7 +31,9 @@ from ._rumd import (  # noqa: E402,F401
     NoShift,
     PairPotential,
     Pot_IPL_12_6,
+    Pot_IPL_n,
     Pot_LJ_12_6,
+    Pot_LJ_12_6_smooth_2_4,
     RUMD_cudaResourceError,
     RUMD_Error,
     Sample,
