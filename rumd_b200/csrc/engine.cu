@@ -286,8 +286,12 @@ EngArgs make_args(b2md_engine* e) {
   // staged list tile (force mode 1): pb slots per block of 8 entries
   a.idx_pitch = e->pb;
   a.idx_rows = 0;
+  a.max_types = 1;
   for (auto& h : e->reps)
-    if (h.active) a.idx_rows = std::max(a.idx_rows, h.d.max_nbrs);
+    if (h.active) {
+      a.idx_rows = std::max(a.idx_rows, h.d.max_nbrs);
+      a.max_types = std::max(a.max_types, h.d.ntypes);
+    }
   a.wl = e->wl;
   a.wseg = e->wseg;
   a.wmeta = e->wmeta;
@@ -299,13 +303,20 @@ EngArgs make_args(b2md_engine* e) {
   return a;
 }
 
-// Dynamic shared memory of k_force: pair table [+ staged list tile | position window].
-size_t force_smem(const EngArgs& a, int mode) {
+// Dynamic shared memory of k_force: pair table [+ staged list tile | position
+// window], at least the block reduction's scratch that overlays it at the end.
+// Streamed blocks hold only the rows of the engine's largest type count, which
+// leaves the rest of the SM's unified memory to L1.
+size_t force_smem(const b2md_engine* e, const EngArgs& a) {
+  const int mode = e->force_mode;
   size_t extra = 0;
   if (mode == FM_STAGED) extra = (size_t)list_rows(a.idx_rows) * a.idx_pitch * sizeof(unsigned);
   if (mode == FM_WINDOW)
     extra = (size_t)a.win_cap * sizeof(float4) + (size_t)a.wl_rows * a.idx_pitch * sizeof(unsigned short);
-  return (size_t)kParSmemFloats * sizeof(float) + extra;
+  const size_t table = mode == FM_STREAMED ? (size_t)a.max_types * a.max_types * kParStride * sizeof(float)
+                                           : (size_t)kParSmemFloats * sizeof(float);
+  const size_t need = std::max(table + extra, (size_t)force_red_bytes(e->pb * e->tp));
+  return (need + 15) & ~(size_t)15;
 }
 
 // Dynamic shared memory of k_rb_build: cut-off table [+ list tile] [+ window scratch].
@@ -615,7 +626,7 @@ ForceFn force_fn_raw(int tp, bool fused, bool stress, int mode) {
 // shared memory the staged list tile `a` needs.
 ForceFn force_fn(const b2md_engine* e, bool fused, bool stress, const EngArgs& a) {
   ForceFn fn = force_fn_raw(e->tp, fused, stress, e->force_mode);
-  if (force_smem(a, e->force_mode) > kMaxDynSmemBytes)
+  if (force_smem(e, a) > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
   return fn;
 }
@@ -660,7 +671,7 @@ int force_grid(const b2md_engine* e, const EngArgs& a, ForceFn fn, size_t smem) 
 void launch_force(b2md_engine* e, cudaStream_t s, const EngArgs& a, bool fused, bool stress) {
   if (e->ntiles == 0) return;
   ForceFn fn = force_fn(e, fused, stress, a);
-  const size_t smem = force_smem(a, e->force_mode);
+  const size_t smem = force_smem(e, a);
   fn<<<force_grid(e, a, fn, smem), e->pb * e->tp, smem, s>>>(a, 0, cudaGraphConditionalHandle{});
 }
 
@@ -671,7 +682,7 @@ void build_graph(b2md_engine* e, int which, int K) {
   EngArgs a = make_args(e);
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
-  const size_t smem = force_smem(a, e->force_mode);
+  const size_t smem = force_smem(e, a);
   ForceFn fstep = force_fn(e, true, false, a);
   if (e->cond_mode) {
     std::vector<cudaGraphConditionalHandle> hs(K);
@@ -1444,7 +1455,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     long long nl = 2;
-    const size_t smem = force_smem(a, e->force_mode);
+    const size_t smem = force_smem(e, a);
     ForceFn fstep = force_fn(e, true, false, a);
     std::vector<cudaEvent_t> ev(2 * nsteps);
     for (auto& x : ev) CK(cudaEventCreate(&x));

@@ -134,6 +134,7 @@ struct EngArgs {
   int nrep;
   int idx_pitch;  // k_force: slots per staged list block (pb)
   int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
+  int max_types;  // largest type count over the active replicas (pair-table rows in shared memory)
   unsigned short* wl;  // window list (force mode 2)
   int4* wseg;          // per-tile window segments
   int2* wmeta;         // per-tile (segments, particles)

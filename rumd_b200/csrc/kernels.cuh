@@ -255,6 +255,51 @@ struct PairAcc {
   float sxx = 0.f, syy = 0.f, szz = 0.f, syz = 0.f, sxz = 0.f, sxy = 0.f;
 };
 
+// The pair rows of particle i's type, looked up by the neighbour's type.
+//   RowsShared  the packed rows in shared memory: any pair function, any
+//               number of types;
+//   RowsLJ<NT>  the LJ 12-6 rows (rc^2, A12, A6, c_s, c_u0) of a replica with
+//               NT = 1 or 2 types, held in registers: no lookup (NT = 1) or a
+//               select (NT = 2), which keeps the table reads off the L1 data
+//               pipe that the neighbour gathers use.
+struct RowsShared {
+  const float* prow;
+  __device__ __forceinline__ const float* row(int tj) const { return prow + tj * kParStride; }
+  __device__ __forceinline__ void lj(int tj, float4& q, float& cu0) const {
+    const float* pp = row(tj);
+    q = *reinterpret_cast<const float4*>(pp);
+    cu0 = pp[4];
+  }
+};
+
+template <int NT>
+struct RowsLJ {
+  float4 q0, q1;
+  float c0, c1;
+  __device__ __forceinline__ explicit RowsLJ(const float* prow) {
+    q0 = *reinterpret_cast<const float4*>(prow);
+    c0 = prow[4];
+    if (NT == 2) {
+      q1 = *reinterpret_cast<const float4*>(prow + kParStride);
+      c1 = prow[kParStride + 4];
+    } else {
+      q1 = q0;
+      c1 = c0;
+    }
+  }
+  __device__ __forceinline__ const float* row(int) const { return nullptr; }
+  __device__ __forceinline__ void lj(int tj, float4& q, float& cu0) const {
+    if (NT == 1) {
+      q = q0;
+      cu0 = c0;
+    } else {
+      const bool b = tj != 0;
+      q = make_float4(b ? q1.x : q0.x, b ? q1.y : q0.y, b ? q1.z : q0.z, b ? q1.w : q0.w);
+      cu0 = b ? c1 : c0;
+    }
+  }
+};
+
 // fij (PairPotential.h:1198-1244) for one neighbour, without branches so
 // that consecutive pairs interleave, for the pair function POT:
 //   POT_LJ_12_6            Pot_IPL_12_6 / Pot_LJ_12_6::ComputeInteraction
@@ -268,8 +313,8 @@ struct PairAcc {
 // s(rc) rc / r and s(rc) rc (r - rc) - u(rc) for SF, -u(rc) for SP, 0 for NS.
 // WRAP = false skips the minimum-image step; the caller uses it only when it
 // is exactly the identity (see k_force).
-template <bool STRESS, bool WRAP, int POT = POT_LJ_12_6>
-__device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const float4& rj, const float* prow, float Lx,
+template <bool STRESS, bool WRAP, int POT, class Rows>
+__device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const float4& rj, const Rows& rows, float Lx,
                                         float Ly, float Lz, float iLx, float iLy, float iLz) {
   float dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
   if (WRAP) {
@@ -278,21 +323,23 @@ __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const floa
     dz = mi_comp(dz, Lz, iLz);
   }
   const float d2 = dist2_ref(dx, dy, dz);
-  const float* pp = prow + __float_as_int(rj.w) * kParStride;
+  const int tj = __float_as_int(rj.w);
   float y = rsqrt_approx(d2);
   y = y * __fmaf_rn(-0.5f * d2 * y, y, 1.5f);
   const float i2 = y * y;
   float s, u;
   bool in;
-  if (POT == POT_LJ_12_6) {
-    const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, A12, A6, c_s
-    const float2 q2 = *reinterpret_cast<const float2*>(pp + 4);  // c_u0, c_ur
+  if constexpr (POT == POT_LJ_12_6) {
+    float4 q;  // rc^2, A12, A6, c_s (= c_ur)
+    float cu0;
+    rows.lj(tj, q, cu0);
     const float i6 = i2 * i2 * i2;
     const float t = q.y * i6;
     s = __fmaf_rn(-q.w, y, i6 * i2 * __fmaf_rn(12.f, t, 6.f * q.z));
-    u = __fmaf_rn(i6, t + q.z, __fmaf_rn(q2.y, d2 * y, q2.x));
+    u = __fmaf_rn(i6, t + q.z, __fmaf_rn(q.w, d2 * y, cu0));
     in = d2 < q.x;
-  } else if (POT == POT_LJ_12_6_SMOOTH_2_4) {
+  } else if constexpr (POT == POT_LJ_12_6_SMOOTH_2_4) {
+    const float* pp = rows.row(tj);
     const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, sigma^2, 4 eps, b
     const float4 q1 = *reinterpret_cast<const float4*>(pp + 4);  // c, e, -, g
     const float2 q2 = *reinterpret_cast<const float2*>(pp + 8);  // c_s, c_u0
@@ -302,6 +349,7 @@ __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const floa
     u = __fmaf_rn(q.z * t6, t6 - 1.f, __fmaf_rn(d2, __fmaf_rn(q1.w, d2, q1.y), __fmaf_rn(q2.x, d2 * y, q2.y)));
     in = d2 < q.x;
   } else {
+    const float* pp = rows.row(tj);
     const float4 q = *reinterpret_cast<const float4*>(pp);       // rc^2, sigma^2, eps, n/2
     const float ne = pp[4];                                       // n eps
     const float2 q2 = *reinterpret_cast<const float2*>(pp + 8);  // c_s, c_u0
@@ -479,9 +527,9 @@ struct PosWindow {
 // The neighbour loop of one thread: its entries (lane_entry) in groups of
 // four -- one vector load of list entries, four neighbour positions in
 // flight -- then the remaining ones singly.  Only entries below nn are read.
-template <int TP, bool STRESS, bool WRAP, int POT, class Idx, class Pos>
+template <int TP, bool STRESS, bool WRAP, int POT, class Idx, class Pos, class Rows>
 __device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos& pos, unsigned lane_t, unsigned nn,
-                                           const float4& ri, const float* prow, float Lx, float Ly, float Lz,
+                                           const float4& ri, const Rows& prow, float Lx, float Ly, float Lz,
                                            float iLx, float iLy, float iLz) {
   const unsigned cnt = lane_count<TP>(nn, lane_t);
   unsigned q = 0;
@@ -499,28 +547,42 @@ __device__ __forceinline__ void force_loop(PairAcc& A, const Idx& idx, const Pos
   }
 }
 
-// The loop for the replica's pair function (block-uniform) and minimum-image need.
-template <int TP, bool STRESS, class Idx, class Pos>
-__device__ __forceinline__ void force_loop_any(bool fast, int pot, PairAcc& A, const Idx& idx, const Pos& pos,
+// The loop for the replica's pair function and type count (block-uniform)
+// and minimum-image need.  REG: single-type LJ 12-6 replicas hold their row
+// in registers (3.5 % faster at N = 1M; for two types the selects cost more
+// than the shared-memory lookups they replace, 40.2 vs 37.6 us at KA 65536).
+template <int TP, bool STRESS, bool REG, class Idx, class Pos>
+__device__ __forceinline__ void force_loop_any(bool fast, int pot, int nt, PairAcc& A, const Idx& idx, const Pos& pos,
                                                unsigned lane_t, unsigned nn, const float4& ri, const float* prow,
                                                float Lx, float Ly, float Lz, float iLx, float iLy, float iLz) {
-#define FL(W, P) force_loop<TP, STRESS, W, P>(A, idx, pos, lane_t, nn, ri, prow, Lx, Ly, Lz, iLx, iLy, iLz)
+#define FL(W, P, ROWS) force_loop<TP, STRESS, W, P>(A, idx, pos, lane_t, nn, ri, ROWS, Lx, Ly, Lz, iLx, iLy, iLz)
+  const RowsShared sh{prow};
   if (pot == POT_LJ_12_6) {
-    if (fast) FL(false, POT_LJ_12_6);
-    else FL(true, POT_LJ_12_6);
+    if (REG && nt == 1) {
+      const RowsLJ<1> rg(prow);
+      if (fast) FL(false, POT_LJ_12_6, rg);
+      else FL(true, POT_LJ_12_6, rg);
+    } else {
+      if (fast) FL(false, POT_LJ_12_6, sh);
+      else FL(true, POT_LJ_12_6, sh);
+    }
   } else if (pot == POT_LJ_12_6_SMOOTH_2_4) {
-    if (fast) FL(false, POT_LJ_12_6_SMOOTH_2_4);
-    else FL(true, POT_LJ_12_6_SMOOTH_2_4);
+    if (fast) FL(false, POT_LJ_12_6_SMOOTH_2_4, sh);
+    else FL(true, POT_LJ_12_6_SMOOTH_2_4, sh);
   } else {
-    if (fast) FL(false, POT_IPL_N);
-    else FL(true, POT_IPL_N);
+    if (fast) FL(false, POT_IPL_N, sh);
+    else FL(true, POT_IPL_N, sh);
   }
 #undef FL
 }
 
 // Shared memory of k_force: [packed pair table, kParSmemFloats]
-// [MODE 1: list tile | MODE 2: position window, win_cap float4]
+// [MODE 1: list tile | MODE 2: position window, win_cap float4]; after the
+// neighbour loop the block reduction's scratch (force_red_bytes) overlays it.
 constexpr int kParSmemFloats = kMaxTypes * kMaxTypes * kParStride;
+__host__ __device__ constexpr int force_red_bytes(int threads) {
+  return ((threads + 31) / 32) * kNPart * (int)sizeof(double) + threads * (int)sizeof(double);
+}
 constexpr unsigned kWaitPolls = 1u << 22;
 
 enum { FM_STREAMED = 0, FM_STAGED = 1, FM_WINDOW = 2 };
@@ -543,8 +605,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
   unsigned short* s_wl = reinterpret_cast<unsigned short*>(s_win + a.win_cap);  // mode 2: staged window list
-  __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
-  __shared__ double s_scr[kMaxBlock];
+  // the block reduction's scratch reuses the start of the dynamic region once
+  // every thread is past the neighbour loop (force_red_bytes)
+  double* s_warp = reinterpret_cast<double*>(s_dyn);
+  double* s_scr = s_warp + (blockDim.x >> 5) * kNPart;
   __shared__ double s_blk[kNPart], s_tot[kNPart];
   __shared__ __align__(8) uint64_t s_bar;
   __shared__ unsigned s_rows;
@@ -658,13 +722,13 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       const bool ok = __syncthreads_and(mbar_wait_bounded(&s_bar, 0, kWaitPolls));
       if (ok) {
         if (MODE == FM_STAGED)
-          force_loop_any<TP, STRESS>(fast, R.potential, A, IdxStaged{s_idx + lp * 8, pitch * 8}, PosGlobal{rc}, lane_t, nn, ri, prow,
+          force_loop_any<TP, STRESS, false>(fast, R.potential, nt, A, IdxStaged{s_idx + lp * 8, pitch * 8}, PosGlobal{rc}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
         else if (wl_staged)
-          force_loop_any<TP, STRESS>(fast, R.potential, A, IdxWindowStaged{s_wl + lp * 8, pitch * 8}, PosWindow{s_win}, lane_t, nn,
+          force_loop_any<TP, STRESS, false>(fast, R.potential, nt, A, IdxWindowStaged{s_wl + lp * 8, pitch * 8}, PosWindow{s_win}, lane_t, nn,
                                      ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
         else
-          force_loop_any<TP, STRESS>(fast, R.potential, A, IdxWindow{wbase, (unsigned)i, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
+          force_loop_any<TP, STRESS, false>(fast, R.potential, nt, A, IdxWindow{wbase, (unsigned)i, lstride}, PosWindow{s_win}, lane_t, nn, ri, prow,
                                      Lx, Ly, Lz, iLx, iLy, iLz);
       } else {
         // the copies did not land in time: record it for the host and wait
@@ -674,7 +738,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     } else {
       __syncthreads();  // the pair table
-      force_loop_any<TP, STRESS>(fast, R.potential, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
+      force_loop_any<TP, STRESS, true>(fast, R.potential, nt, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
                                  Lz, iLx, iLy, iLz);
     }
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
@@ -724,10 +788,10 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
         a.r[rb ^ 1][gi] = rn;
       }
     }
-    if (FUSED) {
-      const int ex = __syncthreads_or(exceed);
-      if (ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
-    }
+    // every thread is past the neighbour loop: the pair table (and the staged
+    // tile) may be overwritten by the reduction scratch
+    const int ex = __syncthreads_or(exceed);
+    if (FUSED && ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
     block_sum8(acc, s_warp, s_blk);
     if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
       if (FUSED) {
