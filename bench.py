@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--force-mode", type=int, default=None, help="kernel variant: 0 streamed, 1 staged, 2 window")
     p.add_argument("--build-lanes", type=int, default=None, help="kernel variant: list-build lanes per particle")
     p.add_argument("--sm-tiles", type=int, default=None, help="kernel variant: 1 = SM-region tile claiming")
+    p.add_argument("--persistent", type=int, default=None,
+                   help="kernel variant: 1 = one cooperative kernel runs the steps between list rebuilds")
     p.add_argument("--profile-launches", action="store_true",
                    help="small plain run only (for the ncu launch list)")
     p.add_argument("--lj1m", action="store_true",
@@ -235,12 +237,17 @@ def time_run(capi, e, steps, device):
     return t0.elapsed_time(t1) / 1e3
 
 
-def launches_in_run(steps, rebuilds, per_rebuild=8):
-    # per step: fused kernel; per graph launch: gate; per rebuild: 8 kernels
-    # (9 with position windows); run start: steps + momentum; run end:
-    # rebuild sequence + force kernel
-    graph_launches = steps // 32 + steps % 32
-    return int(steps + graph_launches + per_rebuild * rebuilds + 2 + per_rebuild + 1)
+def launches_in_run(steps, rebuilds, per_rebuild=8, persistent=False):
+    # run start: steps + momentum; run end: rebuild sequence + force kernel;
+    # per rebuild: 8 kernels (9 with position windows).  Per-step graphs: a
+    # fused kernel per step and a gate per graph launch.  Persistent graph:
+    # one loop gate, then per loop pass a gate and one k_steps launch (a pass
+    # ends at each rebuild).
+    if persistent:
+        core = 1 + 2 * (rebuilds + 1)
+    else:
+        core = steps + steps // 32 + steps % 32
+    return int(core + per_rebuild * rebuilds + 2 + per_rebuild + 1)
 
 
 def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
@@ -402,7 +409,8 @@ def config_block(args, world, engine=None):
     if engine is not None:
         from rumd_b200 import capi
         variants = {"force_mode": engine.get_variant(capi.VARIANT_FORCE_MODE),
-                    "build_lanes": engine.get_variant(capi.VARIANT_BUILD_LANES)}
+                    "build_lanes": engine.get_variant(capi.VARIANT_BUILD_LANES),
+                    "persistent": engine.get_variant(capi.VARIANT_PERSISTENT)}
     return {"workload": f"Kob-Andersen 80:20 LJ, N={N_PLAIN}, rho=1.2, T=0.45, NVT tau=0.2, dt=0.005, skin 0.3, "
                         "SF cut-off 2.5 sigma_ij (plain method, single large system)",
             "n_particles": N_PLAIN, "pb": args.pb, "tp": args.tp, **variants,
@@ -456,6 +464,7 @@ def main():
     KERNEL_VARIANTS[capi.VARIANT_FORCE_MODE] = args.force_mode
     KERNEL_VARIANTS[capi.VARIANT_BUILD_LANES] = args.build_lanes
     KERNEL_VARIANTS[capi.VARIANT_SM_TILES] = args.sm_tiles
+    KERNEL_VARIANTS[capi.VARIANT_PERSISTENT] = args.persistent
     device = local
     if args.lj1m:
         lj_hbm_scale(capi, device, args)
@@ -499,6 +508,7 @@ def main():
     t_max = dist.max(t)
     st = e.stats(rid)
     rebuilds = st["rebuilds"] - rb0
+    persistent_active = e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == 1
     total_ps = dist.sum(N_PLAIN * args.steps)
     value = total_ps / t_max
     # live roofline of the dominant kernel (the fused force+integrate step)
@@ -533,7 +543,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded FCC start, melted and equilibrated untimed)",
                 "config": cfg, "clocks": clk, "e2e": e2e,
-                "gpu_launches": launches_in_run(args.steps, rebuilds, per_rebuild), "rebuilds": rebuilds,
+                "gpu_launches": launches_in_run(args.steps, rebuilds, per_rebuild, persistent_active), "rebuilds": rebuilds,
                 "roofline": roofline}
         line.update(extra)
         print(json.dumps(line), flush=True)

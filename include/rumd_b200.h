@@ -159,6 +159,14 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *                              tiles from its SM's share of the tile range,
  *                              so each SM works on neighbouring tiles whose
  *                              neighbours share its L1; 0 = one block per tile.
+ *   B2MD_VARIANT_PERSISTENT    1 (default): b2md_run drives streamed-mode
+ *                              engines whose tiles all fit on the GPU at once
+ *                              with one cooperative kernel that runs steps
+ *                              back to back, with a grid barrier between
+ *                              them, until a list rebuild is due; 0: one
+ *                              kernel launch per step.
+ *   B2MD_VARIANT_PERSISTENT_ACTIVE  read-only: 1 when the last run used the
+ *                              persistent kernel.
  * No reference counterpart beyond Sample::SetPB_TP (Sample.h:96). */
 enum {
   B2MD_VARIANT_FORCE_MODE = 0,
@@ -166,7 +174,9 @@ enum {
   B2MD_VARIANT_BUILD_SMEM = 2,
   B2MD_VARIANT_WINDOW_CAP = 3,
   B2MD_VARIANT_SM_TILES = 4,
-  B2MD_VARIANT_WINDOW_LIST_ROWS = 5
+  B2MD_VARIANT_WINDOW_LIST_ROWS = 5,
+  B2MD_VARIANT_PERSISTENT = 6,
+  B2MD_VARIANT_PERSISTENT_ACTIVE = 7
 };
 B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
 B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);

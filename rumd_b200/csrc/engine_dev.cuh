@@ -100,6 +100,20 @@ struct RepState {
   int pad_;
 };
 
+// Control block of the persistent step kernel (k_steps), one per engine.
+constexpr int kPersistMaxSm = 1024;    // SM ids the tile order can use
+constexpr int kPersistMaxGrid = 8192;  // blocks the tile order can rank
+struct PersistCtl {
+  unsigned gen;     // grid-barrier generation
+  unsigned arrive;  // blocks arrived at the current grid barrier
+  int go;           // the last barrier's decision: run another step
+  int budget;       // steps this graph launch may still run (set by the host)
+  int more;         // replicas with steps left after the current step
+  int err;          // a grid-barrier wait gave up (reported to the host)
+  unsigned smslot[kPersistMaxSm];  // blocks of this launch seen per SM id
+  unsigned rank[kPersistMaxGrid];  // per block: slot on its SM * nsmid + SM id
+};
+
 struct EngArgs {
   float4* r[2];
   float4* v[2];
@@ -135,6 +149,8 @@ struct EngArgs {
   int idx_pitch;  // k_force: slots per staged list block (pb)
   int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
   int max_types;  // largest type count over the active replicas (pair-table rows in shared memory)
+  PersistCtl* pctl;  // k_steps control block
+  int persist;       // 1 in the persistent step graph: finish_step counts replicas with steps left
   unsigned short* wl;  // window list (force mode 2)
   int4* wseg;          // per-tile window segments
   int2* wmeta;         // per-tile (segments, particles)

@@ -217,31 +217,45 @@ __device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float
 __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState* S, const double* tot,
                             bool with_forces) {
   if (threadIdx.x != 0) return;
+  // the state is read past L1 (in k_steps the previous step's finalizer may
+  // have run on another SM), all loads at once: this runs on the step's
+  // critical path
+  const double T0 = __ldcg(&S->T), dT = __ldcg(&S->dT), xi0 = __ldcg(&S->xi);
+  const double pe0 = __ldcg(&S->pe), vir0 = __ldcg(&S->vir);
+  const long long run_idx = __ldcg(&S->run_step);  // step index inside the current run, before this step
+  const long long steps = __ldcg(&S->steps), left = __ldcg(&S->steps_left);
+  const int rbuf = __ldcg(&S->rbuf), nlog = __ldcg(&S->nlog);
+  double xi = xi0, T = T0;
   if (R.thermo_mask) {
-    double dev = tot[P_KE2] / (R.dof * S->T) - 1.0;
+    double dev = tot[P_KE2] / (R.dof * T0) - 1.0;
     if (dev > 10.0) dev = 10.0;  // updateNVTThermostatState (IntegratorNVT.cu:426-437)
-    S->xi += (double)R.dt * (double)R.omega2 * dev;
-    S->T += S->dT;
+    xi = xi0 + (double)R.dt * (double)R.omega2 * dev;
+    T = T0 + dT;
   }
+  S->xi = xi;
+  S->T = T;
   S->ke2 = tot[P_KE2];
   S->ke_t = tot[P_KET];
-  if (with_forces) { S->pe = tot[P_PE]; S->vir = tot[P_W] / 6.0; }
+  const double pe = with_forces ? tot[P_PE] : pe0, vir = with_forces ? tot[P_W] / 6.0 : vir0;
+  S->pe = pe;
+  S->vir = vir;
   S->P[0] = tot[P_PX]; S->P[1] = tot[P_PY]; S->P[2] = tot[P_PZ]; S->M = tot[P_M];
-  const long long run_idx = S->run_step;  // step index inside the current run, before this step
-  S->rbuf ^= 1;
-  S->steps += 1;
-  S->run_step += 1;
-  if (S->steps_left > 0) S->steps_left -= 1;
+  S->rbuf = rbuf ^ 1;
+  S->steps = steps + 1;
+  S->run_step = run_idx + 1;
+  if (left > 0) S->steps_left = left - 1;
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
   if (ex > 0) atomicAdd(a.any_rebuild, 1);
+  // k_steps: replicas that still have steps after this one
+  if (a.persist && left > 1) atomicAdd(&a.pctl->more, 1);
   // energies at run steps i with i % interval == 0, as Simulation.Run's
   // energies output schedule (Simulation.py:44, 587-589)
   if (R.energy_interval > 0 && (run_idx % R.energy_interval) == 0 && R.energy_cap > 0) {
-    int k = S->nlog % R.energy_cap;
+    int k = nlog % R.energy_cap;
     double* e = a.elog + (size_t)(R.elog0 + k) * 5;
-    e[0] = (double)run_idx; e[1] = S->pe; e[2] = S->vir; e[3] = S->ke_t; e[4] = S->xi;
-    S->nlog += 1;
+    e[0] = (double)run_idx; e[1] = pe; e[2] = vir; e[3] = tot[P_KET]; e[4] = xi;
+    S->nlog = nlog + 1;
   }
 }
 
@@ -519,6 +533,16 @@ struct PosGlobal {
   const float4* __restrict__ p;
   __device__ __forceinline__ float4 operator()(unsigned j) const { return __ldg(p + j); }
 };
+// Positions that other blocks of the same launch rewrite (k_steps): plain
+// L1-cached loads (no __restrict__, so never the read-only path), ordered
+// after the step barrier's acquire.
+struct PosCoherent {
+  const float4* p;
+  __device__ __forceinline__ float4 operator()(unsigned j) const { return p[j]; }
+};
+template <bool B, class T, class F> struct Pick { using type = T; };
+template <class T, class F> struct Pick<false, T, F> { using type = F; };
+
 struct PosWindow {
   const float4* p;
   __device__ __forceinline__ float4 operator()(unsigned j) const { return p[j]; }
@@ -598,9 +622,35 @@ enum { FM_STREAMED = 0, FM_STAGED = 1, FM_WINDOW = 2 };
 //                TMA bulk copy per segment, and the 16-bit window list read
 //                from global memory: every neighbour position comes from shared
 //                memory.  Tiles without a window (wmeta < 0) stream.
-template <int TP, bool FUSED, bool STRESS, int MODE>
-__global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cudaGraphConditionalHandle h) {
-  extern __shared__ __align__(128) unsigned char s_dyn[];
+// One tile of the force kernels (see k_force).  PERSIST: inside k_steps,
+// where other blocks rewrite positions and replica state between steps of
+// the same launch, so those are read through coherent loads (no read-only
+// path) and the state fields past L1.
+// The replica-state fields a step reads.  In k_steps the previous step's
+// finalizer (on another SM) wrote them, so thread 0 reads them past L1 once
+// per tile and the block shares them through shared memory.
+struct StepView {
+  int overflow, rbuf, abuf, pad_;
+  long long steps_left, run_step;
+  double M, P[3], xi;
+};
+
+__device__ __forceinline__ void load_view(StepView& v, const RepState* S) {
+  v.overflow = __ldcg(&S->overflow);
+  v.rbuf = __ldcg(&S->rbuf);
+  v.abuf = __ldcg(&S->abuf);
+  v.steps_left = __ldcg(&S->steps_left);
+  v.run_step = __ldcg(&S->run_step);
+  v.M = __ldcg(&S->M);
+  v.P[0] = __ldcg(&S->P[0]);
+  v.P[1] = __ldcg(&S->P[1]);
+  v.P[2] = __ldcg(&S->P[2]);
+  v.xi = __ldcg(&S->xi);
+}
+
+template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
+__device__ __forceinline__ void force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
+                                           double* s_tot, uint64_t& s_bar, unsigned& s_rows) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -609,36 +659,22 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
   // every thread is past the neighbour loop (force_red_bytes)
   double* s_warp = reinterpret_cast<double*>(s_dyn);
   double* s_scr = s_warp + (blockDim.x >> 5) * kNPart;
-  __shared__ double s_blk[kNPart], s_tot[kNPart];
-  __shared__ __align__(8) uint64_t s_bar;
-  __shared__ unsigned s_rows;
-  __shared__ int s_tile;
-  // SM tiles (streamed mode): a grid of at most as many blocks as fit at once;
-  // each block claims tiles from its SM's region of the tile range, so the
-  // tiles an SM processes are neighbours in space and share its L1
-  const bool sm_tiles = MODE == FM_STREAMED && a.nreg > 0;
-  int tile = blockIdx.x;
-  for (;;) {
-  if (sm_tiles) {
-    __syncthreads();  // the previous tile is done with shared memory
-    if (threadIdx.x < 32) {
-      const int t = claim_tile(a);
-      if (threadIdx.x == 0) s_tile = t;
-    }
-    __syncthreads();
-    tile = s_tile;
-    if (tile < 0) break;
-  }
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
-  const bool skip = (S->overflow != 0) || (FUSED && S->steps_left <= 0) || !R.active;
+  __shared__ StepView s_view;
+  if constexpr (PERSIST) {
+    if (threadIdx.x == 0) load_view(s_view, S);
+    __syncthreads();
+  }
+#define SV(f) (PERSIST ? s_view.f : S->f)
+  const bool skip = (SV(overflow) != 0) || (FUSED && SV(steps_left) <= 0) || !R.active;
   if (!skip) {
     const int pb = blockDim.x / TP;
     const int first = a.tile_first[tile];
     const int pitch = a.idx_pitch;
-    const int rb = S->rbuf;
-    const float4* __restrict__ rc = a.r[rb] + R.p0;
+    const int rb = SV(rbuf);
+    const float4* rc = a.r[rb] + R.p0;
     const int2 wm = MODE == FM_WINDOW ? a.wmeta[tile] : make_int2(-1, -1);
     const bool use_bar = MODE == FM_STAGED || (MODE == FM_WINDOW && wm.x >= 0);
     if (use_bar) {
@@ -702,7 +738,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
     const bool valid = i < R.n;
     const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
-    const float4 ri = valid ? rc[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 ri = valid ? (PERSIST ? rc[i] : __ldg(rc + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
     const int ti = valid ? __float_as_int(ri.w) : 0;
     const float* prow = s_par + ti * nt * kParStride;
     const unsigned nn = valid ? a.nn[R.p0 + i] : 0u;
@@ -738,7 +774,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     } else {
       __syncthreads();  // the pair table
-      force_loop_any<TP, STRESS, true>(fast, R.potential, nt, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosGlobal{rc}, lane_t, nn, ri, prow, Lx, Ly,
+      using PosS = typename Pick<PERSIST, PosCoherent, PosGlobal>::type;
+      force_loop_any<TP, STRESS, true>(fast, R.potential, nt, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosS{rc}, lane_t, nn, ri, prow, Lx, Ly,
                                  Lz, iLx, iLy, iLz);
     }
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
@@ -774,15 +811,16 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       acc[P_PE] = (double)fo.w;
       acc[P_W] = (double)ww;
       if (FUSED) {
-        const int ab = S->abuf;
+        const int ab = SV(abuf);
         float4 v = a.v[ab][gi];
         int4 im = a.im[ab][gi];
-        const bool do_reset = R.reset_interval > 0 && (S->run_step % R.reset_interval) == 0;
+        const bool do_reset = R.reset_interval > 0 && (SV(run_step) % R.reset_interval) == 0;
         float3 vs = make_float3(0.f, 0.f, 0.f);
-        if (do_reset && S->M > 0.0)
-          vs = make_float3((float)(S->P[0] / S->M), (float)(S->P[1] / S->M), (float)(S->P[2] / S->M));
+        const double M = SV(M);
+        if (do_reset && M > 0.0)
+          vs = make_float3((float)(SV(P[0]) / M), (float)(SV(P[1]) / M), (float)(SV(P[2]) / M));
         float4 rn;
-        integrate_one(R, (float)S->xi, vs, do_reset, ri, fo, v, im, rn, acc, exceed, a.last_r[gi]);
+        integrate_one(R, (float)SV(xi), vs, do_reset, ri, fo, v, im, rn, acc, exceed, a.last_r[gi]);
         a.v[ab][gi] = v;
         a.im[ab][gi] = im;
         a.r[rb ^ 1][gi] = rn;
@@ -802,9 +840,199 @@ __global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cu
       }
     }
   }
-  if (!sm_tiles) break;
-  }  // tiles
+#undef SV
+}
+
+// One tile of pb particles per block, tp threads per particle.  MODE selects
+// how the neighbours are read:
+//   FM_STREAMED  list entries and neighbour positions read from global memory
+//                inside the loop (positions through L1);
+//   FM_STAGED    the tile's list rows copied to shared memory first (TMA bulk
+//                copies), positions gathered from global memory;
+//   FM_WINDOW    the tile's position window (every slot segment holding a
+//                listed neighbour of the tile) copied to shared memory with one
+//                TMA bulk copy per segment, and the 16-bit window list read
+//                from global memory: every neighbour position comes from shared
+//                memory.  Tiles without a window (wmeta < 0) stream.
+template <int TP, bool FUSED, bool STRESS, int MODE>
+__global__ void __launch_bounds__(kMaxBlock) k_force(EngArgs a, int has_cond, cudaGraphConditionalHandle h) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ unsigned s_rows;
+  __shared__ int s_tile;
+  // SM tiles (streamed mode): a grid of at most as many blocks as fit at once;
+  // each block claims tiles from its SM's region of the tile range, so the
+  // tiles an SM processes are neighbours in space and share its L1
+  const bool sm_tiles = MODE == FM_STREAMED && a.nreg > 0;
+  int tile = blockIdx.x;
+  for (;;) {
+    if (sm_tiles) {
+      __syncthreads();  // the previous tile is done with shared memory
+      if (threadIdx.x < 32) {
+        const int t = claim_tile(a);
+        if (threadIdx.x == 0) s_tile = t;
+      }
+      __syncthreads();
+      tile = s_tile;
+      if (tile < 0) break;
+    }
+    force_tile<TP, FUSED, STRESS, MODE, false>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows);
+    if (!sm_tiles) break;
+  }
   grid_final(a, has_cond, h);
+}
+
+// End of one step of k_steps: a grid barrier.  Every block arrives once its
+// tiles are done (the replica finalizers after their finish_step); the last
+// one to arrive resets the barrier and decides whether the launch goes on:
+// not when a list rebuild is due (the graph's rebuild node runs first), the
+// step budget of the graph launch is spent, or no replica has steps left; it
+// then sets the graph's loop condition.  The others wait for the decision,
+// at most kBarrierPolls polls; a wait that gives up records the error and
+// ends the graph's loop, so every block returns.
+constexpr unsigned kBarrierPolls = 1u << 22;  // > 0.25 s of 64 ns sleeps
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits (bounded) until the grid barrier of generation gen is released;
+// false when the wait gave up (recorded, and the graph's loop ended).
+__device__ bool barrier_wait(PersistCtl* c, unsigned gen, cudaGraphConditionalHandle h_loop) {
+  for (unsigned it = 0;; ++it) {
+    if (ld_acquire_u32(&c->gen) != gen) break;
+    if (it >= kBarrierPolls) {
+      atomicExch(&c->err, 1);
+      cudaGraphSetConditional(h_loop, 0u);
+      return false;
+    }
+    __nanosleep(64);
+  }
+  __threadfence();
+  return true;
+}
+
+// Grid barrier at the start of k_steps, after every block has entered its
+// rank; the last block to arrive clears the per-SM counters for the next
+// launch.
+__device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditionalHandle h_loop) {
+  PersistCtl* c = a.pctl;
+  const unsigned gen = ld_acquire_u32(&c->gen);
+  __threadfence();
+  const unsigned n = atomicAdd(&c->arrive, 1u);
+  if (n == gridDim.x - 1) {
+    __threadfence();
+    c->arrive = 0u;
+    for (unsigned k = 0; k < nsmid && k < (unsigned)kPersistMaxSm; ++k) c->smslot[k] = 0u;
+    __threadfence();
+    st_release_u32(&c->gen, gen + 1u);
+    return true;
+  }
+  return barrier_wait(c, gen, h_loop);
+}
+
+__device__ int step_barrier(const EngArgs& a, cudaGraphConditionalHandle h_loop) {
+  PersistCtl* c = a.pctl;
+  const unsigned gen = ld_acquire_u32(&c->gen);
+  __threadfence();
+  const unsigned n = atomicAdd(&c->arrive, 1u);
+  if (n == gridDim.x - 1) {
+    __threadfence();
+    c->arrive = 0u;
+    const int any = atomicExch(a.any_rebuild, 0);
+    const int more = atomicExch(&c->more, 0);
+    const int budget = c->budget - 1;
+    c->budget = budget;
+    const int go = any == 0 && more > 0 && budget > 0;
+    c->go = go;
+    if (!go) cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
+    __threadfence();
+    st_release_u32(&c->gen, gen + 1u);
+    return go;
+  }
+  if (!barrier_wait(c, gen, h_loop)) return 0;
+  return __ldcg(&c->go);
+}
+
+// Many fused steps in one cooperative launch (every block resident): each
+// block works its tiles of a step, then the grid meets at step_barrier.
+// Tile order: at launch each block takes a slot on its SM and ranks itself
+// by (slot, SM id); the block of dense rank d works tiles d, d + gridDim.x,
+// ...  An SM's blocks then hold tiles about one SM count apart, spread over
+// the box, as the hardware places a plain launch's blocks (the scheduler
+// puts consecutive blocks of a cooperative grid on the same SM, and
+// neighbouring tiles on one SM made the SMs holding the box faces, whose
+// particles need the minimum image, finish last).  The launch ends when a list rebuild is due,
+// the step budget is spent or no replica has steps left; the step graph's
+// loop then runs the rebuild (when due) and launches it again.  Positions,
+// forces, the thermostat and every reduction are those of k_force<TP, true,
+// false, FM_STREAMED>, bit for bit.
+template <int TP>
+__global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditionalHandle h_loop) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ unsigned s_rows;
+  __shared__ int s_go;
+  __shared__ unsigned s_rank;
+  __shared__ int s_first;
+  PersistCtl* c = a.pctl;
+  const bool ranked = gridDim.x <= (unsigned)kPersistMaxGrid;
+  if (threadIdx.x == 0) {
+    s_go = __ldcg(&c->err) == 0;
+    if (!s_go && blockIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
+    s_first = ranked ? 0 : (int)blockIdx.x;
+    if (s_go && ranked) {
+      unsigned smid, nsmid;
+      asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+      asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsmid));
+      // ranks are unique: (slot, SM id) pairs, or 2^31 + block index
+      const unsigned r = smid < (unsigned)kPersistMaxSm ? atomicAdd(&c->smslot[smid], 1u) * nsmid + smid
+                                                        : 0x80000000u + blockIdx.x;
+      s_rank = r;
+      c->rank[blockIdx.x] = r;
+      s_go = setup_barrier(a, nsmid, h_loop);
+    }
+  }
+  __syncthreads();
+  if (s_go && ranked) {
+    unsigned below = 0;
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) below += __ldcg(&c->rank[b]) < s_rank;
+    if (threadIdx.x == 0) s_first = 0;
+    __syncthreads();
+    atomicAdd(&s_first, (int)below);
+    __syncthreads();
+  }
+  while (s_go) {
+    for (int tile = s_first; tile < a.ntiles; tile += gridDim.x) {
+      force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows);
+      __syncthreads();  // the next tile reloads the pair table
+    }
+    if (threadIdx.x == 0) s_go = step_barrier(a, h_loop);
+    __syncthreads();
+  }
+}
+
+// Start of the persistent step graph: whether its loop runs at all.
+__global__ void k_gate_loop(EngArgs a, cudaGraphConditionalHandle h_loop) {
+  __shared__ int s_any;
+  if (threadIdx.x == 0) s_any = 0;
+  __syncthreads();
+  for (int r = threadIdx.x; r < a.nrep; r += blockDim.x)
+    if (a.rep[r].active && !a.st[r].overflow && a.st[r].steps_left > 0) s_any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    PersistCtl* c = a.pctl;
+    c->arrive = 0u;
+    c->more = 0;
+    cudaGraphSetConditional(h_loop, (s_any && c->budget > 0 && c->err == 0) ? 1u : 0u);
+  }
 }
 
 // IntegratorNVT::Integrate alone (forces already in f).  Particle p of the
