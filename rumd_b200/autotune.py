@@ -14,6 +14,8 @@ and, in a second stage at the winning shape, the kernel variants
                 warp per cell)
   sm_tiles      streamed mode: blocks claim tiles from their SM's region (1)
                 or one block per tile (0)
+  persistent    streamed mode, one block per tile: the steps between list
+                rebuilds in one cooperative kernel (1) or one launch per step (0)
 Each candidate is timed on the device (CUDA events around a short run of the
 real workload, after a warm-up run).  As in RUMD's test mode
 (Autotune.py:929-937), every candidate's potential energy after its run must
@@ -28,10 +30,11 @@ import os
 DEFAULT_PB = (32, 64, 128)
 DEFAULT_TP = (1, 2, 4, 8)
 DEFAULT_SKIN = (0.2, 0.3, 0.4, 0.5)
-VARIANT_KEYS = ("force_mode", "build_lanes", "sm_tiles")
-# kernel-variant candidates: (force_mode, sm_tiles) x build_lanes
-VARIANTS = tuple(dict(force_mode=fm, sm_tiles=st, build_lanes=bl)
-                 for (fm, st), bl in itertools.product(((0, 0), (0, 1), (1, 0), (2, 0)), (1, 2, 4, 8, 32)))
+VARIANT_KEYS = ("force_mode", "build_lanes", "sm_tiles", "persistent")
+# kernel-variant candidates: (force_mode, sm_tiles, persistent) x build_lanes
+VARIANTS = tuple(dict(force_mode=fm, sm_tiles=st, persistent=ps, build_lanes=bl)
+                 for (fm, st, ps), bl in itertools.product(((0, 0, 1), (0, 0, 0), (0, 1, 0), (1, 0, 0), (2, 0, 0)),
+                                                           (1, 2, 4, 8, 32)))
 
 
 def candidates(pbs=DEFAULT_PB, tps=DEFAULT_TP, skins=DEFAULT_SKIN, max_block=512):
@@ -81,7 +84,7 @@ def apply(engine, entry):
     from . import capi
     engine.set_launch(entry["pb"], entry["tp"])
     codes = {"force_mode": capi.VARIANT_FORCE_MODE, "build_lanes": capi.VARIANT_BUILD_LANES,
-             "sm_tiles": capi.VARIANT_SM_TILES}
+             "sm_tiles": capi.VARIANT_SM_TILES, "persistent": capi.VARIANT_PERSISTENT}
     for k, code in codes.items():
         if k in entry:
             engine.set_variant(code, entry[k])
@@ -147,8 +150,10 @@ def device_measure(capi, replicas, device=0, steps=300, warmup=100):
     replicas: list of dicts with pos4, vel4, box, params, ntypes, T, n, density."""
     import torch
 
-    def measure(pb, tp, skin, force_mode=None, build_lanes=None, sm_tiles=None):
+    def measure(pb, tp, skin, force_mode=None, build_lanes=None, sm_tiles=None, persistent=None):
         e = capi.Engine(device=device, max_replicas=len(replicas), pb=pb, tp=tp)
+        if persistent is not None:
+            e.set_variant(capi.VARIANT_PERSISTENT, persistent)
         if force_mode is not None:
             e.set_variant(capi.VARIANT_FORCE_MODE, force_mode)
         if build_lanes is not None:
@@ -199,7 +204,8 @@ def main(argv=None):
         print(f"pb={r['pb']:4d} tp={r['tp']} skin={r['skin']:.2f}  {r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
     for r in best.get("variant_table", []):
-        print(f"force_mode={r['force_mode']} sm_tiles={r['sm_tiles']} build_lanes={r['build_lanes']}  "
+        print(f"force_mode={r['force_mode']} sm_tiles={r['sm_tiles']} persistent={r['persistent']} "
+              f"build_lanes={r['build_lanes']}  "
               f"{r['rate']:.4e} particle-steps/s  "
               f"pe/N={r['pe']:.6f} {'ok' if r['ok'] else 'REJECTED'}")
     print(json.dumps({k: best[k] for k in ("pb", "tp", "skin", "rate") + VARIANT_KEYS if k in best}))

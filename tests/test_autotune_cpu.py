@@ -42,18 +42,19 @@ def test_cache_round_trip(tmp_path):
 def test_variant_stage_picks_fastest_and_is_cached(tmp_path):
     from rumd_b200 import autotune
 
-    def measure(pb, tp, skin, force_mode=None, build_lanes=None, sm_tiles=None):
+    def measure(pb, tp, skin, force_mode=None, build_lanes=None, sm_tiles=None, persistent=None):
         if force_mode is None:
             return float(pb * tp), -5.0
-        # streamed index loads and two build lanes fastest; staged with one lane breaks pe
-        rate = 1000.0 + (200.0 if force_mode == 0 else 0.0) - 10.0 * abs(build_lanes - 2)
+        # streamed index loads, the persistent kernel and two build lanes
+        # fastest; staged with one lane breaks pe
+        rate = 1000.0 + (200.0 if force_mode == 0 else 0.0) - 10.0 * abs(build_lanes - 2) + 5.0 * (persistent or 0)
         pe = -5.0 if (force_mode, build_lanes) != (1, 1) else -4.0
         return rate, pe
 
     reps = [{"n": 2000, "density": 1.2, "ntypes": 2}]
     at = autotune.Autotune(cache_path=str(tmp_path / "v.json"), pbs=(32, 64), tps=(1, 2), skins=(0.3,))
     r = at.tune(reps, measure, variants=True)
-    assert (r["force_mode"], r["build_lanes"]) == (0, 2)
+    assert (r["force_mode"], r["build_lanes"], r["persistent"]) == (0, 2, 1)
     assert len(r["variant_table"]) == len(autotune.VARIANTS)
     assert any(not v["ok"] for v in r["variant_table"])
     assert json.load(open(tmp_path / "v.json"))[autotune.signature(reps)]["build_lanes"] == 2
