@@ -277,18 +277,22 @@ def e2e_run(capi, device, pb, tp, pos4, vel4, im3, box, params, steps):
     n = len(pos4)
     t = time.perf_counter()
     rid = e.add(pos4, box, params, 2, cutoff="SF", skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU, vel4=vel4, im3=im3)
+    t_add = time.perf_counter()
     e.run(steps)
+    t_run = time.perf_counter()
     p = e.get(rid, "pos", n)
     v = e.get(rid, "vel", n)
     im = e.get(rid, "images", n)
     st = e.stats(rid)
-    dt = time.perf_counter() - t
+    t_end = time.perf_counter()
+    dt = t_end - t
     e.close()
     assert np.isfinite(p).all() and np.isfinite(st["pe"])
     h2d = n * (16 + 16 + 16 + 16 + 4)          # r, last_r, v, images, ids
     d2h = n * (3 * (16 + 4) + 4) + 256         # pos, vel, images (+ ids each), list lengths, state
     return {"value": n * steps / dt, "unit": "particle-steps/s",
-            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps}
+            "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
+            "phases_ms": {"add": 1e3 * (t_add - t), "run": 1e3 * (t_run - t_add), "read_back": 1e3 * (t_end - t_run)}}
 
 
 def batched(capi, device, pb, tp, steps, seed=0):

@@ -1892,7 +1892,12 @@ __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
         for (int v = max(off, ch); v < min(off + l0, ch + mc); ++v) wslot[v - ch] = b0 + (v - off);
         for (int v = max(off + l0, ch); v < min(off + len, ch + mc); ++v) wslot[v - ch] = b1 + (v - off - l0);
         __syncwarp();
-        for (int v = lane; v < mc; v += 32) wpos[v] = __ldg(rc + wslot[v]);
+        // the lane's position loads all in flight together
+#pragma unroll
+        for (int u = 0; u < kCwCand / 32; ++u) {
+          const int v = lane + 32 * u;
+          if (v < mc) wpos[v] = __ldg(rc + wslot[v]);
+        }
         __syncwarp();
         // two particles at a time: each staged candidate is read once and
         // tested against both (the second is a copy of the first when the
