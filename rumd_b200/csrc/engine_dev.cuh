@@ -108,8 +108,8 @@ struct PersistCtl {
   unsigned arrive;  // blocks arrived at the current grid barrier
   int go;           // the last barrier's decision: run another step
   int budget;       // steps this graph launch may still run (set by the host)
-  int more;         // replicas with steps left after the current step
   int err;          // a grid-barrier wait gave up (reported to the host)
+  unsigned long long tally;  // this step: rebuild requests << 32 | replicas with steps left
   unsigned smslot[kPersistMaxSm];  // blocks of this launch seen per SM id
   unsigned rank[kPersistMaxGrid];  // per block: slot on its SM * nsmid + SM id
 };

@@ -246,9 +246,14 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   if (left > 0) S->steps_left = left - 1;
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
-  if (ex > 0) atomicAdd(a.any_rebuild, 1);
-  // k_steps: replicas that still have steps after this one
-  if (a.persist && left > 1) atomicAdd(&a.pctl->more, 1);
+  if (a.persist) {
+    // k_steps: rebuild requests (high word) and replicas that still have
+    // steps after this one (low word), in one atomic
+    const unsigned long long t = (ex > 0 ? (1ull << 32) : 0ull) + (left > 1 ? 1ull : 0ull);
+    if (t) atomicAdd(&a.pctl->tally, t);
+  } else if (ex > 0) {
+    atomicAdd(a.any_rebuild, 1);
+  }
   // energies at run steps i with i % interval == 0, as Simulation.Run's
   // energies output schedule (Simulation.py:44, 587-589)
   if (R.energy_interval > 0 && (run_idx % R.energy_interval) == 0 && R.energy_cap > 0) {
@@ -930,7 +935,6 @@ __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditi
     __threadfence();
     c->arrive = 0u;
     for (unsigned k = 0; k < nsmid && k < (unsigned)kPersistMaxSm; ++k) c->smslot[k] = 0u;
-    __threadfence();
     st_release_u32(&c->gen, gen + 1u);
     return true;
   }
@@ -945,15 +949,14 @@ __device__ int step_barrier(const EngArgs& a, cudaGraphConditionalHandle h_loop)
   if (n == gridDim.x - 1) {
     __threadfence();
     c->arrive = 0u;
-    const int any = atomicExch(a.any_rebuild, 0);
-    const int more = atomicExch(&c->more, 0);
-    const int budget = c->budget - 1;
+    const unsigned long long t = atomicExch(&c->tally, 0ull);
+    const unsigned any = (unsigned)(t >> 32), more = (unsigned)(t & 0xffffffffu);
+    const int budget = __ldcg(&c->budget) - 1;
     c->budget = budget;
     const int go = any == 0 && more > 0 && budget > 0;
     c->go = go;
     if (!go) cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
-    __threadfence();
-    st_release_u32(&c->gen, gen + 1u);
+    st_release_u32(&c->gen, gen + 1u);  // orders the writes above before the release
     return go;
   }
   if (!barrier_wait(c, gen, h_loop)) return 0;
@@ -1030,7 +1033,7 @@ __global__ void k_gate_loop(EngArgs a, cudaGraphConditionalHandle h_loop) {
   if (threadIdx.x == 0) {
     PersistCtl* c = a.pctl;
     c->arrive = 0u;
-    c->more = 0;
+    c->tally = 0ull;
     cudaGraphSetConditional(h_loop, (s_any && c->budget > 0 && c->err == 0) ? 1u : 0u);
   }
 }
