@@ -862,7 +862,7 @@ void ensure_graphs(b2md_engine* e) {
   if (e->graphs_valid) return;
   invalidate_graphs(e);
   e->persist_on = false;
-  if (persist_mode(e) && e->ntiles > 0) {
+  if (persist_mode(e) && e->ntiles > 0 && e->reps.size() < (1u << 20)) {  // the barrier word's tally fields
     EngArgs a = make_args(e);
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)steps_fn(e->tp), e->pb * e->tp,

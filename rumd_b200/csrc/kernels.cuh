@@ -48,8 +48,17 @@ __device__ __forceinline__ void block_rows_sum(const double* base, int count, do
   const int nslot = blockDim.x / kNPart;
   const int k = threadIdx.x % kNPart, slot = threadIdx.x / kNPart;
   double acc = 0.0;
-  if (slot < nslot)
-    for (int t = slot; t < count; t += nslot) acc += __ldcg(base + (size_t)t * kNPart + k);
+  if (slot < nslot) {
+    // two rows' loads in flight at a time (the sum stays in row order)
+    int t = slot;
+    for (; t + nslot < count; t += 2 * nslot) {
+      const double x0 = __ldcg(base + (size_t)t * kNPart + k);
+      const double x1 = __ldcg(base + (size_t)(t + nslot) * kNPart + k);
+      acc += x0;
+      acc += x1;
+    }
+    if (t < count) acc += __ldcg(base + (size_t)t * kNPart + k);
+  }
   s_scr[threadIdx.x] = acc;
   __syncthreads();
   if (threadIdx.x < kNPart) {
@@ -58,6 +67,16 @@ __device__ __forceinline__ void block_rows_sum(const double* base, int count, do
     s_out[threadIdx.x] = s;
   }
   __syncthreads();
+}
+
+// atomicAdd with release (the block's earlier writes, ordered before by a
+// block barrier, are visible first) and acquire (the caller then sees the
+// writes the other blocks released) at GPU scope: one round trip where a
+// fence followed by an atomic took two.
+__device__ __forceinline__ unsigned atom_add_acq_rel(unsigned* p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
 }
 
 // Two-level deterministic replica reduction.  Every block of the replica
@@ -69,32 +88,24 @@ __device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int l
   const int g = lt / kGroup;
   const int gfirst = g * kGroup;
   const int gsize = min(kGroup, R.ntiles - gfirst);
-  if (threadIdx.x < kNPart) {
-    a.tpart[(size_t)(R.tile0 + lt) * kNPart + threadIdx.x] = s_blk[threadIdx.x];
-    __threadfence();
-  }
+  if (threadIdx.x < kNPart) a.tpart[(size_t)(R.tile0 + lt) * kNPart + threadIdx.x] = s_blk[threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned c = atomicAdd(&a.gctr[R.group0 + g], 1u);
+    unsigned c = atom_add_acq_rel(&a.gctr[R.group0 + g], 1u);
     s_last = (c == (unsigned)(gsize - 1));
   }
   __syncthreads();
   if (!s_last) return false;
-  __threadfence();
   block_rows_sum(a.tpart + (size_t)(R.tile0 + gfirst) * kNPart, gsize, s_scr, s_tot);
-  if (threadIdx.x < kNPart) {
-    a.gpart[(size_t)(R.group0 + g) * kNPart + threadIdx.x] = s_tot[threadIdx.x];
-    __threadfence();
-  }
+  if (threadIdx.x < kNPart) a.gpart[(size_t)(R.group0 + g) * kNPart + threadIdx.x] = s_tot[threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
     a.gctr[R.group0 + g] = 0u;
-    unsigned c = atomicAdd(&a.rctr[rep], 1u);
+    unsigned c = atom_add_acq_rel(&a.rctr[rep], 1u);
     s_last = (c == (unsigned)(R.ngroups - 1));
   }
   __syncthreads();
   if (!s_last) return false;
-  __threadfence();
   block_rows_sum(a.gpart + (size_t)R.group0 * kNPart, R.ngroups, s_scr, s_tot);
   if (threadIdx.x == 0) a.rctr[rep] = 0u;
   return true;
@@ -105,10 +116,8 @@ __device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int l
 // clears the SM-region tile counters (every block has made its last claim).
 __device__ __forceinline__ void grid_final(const EngArgs& a, int has_cond, cudaGraphConditionalHandle h) {
   if (threadIdx.x == 0) {
-    __threadfence();
-    unsigned c = atomicAdd(a.fctr, 1u);
+    unsigned c = atom_add_acq_rel(a.fctr, 1u);
     if (c == gridDim.x - 1) {
-      __threadfence();
       int any = atomicExch(a.any_rebuild, 0);
       *a.fctr = 0u;
       for (int k = 0; k <= a.nreg && a.nreg > 0; ++k) a.smctr[k] = 0u;
@@ -929,10 +938,8 @@ __device__ bool barrier_wait(PersistCtl* c, unsigned gen, cudaGraphConditionalHa
 __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
   const unsigned gen = ld_acquire_u32(&c->gen);
-  __threadfence();
-  const unsigned n = atomicAdd(&c->arrive, 1u);
+  const unsigned n = atom_add_acq_rel(&c->arrive, 1u);
   if (n == gridDim.x - 1) {
-    __threadfence();
     c->arrive = 0u;
     for (unsigned k = 0; k < nsmid && k < (unsigned)kPersistMaxSm; ++k) c->smslot[k] = 0u;
     st_release_u32(&c->gen, gen + 1u);
@@ -944,10 +951,8 @@ __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditi
 __device__ int step_barrier(const EngArgs& a, cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
   const unsigned gen = ld_acquire_u32(&c->gen);
-  __threadfence();
-  const unsigned n = atomicAdd(&c->arrive, 1u);
+  const unsigned n = atom_add_acq_rel(&c->arrive, 1u);
   if (n == gridDim.x - 1) {
-    __threadfence();
     c->arrive = 0u;
     const unsigned long long t = atomicExch(&c->tally, 0ull);
     const unsigned any = (unsigned)(t >> 32), more = (unsigned)(t & 0xffffffffu);
