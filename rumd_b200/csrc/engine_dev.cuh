@@ -104,12 +104,11 @@ struct RepState {
 constexpr int kPersistMaxSm = 1024;    // SM ids the tile order can use
 constexpr int kPersistMaxGrid = 8192;  // blocks the tile order can rank
 struct PersistCtl {
+  unsigned long long arrive;  // current grid barrier: blocks arrived, with the finalizers' tallies
   unsigned gen;     // grid-barrier generation
-  unsigned arrive;  // blocks arrived at the current grid barrier
   int go;           // the last barrier's decision: run another step
   int budget;       // steps this graph launch may still run (set by the host)
   int err;          // a grid-barrier wait gave up (reported to the host)
-  unsigned long long tally;  // this step: rebuild requests << 32 | replicas with steps left
   unsigned smslot[kPersistMaxSm];  // blocks of this launch seen per SM id
   unsigned rank[kPersistMaxGrid];  // per block: slot on its SM * nsmid + SM id
 };

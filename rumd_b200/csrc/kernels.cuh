@@ -222,6 +222,13 @@ __device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float
   exceed = d2 > R.skin2_4;
 }
 
+// k_steps: what this block's finalizer adds to its step-barrier arrival
+// (replicas that still have steps, rebuild requests); thread 0 only.
+__shared__ unsigned long long s_step_tally;
+constexpr int kTallyMoreShift = 24, kTallyRebuildShift = 44;
+constexpr unsigned long long kTallyArriveMask = (1ull << kTallyMoreShift) - 1ull;
+constexpr unsigned long long kTallyField = (1ull << 20) - 1ull;
+
 // Replica bookkeeping after an integration step (last block only).
 __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState* S, const double* tot,
                             bool with_forces) {
@@ -256,10 +263,7 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
   if (a.persist) {
-    // k_steps: rebuild requests (high word) and replicas that still have
-    // steps after this one (low word), in one atomic
-    const unsigned long long t = (ex > 0 ? (1ull << 32) : 0ull) + (left > 1 ? 1ull : 0ull);
-    if (t) atomicAdd(&a.pctl->tally, t);
+    s_step_tally += (ex > 0 ? (1ull << kTallyRebuildShift) : 0ull) + (left > 1 ? (1ull << kTallyMoreShift) : 0ull);
   } else if (ex > 0) {
     atomicAdd(a.any_rebuild, 1);
   }
@@ -915,6 +919,11 @@ __device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
 __device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long long* p, unsigned long long v) {
+  unsigned long long old;
+  asm volatile("atom.acq_rel.gpu.global.add.u64 %0, [%1], %2;" : "=l"(old) : "l"(p), "l"(v) : "memory");
+  return old;
+}
 
 // Waits (bounded) until the grid barrier of generation gen is released;
 // false when the wait gave up (recorded, and the graph's loop ended).
@@ -938,9 +947,9 @@ __device__ bool barrier_wait(PersistCtl* c, unsigned gen, cudaGraphConditionalHa
 __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
   const unsigned gen = ld_acquire_u32(&c->gen);
-  const unsigned n = atom_add_acq_rel(&c->arrive, 1u);
-  if (n == gridDim.x - 1) {
-    c->arrive = 0u;
+  const unsigned long long n = atom_add_acq_rel_u64(&c->arrive, 1ull) + 1ull;
+  if ((n & kTallyArriveMask) == gridDim.x) {
+    c->arrive = 0ull;
     for (unsigned k = 0; k < nsmid && k < (unsigned)kPersistMaxSm; ++k) c->smslot[k] = 0u;
     st_release_u32(&c->gen, gen + 1u);
     return true;
@@ -948,19 +957,26 @@ __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditi
   return barrier_wait(c, gen, h_loop);
 }
 
-__device__ int step_barrier(const EngArgs& a, cudaGraphConditionalHandle h_loop) {
+// The arrival word packs the blocks arrived (low 24 bits), the replicas that
+// still have steps (next 20) and the rebuild requests (top 20) that the
+// blocks' finalizers add with their arrival (s_step_tally), so the last block
+// learns everything from one atomic.  budget: the steps this launch may still
+// run after the current one, counted down by every block alike.
+__device__ int step_barrier(const EngArgs& a, int budget, cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
   const unsigned gen = ld_acquire_u32(&c->gen);
-  const unsigned n = atom_add_acq_rel(&c->arrive, 1u);
-  if (n == gridDim.x - 1) {
-    c->arrive = 0u;
-    const unsigned long long t = atomicExch(&c->tally, 0ull);
-    const unsigned any = (unsigned)(t >> 32), more = (unsigned)(t & 0xffffffffu);
-    const int budget = __ldcg(&c->budget) - 1;
-    c->budget = budget;
+  const unsigned long long mine = 1ull + s_step_tally;
+  const unsigned long long n = atom_add_acq_rel_u64(&c->arrive, mine) + mine;
+  if ((n & kTallyArriveMask) == gridDim.x) {
+    c->arrive = 0ull;
+    const unsigned more = (unsigned)((n >> kTallyMoreShift) & kTallyField);
+    const unsigned any = (unsigned)((n >> kTallyRebuildShift) & kTallyField);
     const int go = any == 0 && more > 0 && budget > 0;
     c->go = go;
-    if (!go) cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
+    if (!go) {
+      c->budget = budget;  // for the launch after the rebuild
+      cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
+    }
     st_release_u32(&c->gen, gen + 1u);  // orders the writes above before the release
     return go;
   }
@@ -1017,12 +1033,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     atomicAdd(&s_first, (int)below);
     __syncthreads();
   }
+  // the launch's step budget (written before the launch, or by the previous
+  // launch's last block), counted down by every block alike
+  int budget = __ldcg(&c->budget);
   while (s_go) {
+    if (threadIdx.x == 0) s_step_tally = 0ull;
     for (int tile = s_first; tile < a.ntiles; tile += gridDim.x) {
       force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows);
       __syncthreads();  // the next tile reloads the pair table
     }
-    if (threadIdx.x == 0) s_go = step_barrier(a, h_loop);
+    budget -= 1;
+    if (threadIdx.x == 0) s_go = step_barrier(a, budget, h_loop);
     __syncthreads();
   }
 }
@@ -1037,8 +1058,7 @@ __global__ void k_gate_loop(EngArgs a, cudaGraphConditionalHandle h_loop) {
   __syncthreads();
   if (threadIdx.x == 0) {
     PersistCtl* c = a.pctl;
-    c->arrive = 0u;
-    c->tally = 0ull;
+    c->arrive = 0ull;
     cudaGraphSetConditional(h_loop, (s_any && c->budget > 0 && c->err == 0) ? 1u : 0u);
   }
 }
