@@ -104,9 +104,9 @@ struct RepState {
 constexpr int kPersistMaxSm = 1024;    // SM ids the tile order can use
 constexpr int kPersistMaxGrid = 8192;  // blocks the tile order can rank
 struct PersistCtl {
-  unsigned long long arrive;  // current grid barrier: blocks arrived, with the finalizers' tallies
+  unsigned long long arrive;  // setup barrier: blocks arrived
+  unsigned long long word[2];  // step barriers (alternating): arrivals and the finalizers' tallies
   unsigned gen;     // grid-barrier generation
-  int go;           // the last barrier's decision: run another step
   int budget;       // steps this graph launch may still run (set by the host)
   int err;          // a grid-barrier wait gave up (reported to the host)
   unsigned smslot[kPersistMaxSm];  // blocks of this launch seen per SM id

@@ -942,14 +942,16 @@ __device__ bool barrier_wait(PersistCtl* c, unsigned gen, cudaGraphConditionalHa
 }
 
 // Grid barrier at the start of k_steps, after every block has entered its
-// rank; the last block to arrive clears the per-SM counters for the next
-// launch.
+// rank; the last block to arrive zeroes the step-barrier words and clears
+// the per-SM counters for the next launch before it releases the others.
 __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
   const unsigned gen = ld_acquire_u32(&c->gen);
   const unsigned long long n = atom_add_acq_rel_u64(&c->arrive, 1ull) + 1ull;
   if ((n & kTallyArriveMask) == gridDim.x) {
     c->arrive = 0ull;
+    c->word[0] = 0ull;
+    c->word[1] = 0ull;
     for (unsigned k = 0; k < nsmid && k < (unsigned)kPersistMaxSm; ++k) c->smslot[k] = 0u;
     st_release_u32(&c->gen, gen + 1u);
     return true;
@@ -957,31 +959,60 @@ __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditi
   return barrier_wait(c, gen, h_loop);
 }
 
-// The arrival word packs the blocks arrived (low 24 bits), the replicas that
-// still have steps (next 20) and the rebuild requests (top 20) that the
-// blocks' finalizers add with their arrival (s_step_tally), so the last block
-// learns everything from one atomic.  budget: the steps this launch may still
-// run after the current one, counted down by every block alike.
-__device__ int step_barrier(const EngArgs& a, int budget, cudaGraphConditionalHandle h_loop) {
+// The step barrier needs no release step.  Steps alternate between two
+// words (step s uses word[s & 1]); each word only grows during a launch (the
+// setup barrier zeroes both).  A block adds, in one release/acquire atomic,
+// its arrival (low 24 bits) and its finalizer's tallies (s_step_tally:
+// replicas that still have steps, next 20 bits; rebuild requests, top 20),
+// then polls the word until the step's arrivals are complete.  Nothing else
+// can reach that word before every block has left this barrier (the next
+// contributions to it come two steps later), so every block reads the same
+// totals and takes the same decision: go on unless a rebuild is due, the
+// budget (counted down by every block alike) is spent, no replica has steps
+// left, or the launch has run kMaxLaunchSteps steps (the words' fields would
+// otherwise carry).  The block whose arrival completed the step sets the
+// graph's loop condition and, when stopping, the budget of the next launch.
+// seen[w]: the totals of word w at its previous barrier.
+constexpr int kMaxLaunchSteps = 4096;
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ int step_barrier(const EngArgs& a, int step, int budget, unsigned long long* seen,
+                            cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
-  const unsigned gen = ld_acquire_u32(&c->gen);
+  const int w = step & 1;
+  const unsigned long long base = seen[w];
   const unsigned long long mine = 1ull + s_step_tally;
-  const unsigned long long n = atom_add_acq_rel_u64(&c->arrive, mine) + mine;
-  if ((n & kTallyArriveMask) == gridDim.x) {
-    c->arrive = 0ull;
-    const unsigned more = (unsigned)((n >> kTallyMoreShift) & kTallyField);
-    const unsigned any = (unsigned)((n >> kTallyRebuildShift) & kTallyField);
-    const int go = any == 0 && more > 0 && budget > 0;
-    c->go = go;
-    if (!go) {
-      c->budget = budget;  // for the launch after the rebuild
-      cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
+  const unsigned long long old = atom_add_acq_rel_u64(&c->word[w], mine);
+  const bool last = ((old + mine - base) & kTallyArriveMask) == gridDim.x;
+  unsigned long long now = old + mine;
+  if (!last) {
+    for (unsigned it = 0;; ++it) {
+      now = ld_acquire_u64(&c->word[w]);
+      if (((now - base) & kTallyArriveMask) == gridDim.x) break;
+      if (it >= kBarrierPolls) {
+        atomicExch(&c->err, 1);
+        cudaGraphSetConditional(h_loop, 0u);
+        return 0;
+      }
+      __nanosleep(32);
     }
-    st_release_u32(&c->gen, gen + 1u);  // orders the writes above before the release
-    return go;
   }
-  if (!barrier_wait(c, gen, h_loop)) return 0;
-  return __ldcg(&c->go);
+  seen[w] = now;
+  const unsigned long long d = now - base;
+  const unsigned more = (unsigned)((d >> kTallyMoreShift) & kTallyField);
+  const unsigned any = (unsigned)((d >> kTallyRebuildShift) & kTallyField);
+  const int cap = min(kMaxLaunchSteps, (int)(kTallyField / (unsigned)(a.nrep + 1)));
+  const int go = any == 0 && more > 0 && budget > 0 && step + 1 < cap;
+  if (last && !go) {
+    c->budget = budget;  // for the launch after the rebuild
+    cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
+  }
+  return go;
 }
 
 // Many fused steps in one cooperative launch (every block resident): each
@@ -1012,15 +1043,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     s_go = __ldcg(&c->err) == 0;
     if (!s_go && blockIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
     s_first = ranked ? 0 : (int)blockIdx.x;
-    if (s_go && ranked) {
+    if (s_go) {
       unsigned smid, nsmid;
       asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
       asm volatile("mov.u32 %0, %%nsmid;" : "=r"(nsmid));
-      // ranks are unique: (slot, SM id) pairs, or 2^31 + block index
-      const unsigned r = smid < (unsigned)kPersistMaxSm ? atomicAdd(&c->smslot[smid], 1u) * nsmid + smid
-                                                        : 0x80000000u + blockIdx.x;
-      s_rank = r;
-      c->rank[blockIdx.x] = r;
+      if (ranked) {
+        // ranks are unique: (slot, SM id) pairs, or 2^31 + block index
+        const unsigned r = smid < (unsigned)kPersistMaxSm ? atomicAdd(&c->smslot[smid], 1u) * nsmid + smid
+                                                          : 0x80000000u + blockIdx.x;
+        s_rank = r;
+        c->rank[blockIdx.x] = r;
+      }
       s_go = setup_barrier(a, nsmid, h_loop);
     }
   }
@@ -1036,14 +1069,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
   // the launch's step budget (written before the launch, or by the previous
   // launch's last block), counted down by every block alike
   int budget = __ldcg(&c->budget);
-  while (s_go) {
+  unsigned long long seen[2] = {0ull, 0ull};  // thread 0: the step words' totals so far
+  for (int step = 0; s_go; ++step) {
     if (threadIdx.x == 0) s_step_tally = 0ull;
     for (int tile = s_first; tile < a.ntiles; tile += gridDim.x) {
       force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows);
       __syncthreads();  // the next tile reloads the pair table
     }
     budget -= 1;
-    if (threadIdx.x == 0) s_go = step_barrier(a, budget, h_loop);
+    if (threadIdx.x == 0) s_go = step_barrier(a, step, budget, seen, h_loop);
     __syncthreads();
   }
 }
