@@ -288,7 +288,7 @@ EngArgs make_args(b2md_engine* e) {
   a.ntiles = e->ntiles;
   a.nrep = (int)e->reps.size();
   a.pctl = e->pctl;
-  a.persist = 0;
+  a.gpart_half = (long long)e->gcap * kNPart;
 
   // staged list tile (force mode 1): pb slots per block of 8 entries
   a.idx_pitch = e->pb;
@@ -365,7 +365,7 @@ void relayout(b2md_engine* e) {
   }
   if (G > e->gcap) {
     int nc = std::max(G, e->gcap * 2);
-    dev_grow(e, e->gpart, (long long)e->gcap * kNPart, (long long)nc * kNPart, true);
+    dev_grow(e, e->gpart, 2LL * e->gcap * kNPart, 2LL * nc * kNPart, false);  // two halves
     dev_grow(e, e->gctr, e->gcap, nc, true);
     e->gcap = nc;
   }
@@ -783,7 +783,6 @@ int steps_grid(const b2md_engine* e, StepsFn fn, size_t smem) {
 // conditional node and a kernel launch.
 void build_persist_graph(b2md_engine* e) {
   EngArgs a = make_args(e);
-  a.persist = 1;
   const size_t smem = force_smem(e, a);
   force_fn(e, true, false, a);  // checks the shared-memory need
   StepsFn fs = steps_fn(e->tp);

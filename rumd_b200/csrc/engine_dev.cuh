@@ -149,7 +149,7 @@ struct EngArgs {
   int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
   int max_types;  // largest type count over the active replicas (pair-table rows in shared memory)
   PersistCtl* pctl;  // k_steps control block
-  int persist;       // 1 in the persistent step graph: finish_step counts replicas with steps left
+  long long gpart_half;  // gpart holds two halves (k_steps alternates them by step parity)
   unsigned short* wl;  // window list (force mode 2)
   int4* wseg;          // per-tile window segments
   int2* wmeta;         // per-tile (segments, particles)

@@ -111,6 +111,39 @@ __device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int l
   return true;
 }
 
+// The group level of replica_reduce for k_steps, whose replica level runs
+// after the block's step-barrier arrival (so the next step's group totals go
+// to the other half of the double-buffered gpart, gpar = step parity).
+// Returns true in the block that must finish the replica (the last group's
+// last block); it has already reset the replica counter for the next step.
+__device__ bool group_reduce(const EngArgs& a, int rep, const RepDev& R, int lt, const double* s_blk,
+                             double* s_scr, double* s_tot, int gpar) {
+  __shared__ int s_last;
+  const int g = lt / kGroup;
+  const int gfirst = g * kGroup;
+  const int gsize = min(kGroup, R.ntiles - gfirst);
+  double* gpart = a.gpart + (size_t)gpar * a.gpart_half;
+  if (threadIdx.x < kNPart) a.tpart[(size_t)(R.tile0 + lt) * kNPart + threadIdx.x] = s_blk[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned c = atom_add_acq_rel(&a.gctr[R.group0 + g], 1u);
+    s_last = (c == (unsigned)(gsize - 1));
+  }
+  __syncthreads();
+  if (!s_last) return false;
+  block_rows_sum(a.tpart + (size_t)(R.tile0 + gfirst) * kNPart, gsize, s_scr, s_tot);
+  if (threadIdx.x < kNPart) gpart[(size_t)(R.group0 + g) * kNPart + threadIdx.x] = s_tot[threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a.gctr[R.group0 + g] = 0u;
+    unsigned c = atom_add_acq_rel(&a.rctr[rep], 1u);
+    s_last = (c == (unsigned)(R.ngroups - 1));
+    if (s_last) a.rctr[rep] = 0u;
+  }
+  __syncthreads();
+  return s_last != 0;
+}
+
 // Last block of the whole grid: publishes "any replica needs a rebuild" to
 // the next conditional graph node (or nothing when launched eagerly), and
 // clears the SM-region tile counters (every block has made its last claim).
@@ -222,8 +255,8 @@ __device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float
   exceed = d2 > R.skin2_4;
 }
 
-// k_steps: what this block's finalizer adds to its step-barrier arrival
-// (replicas that still have steps, rebuild requests); thread 0 only.
+// k_steps: what this block adds to its step-barrier arrival (its replica
+// still has steps, its tile asks for a rebuild); thread 0 only.
 __shared__ unsigned long long s_step_tally;
 constexpr int kTallyMoreShift = 24, kTallyRebuildShift = 44;
 constexpr unsigned long long kTallyArriveMask = (1ull << kTallyMoreShift) - 1ull;
@@ -262,11 +295,7 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   if (left > 0) S->steps_left = left - 1;
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
-  if (a.persist) {
-    s_step_tally += (ex > 0 ? (1ull << kTallyRebuildShift) : 0ull) + (left > 1 ? (1ull << kTallyMoreShift) : 0ull);
-  } else if (ex > 0) {
-    atomicAdd(a.any_rebuild, 1);
-  }
+  if (ex > 0) atomicAdd(a.any_rebuild, 1);
   // energies at run steps i with i % interval == 0, as Simulation.Run's
   // energies output schedule (Simulation.py:44, 587-589)
   if (R.energy_interval > 0 && (run_idx % R.energy_interval) == 0 && R.energy_cap > 0) {
@@ -275,6 +304,53 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
     e[0] = (double)run_idx; e[1] = pe; e[2] = vir; e[3] = tot[P_KET]; e[4] = xi;
     S->nlog = nlog + 1;
   }
+}
+
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// finish_step for k_steps, run by the replica's finalizer after its
+// step-barrier arrival: the same updates, except that the rebuild flag is
+// raised by the blocks themselves (and cleared by the list build) and the
+// loop tallies go with the arrivals.  The step count is stored last, with
+// release: the next step's blocks wait for it before they integrate.
+__device__ void finish_step_persist(const EngArgs& a, const RepDev& R, RepState* S, const double* tot) {
+  if (threadIdx.x != 0) return;
+  const double T0 = __ldcg(&S->T), dT = __ldcg(&S->dT), xi0 = __ldcg(&S->xi);
+  const long long run_idx = __ldcg(&S->run_step);
+  const long long steps = __ldcg(&S->steps), left = __ldcg(&S->steps_left);
+  const int rbuf = __ldcg(&S->rbuf), nlog = __ldcg(&S->nlog);
+  double xi = xi0, T = T0;
+  if (R.thermo_mask) {
+    double dev = tot[P_KE2] / (R.dof * T0) - 1.0;
+    if (dev > 10.0) dev = 10.0;  // updateNVTThermostatState (IntegratorNVT.cu:426-437)
+    xi = xi0 + (double)R.dt * (double)R.omega2 * dev;
+    T = T0 + dT;
+  }
+  S->xi = xi;
+  S->T = T;
+  S->ke2 = tot[P_KE2];
+  S->ke_t = tot[P_KET];
+  const double pe = tot[P_PE], vir = tot[P_W] / 6.0;
+  S->pe = pe;
+  S->vir = vir;
+  S->P[0] = tot[P_PX]; S->P[1] = tot[P_PY]; S->P[2] = tot[P_PZ]; S->M = tot[P_M];
+  S->rbuf = rbuf ^ 1;
+  S->run_step = run_idx + 1;
+  if (left > 0) S->steps_left = left - 1;
+  if (R.energy_interval > 0 && (run_idx % R.energy_interval) == 0 && R.energy_cap > 0) {
+    int k = nlog % R.energy_cap;
+    double* e = a.elog + (size_t)(R.elog0 + k) * 5;
+    e[0] = (double)run_idx; e[1] = pe; e[2] = vir; e[3] = tot[P_KET]; e[4] = xi;
+    S->nlog = nlog + 1;
+  }
+  st_release_u64(reinterpret_cast<unsigned long long*>(&S->steps), (unsigned long long)(steps + 1));
 }
 
 // ---------------------------------------------------------------------------
@@ -649,7 +725,7 @@ enum { FM_STREAMED = 0, FM_STAGED = 1, FM_WINDOW = 2 };
 // per tile and the block shares them through shared memory.
 struct StepView {
   int overflow, rbuf, abuf, pad_;
-  long long steps_left, run_step;
+  long long steps_left, run_step, steps;
   double M, P[3], xi;
 };
 
@@ -659,6 +735,7 @@ __device__ __forceinline__ void load_view(StepView& v, const RepState* S) {
   v.abuf = __ldcg(&S->abuf);
   v.steps_left = __ldcg(&S->steps_left);
   v.run_step = __ldcg(&S->run_step);
+  v.steps = __ldcg(&S->steps);
   v.M = __ldcg(&S->M);
   v.P[0] = __ldcg(&S->P[0]);
   v.P[1] = __ldcg(&S->P[1]);
@@ -667,8 +744,9 @@ __device__ __forceinline__ void load_view(StepView& v, const RepState* S) {
 }
 
 template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
-__device__ __forceinline__ void force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
-                                           double* s_tot, uint64_t& s_bar, unsigned& s_rows) {
+__device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
+                                           double* s_tot, uint64_t& s_bar, unsigned& s_rows,
+                                           const StepView* pv = nullptr, int gpar = 0, int* s_fin = nullptr) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -680,12 +758,11 @@ __device__ __forceinline__ void force_tile(const EngArgs& a, int tile, unsigned 
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
-  __shared__ StepView s_view;
-  if constexpr (PERSIST) {
-    if (threadIdx.x == 0) load_view(s_view, S);
-    __syncthreads();
-  }
-#define SV(f) (PERSIST ? s_view.f : S->f)
+  // PERSIST: the block's view of its replica's state, kept by k_steps
+  // (the buffer parity, step counters); xi and the momentum come from the
+  // previous step's finalizer just before the integration
+  __shared__ double s_xi, s_M, s_P[3];
+#define SV(f) (PERSIST ? pv->f : S->f)
   const bool skip = (SV(overflow) != 0) || (FUSED && SV(steps_left) <= 0) || !R.active;
   if (!skip) {
     const int pb = blockDim.x / TP;
@@ -816,6 +893,27 @@ __device__ __forceinline__ void force_tile(const EngArgs& a, int tile, unsigned 
         }
       }
     }
+    if constexpr (PERSIST && FUSED) {
+      // wait (bounded) for the previous step's finalizer: it stores the step
+      // count last, with release
+      if (threadIdx.x == 0) {
+        const unsigned long long want = (unsigned long long)pv->steps;
+        for (unsigned it = 0; ld_acquire_u64(reinterpret_cast<const unsigned long long*>(&S->steps)) < want; ++it) {
+          if (it >= kWaitPolls) {
+            atomicExch(&a.pctl->err, 1);
+            break;
+          }
+          __nanosleep(32);
+        }
+        s_xi = __ldcg(&S->xi);
+        s_M = __ldcg(&S->M);
+        s_P[0] = __ldcg(&S->P[0]);
+        s_P[1] = __ldcg(&S->P[1]);
+        s_P[2] = __ldcg(&S->P[2]);
+      }
+      __syncthreads();
+    }
+#define SVS(f, pf) (PERSIST ? (pf) : S->f)
     double acc[kNPart];
 #pragma unroll
     for (int k = 0; k < kNPart; ++k) acc[k] = 0.0;
@@ -834,11 +932,12 @@ __device__ __forceinline__ void force_tile(const EngArgs& a, int tile, unsigned 
         int4 im = a.im[ab][gi];
         const bool do_reset = R.reset_interval > 0 && (SV(run_step) % R.reset_interval) == 0;
         float3 vs = make_float3(0.f, 0.f, 0.f);
-        const double M = SV(M);
+        const double M = SVS(M, s_M);
         if (do_reset && M > 0.0)
-          vs = make_float3((float)(SV(P[0]) / M), (float)(SV(P[1]) / M), (float)(SV(P[2]) / M));
+          vs = make_float3((float)(SVS(P[0], s_P[0]) / M), (float)(SVS(P[1], s_P[1]) / M),
+                           (float)(SVS(P[2], s_P[2]) / M));
         float4 rn;
-        integrate_one(R, (float)SV(xi), vs, do_reset, ri, fo, v, im, rn, acc, exceed, a.last_r[gi]);
+        integrate_one(R, (float)SVS(xi, s_xi), vs, do_reset, ri, fo, v, im, rn, acc, exceed, a.last_r[gi]);
         a.v[ab][gi] = v;
         a.im[ab][gi] = im;
         a.r[rb ^ 1][gi] = rn;
@@ -847,18 +946,32 @@ __device__ __forceinline__ void force_tile(const EngArgs& a, int tile, unsigned 
     // every thread is past the neighbour loop: the pair table (and the staged
     // tile) may be overwritten by the reduction scratch
     const int ex = __syncthreads_or(exceed);
-    if (FUSED && ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
-    block_sum8(acc, s_warp, s_blk);
-    if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
-      if (FUSED) {
-        finish_step(a, rep, R, S, s_tot, true);
-      } else if (threadIdx.x == 0) {
-        S->pe = s_tot[P_PE];
-        S->vir = s_tot[P_W] / 6.0;
+    if constexpr (PERSIST) {
+      // the rebuild request and "steps left" go with the block's arrival
+      if (threadIdx.x == 0) {
+        if (ex) S->rebuild = 1;
+        s_step_tally += (ex ? (1ull << kTallyRebuildShift) : 0ull) +
+                        (pv->steps_left > 1 ? (1ull << kTallyMoreShift) : 0ull);
+      }
+      block_sum8(acc, s_warp, s_blk);
+      const bool fin = group_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot, gpar);
+      if (threadIdx.x == 0 && fin) *s_fin = rep;
+    } else {
+      if (FUSED && ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
+      block_sum8(acc, s_warp, s_blk);
+      if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
+        if (FUSED) {
+          finish_step(a, rep, R, S, s_tot, true);
+        } else if (threadIdx.x == 0) {
+          S->pe = s_tot[P_PE];
+          S->vir = s_tot[P_W] / 6.0;
+        }
       }
     }
+#undef SVS
   }
 #undef SV
+  return !skip;
 }
 
 // One tile of pb particles per block, tp threads per particle.  MODE selects
@@ -975,21 +1088,17 @@ __device__ bool setup_barrier(const EngArgs& a, unsigned nsmid, cudaGraphConditi
 // seen[w]: the totals of word w at its previous barrier.
 constexpr int kMaxLaunchSteps = 4096;
 
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-  unsigned long long v;
-  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-  return v;
+__device__ unsigned long long step_arrive(const EngArgs& a, int step) {
+  const unsigned long long mine = 1ull + s_step_tally;
+  return atom_add_acq_rel_u64(&a.pctl->word[step & 1], mine) + mine;
 }
 
-__device__ int step_barrier(const EngArgs& a, int step, int budget, unsigned long long* seen,
-                            cudaGraphConditionalHandle h_loop) {
+__device__ int step_decide(const EngArgs& a, int step, int budget, unsigned long long* seen, unsigned long long now,
+                           cudaGraphConditionalHandle h_loop) {
   PersistCtl* c = a.pctl;
   const int w = step & 1;
   const unsigned long long base = seen[w];
-  const unsigned long long mine = 1ull + s_step_tally;
-  const unsigned long long old = atom_add_acq_rel_u64(&c->word[w], mine);
-  const bool last = ((old + mine - base) & kTallyArriveMask) == gridDim.x;
-  unsigned long long now = old + mine;
+  const bool last = ((now - base) & kTallyArriveMask) == gridDim.x;
   if (!last) {
     for (unsigned it = 0;; ++it) {
       now = ld_acquire_u64(&c->word[w]);
@@ -1070,14 +1179,46 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
   // launch's last block), counted down by every block alike
   int budget = __ldcg(&c->budget);
   unsigned long long seen[2] = {0ull, 0ull};  // thread 0: the step words' totals so far
+  // one tile per block (the engine uses k_steps only when every tile has a
+  // resident block); the block's view of its replica's state
+  __shared__ StepView s_view;
+  __shared__ int s_fin;
+  const int tile = s_first;
+  const bool has_tile = tile < a.ntiles;
+  if (threadIdx.x == 0 && has_tile) load_view(s_view, a.st + a.tile_rep[tile]);
+  __syncthreads();
   for (int step = 0; s_go; ++step) {
-    if (threadIdx.x == 0) s_step_tally = 0ull;
-    for (int tile = s_first; tile < a.ntiles; tile += gridDim.x) {
-      force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows);
-      __syncthreads();  // the next tile reloads the pair table
+    if (threadIdx.x == 0) {
+      s_step_tally = 0ull;
+      s_fin = -1;
     }
+    __syncthreads();
+    bool stepped = false;
+    if (has_tile)
+      stepped = force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, &s_view,
+                                                               step & 1, &s_fin);
     budget -= 1;
-    if (threadIdx.x == 0) s_go = step_barrier(a, step, budget, seen, h_loop);
+    unsigned long long now = 0ull;
+    if (threadIdx.x == 0) now = step_arrive(a, step);
+    __syncthreads();
+    // the replica's finalizer: replica totals and state update, between its
+    // arrival and the barrier's completion
+    const int fr = s_fin;
+    if (fr >= 0) {
+      const RepDev& R = a.rep[fr];
+      block_rows_sum(a.gpart + (size_t)(step & 1) * a.gpart_half + (size_t)R.group0 * kNPart, R.ngroups,
+                     reinterpret_cast<double*>(s_dyn) + (blockDim.x >> 5) * kNPart, s_tot);
+      finish_step_persist(a, R, a.st + fr, s_tot);
+    }
+    if (threadIdx.x == 0) {
+      s_go = step_decide(a, step, budget, seen, now, h_loop);
+      if (stepped) {
+        s_view.rbuf ^= 1;
+        if (s_view.steps_left > 0) s_view.steps_left -= 1;
+        s_view.run_step += 1;
+        s_view.steps += 1;
+      }
+    }
     __syncthreads();
   }
 }
