@@ -272,7 +272,7 @@ void grow_reps(b2md_engine* e, int need) {
   int nc = std::max(need, std::max(e->rcap * 2, 8));
   dev_grow(e, e->rep, e->rcap, nc, true);
   dev_grow(e, e->st, e->rcap, nc, true);
-  dev_grow(e, e->rctr, e->rcap, nc, true);
+  dev_grow(e, e->rctr, 2LL * e->rcap, 2LL * nc, true);  // two halves (k_steps: by step parity)
   e->rcap = nc;
   invalidate_graphs(e);
 }
@@ -289,6 +289,9 @@ EngArgs make_args(b2md_engine* e) {
   a.nrep = (int)e->reps.size();
   a.pctl = e->pctl;
   a.gpart_half = (long long)e->gcap * kNPart;
+  a.tpart_half = (long long)e->tcap * kNPart;
+  a.gctr_half = e->gcap;
+  a.rctr_half = e->rcap;
 
   // staged list tile (force mode 1): pb slots per block of 8 entries
   a.idx_pitch = e->pb;
@@ -358,7 +361,7 @@ void relayout(b2md_engine* e) {
     dev_grow(e, e->tile_first, e->tcap, nc, true);
     dev_grow(e, e->ctot, e->tcap, nc, true);
     dev_grow(e, e->cpref, e->tcap, nc, true);
-    dev_grow(e, e->tpart, (long long)e->tcap * kNPart, (long long)nc * kNPart, true);
+    dev_grow(e, e->tpart, 2LL * e->tcap * kNPart, 2LL * nc * kNPart, false);  // two halves
     dev_grow(e, e->wseg, (long long)e->tcap * kWinSeg, (long long)nc * kWinSeg, false);
     dev_grow(e, e->wmeta, e->tcap, nc, false);
     e->tcap = nc;
@@ -366,7 +369,7 @@ void relayout(b2md_engine* e) {
   if (G > e->gcap) {
     int nc = std::max(G, e->gcap * 2);
     dev_grow(e, e->gpart, 2LL * e->gcap * kNPart, 2LL * nc * kNPart, false);  // two halves
-    dev_grow(e, e->gctr, e->gcap, nc, true);
+    dev_grow(e, e->gctr, 2LL * e->gcap, 2LL * nc, true);  // two halves
     e->gcap = nc;
   }
   std::vector<int> trep(T), tfirst(T);

@@ -149,7 +149,10 @@ struct EngArgs {
   int idx_rows;   // k_force: rows of the staged list tile (max list capacity over replicas)
   int max_types;  // largest type count over the active replicas (pair-table rows in shared memory)
   PersistCtl* pctl;  // k_steps control block
-  long long gpart_half;  // gpart holds two halves (k_steps alternates them by step parity)
+  // tpart, gpart, gctr and rctr hold two halves each: k_steps alternates
+  // them by step parity (the other kernels use the first)
+  long long gpart_half, tpart_half;
+  int gctr_half, rctr_half;
   unsigned short* wl;  // window list (force mode 2)
   int4* wseg;          // per-tile window segments
   int2* wmeta;         // per-tile (segments, particles)

@@ -111,37 +111,43 @@ __device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int l
   return true;
 }
 
-// The group level of replica_reduce for k_steps, whose replica level runs
-// after the block's step-barrier arrival (so the next step's group totals go
-// to the other half of the double-buffered gpart, gpar = step parity).
-// Returns true in the block that must finish the replica (the last group's
-// last block); it has already reset the replica counter for the next step.
-__device__ bool group_reduce(const EngArgs& a, int rep, const RepDev& R, int lt, const double* s_blk,
-                             double* s_scr, double* s_tot, int gpar) {
+// The replica reduction of k_steps, run by every block after its step-barrier
+// arrival, on the step's half (par) of the partial-sum and counter buffers:
+// the tile's group counter, then (last block of the group) the group total
+// and the replica counter.  Returns true in the replica's last block, which
+// then sums the group totals and finishes the step; the other blocks have
+// gone on to the next step and wait for that only before they integrate.
+__device__ bool post_reduce(const EngArgs& a, int tile, int par, double* s_scr, double* s_tot) {
   __shared__ int s_last;
+  const int rep = a.tile_rep[tile];
+  const RepDev& R = a.rep[rep];
+  const int lt = tile - R.tile0;
   const int g = lt / kGroup;
   const int gfirst = g * kGroup;
   const int gsize = min(kGroup, R.ntiles - gfirst);
-  double* gpart = a.gpart + (size_t)gpar * a.gpart_half;
-  if (threadIdx.x < kNPart) a.tpart[(size_t)(R.tile0 + lt) * kNPart + threadIdx.x] = s_blk[threadIdx.x];
-  __syncthreads();
+  unsigned* gctr = a.gctr + (size_t)par * a.gctr_half;
+  unsigned* rctr = a.rctr + (size_t)par * a.rctr_half;
+  double* gpart = a.gpart + (size_t)par * a.gpart_half;
+  const double* tpart = a.tpart + (size_t)par * a.tpart_half;
   if (threadIdx.x == 0) {
-    unsigned c = atom_add_acq_rel(&a.gctr[R.group0 + g], 1u);
+    unsigned c = atom_add_acq_rel(&gctr[R.group0 + g], 1u);
     s_last = (c == (unsigned)(gsize - 1));
   }
   __syncthreads();
   if (!s_last) return false;
-  block_rows_sum(a.tpart + (size_t)(R.tile0 + gfirst) * kNPart, gsize, s_scr, s_tot);
+  block_rows_sum(tpart + (size_t)(R.tile0 + gfirst) * kNPart, gsize, s_scr, s_tot);
   if (threadIdx.x < kNPart) gpart[(size_t)(R.group0 + g) * kNPart + threadIdx.x] = s_tot[threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
-    a.gctr[R.group0 + g] = 0u;
-    unsigned c = atom_add_acq_rel(&a.rctr[rep], 1u);
+    gctr[R.group0 + g] = 0u;
+    unsigned c = atom_add_acq_rel(&rctr[rep], 1u);
     s_last = (c == (unsigned)(R.ngroups - 1));
-    if (s_last) a.rctr[rep] = 0u;
+    if (s_last) rctr[rep] = 0u;
   }
   __syncthreads();
-  return s_last != 0;
+  if (!s_last) return false;
+  block_rows_sum(gpart + (size_t)R.group0 * kNPart, R.ngroups, s_scr, s_tot);
+  return true;
 }
 
 // Last block of the whole grid: publishes "any replica needs a rebuild" to
@@ -746,7 +752,7 @@ __device__ __forceinline__ void load_view(StepView& v, const RepState* S) {
 template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
 __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
                                            double* s_tot, uint64_t& s_bar, unsigned& s_rows,
-                                           const StepView* pv = nullptr, int gpar = 0, int* s_fin = nullptr) {
+                                           const StepView* pv = nullptr, int gpar = 0) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -953,9 +959,11 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
         s_step_tally += (ex ? (1ull << kTallyRebuildShift) : 0ull) +
                         (pv->steps_left > 1 ? (1ull << kTallyMoreShift) : 0ull);
       }
+      // the tile's partial sums; k_steps reduces them after the block's
+      // barrier arrival (the arrival releases them)
       block_sum8(acc, s_warp, s_blk);
-      const bool fin = group_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot, gpar);
-      if (threadIdx.x == 0 && fin) *s_fin = rep;
+      if (threadIdx.x < kNPart)
+        a.tpart[(size_t)gpar * a.tpart_half + (size_t)tile * kNPart + threadIdx.x] = s_blk[threadIdx.x];
     } else {
       if (FUSED && ex && threadIdx.x == 0) atomicAdd(&S->exceed, 1);
       block_sum8(acc, s_warp, s_blk);
@@ -1182,33 +1190,27 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
   // one tile per block (the engine uses k_steps only when every tile has a
   // resident block); the block's view of its replica's state
   __shared__ StepView s_view;
-  __shared__ int s_fin;
   const int tile = s_first;
   const bool has_tile = tile < a.ntiles;
   if (threadIdx.x == 0 && has_tile) load_view(s_view, a.st + a.tile_rep[tile]);
   __syncthreads();
   for (int step = 0; s_go; ++step) {
-    if (threadIdx.x == 0) {
-      s_step_tally = 0ull;
-      s_fin = -1;
-    }
+    if (threadIdx.x == 0) s_step_tally = 0ull;
     __syncthreads();
     bool stepped = false;
     if (has_tile)
       stepped = force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, &s_view,
-                                                               step & 1, &s_fin);
+                                                               step & 1);
     budget -= 1;
+    __syncthreads();  // the tile's partial sums are written
     unsigned long long now = 0ull;
     if (threadIdx.x == 0) now = step_arrive(a, step);
-    __syncthreads();
-    // the replica's finalizer: replica totals and state update, between its
-    // arrival and the barrier's completion
-    const int fr = s_fin;
-    if (fr >= 0) {
-      const RepDev& R = a.rep[fr];
-      block_rows_sum(a.gpart + (size_t)(step & 1) * a.gpart_half + (size_t)R.group0 * kNPart, R.ngroups,
-                     reinterpret_cast<double*>(s_dyn) + (blockDim.x >> 5) * kNPart, s_tot);
-      finish_step_persist(a, R, a.st + fr, s_tot);
+    // the replica reduction and the step's finish, between the arrival and
+    // the barrier's completion
+    if (stepped && post_reduce(a, tile, step & 1, reinterpret_cast<double*>(s_dyn) + (blockDim.x >> 5) * kNPart,
+                               s_tot)) {
+      const int rep = a.tile_rep[tile];
+      finish_step_persist(a, a.rep[rep], a.st + rep, s_tot);
     }
     if (threadIdx.x == 0) {
       s_go = step_decide(a, step, budget, seen, now, h_loop);
