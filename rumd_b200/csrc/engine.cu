@@ -777,13 +777,13 @@ int steps_grid(const b2md_engine* e, StepsFn fn, size_t smem) {
 }
 
 // The persistent step graph:
-//   gate_loop -> WHILE(loop) { gate -> IF(rebuild) {rebuild kernels} -> k_steps }
+//   gate_loop -> WHILE(loop) { rebuild kernels -> k_steps }
 // k_steps runs fused steps with a grid barrier between them until a list
 // rebuild is due, the step budget (pctl->budget, written by the host before
 // each launch) is spent or no replica has steps left, and sets the loop
-// condition; the gate inside the loop decides the rebuild from the replicas'
-// flags.  Between rebuilds the steps cost one grid barrier each instead of a
-// conditional node and a kernel launch.
+// condition.  The rebuild kernels act on the replicas whose rebuild flag is
+// set and exit at once otherwise.  Between rebuilds the steps cost one grid
+// barrier each instead of a conditional node and a kernel launch.
 void build_persist_graph(b2md_engine* e) {
   EngArgs a = make_args(e);
   const size_t smem = force_smem(e, a);
@@ -811,28 +811,16 @@ void build_persist_graph(b2md_engine* e) {
   cudaGraphNode_t wnode;
   CK(cudaGraphAddNode(&wnode, g, &gate, 1, &wp));
   cudaGraph_t body = wp.conditional.phGraph_out[0];
-  cudaGraphConditionalHandle hr;
-  CK(cudaGraphConditionalHandleCreate(&hr, body, 0, cudaGraphCondAssignDefault));
-  cudaGraphNode_t bgate;
-  {
-    cudaKernelNodeParams kp = {};
-    void* args[] = {&a, &hr};
-    kp.func = (void*)k_gate;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(256);
-    kp.kernelParams = args;
-    CK(cudaGraphAddKernelNode(&bgate, body, nullptr, 0, &kp));
-  }
-  cudaGraphNodeParams ip = {};
-  ip.type = cudaGraphNodeTypeConditional;
-  ip.conditional.handle = hr;
-  ip.conditional.type = cudaGraphCondTypeIf;
-  ip.conditional.size = 1;
-  cudaGraphNode_t inode;
-  CK(cudaGraphAddNode(&inode, body, &bgate, 1, &ip));
-  cudaGraph_t rbody = ip.conditional.phGraph_out[0];
-  CK(cudaStreamBeginCaptureToGraph(e->cap_stream, rbody, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  // the loop body: the rebuild kernels (each exits at once for replicas
+  // whose rebuild flag is clear: k_steps stops only when one is due, or at
+  // the budget, or at the start of the run), then k_steps
+  CK(cudaStreamBeginCaptureToGraph(e->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
   launch_rebuild(e, e->cap_stream, a);
+  cudaStreamCaptureStatus cst;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  CK(cudaStreamGetCaptureInfo(e->cap_stream, &cst, nullptr, nullptr, &deps, &ndeps));
+  std::vector<cudaGraphNode_t> leaf(deps, deps + ndeps);
   cudaGraph_t captured;
   CK(cudaStreamEndCapture(e->cap_stream, &captured));
   {
@@ -844,7 +832,7 @@ void build_persist_graph(b2md_engine* e) {
     kp.sharedMemBytes = (unsigned)smem;
     kp.kernelParams = args;
     cudaGraphNode_t knode;
-    CK(cudaGraphAddKernelNode(&knode, body, &inode, 1, &kp));
+    CK(cudaGraphAddKernelNode(&knode, body, leaf.data(), leaf.size(), &kp));
     cudaKernelNodeAttrValue av = {};
     av.cooperative = 1;
     CK(cudaGraphKernelNodeSetAttribute(knode, cudaKernelNodeAttributeCooperative, &av));
