@@ -238,16 +238,17 @@ def time_run(capi, e, steps, device):
 
 
 def launches_in_run(steps, rebuilds, per_rebuild=8, persistent=False):
-    # run start: steps + momentum; run end: rebuild sequence + force kernel;
-    # per rebuild: 8 kernels (9 with position windows).  Per-step graphs: a
-    # fused kernel per step and a gate per graph launch.  Persistent graph:
-    # one loop gate, then per loop pass a gate and one k_steps launch (a pass
-    # ends at each rebuild).
+    # run start: steps + momentum; run end: rebuild sequence + force kernel.
+    # Per-step graphs: a fused kernel per step, a gate per graph launch and
+    # the rebuild kernels (8, 9 with position windows) per rebuild.
+    # Persistent graph: one loop gate, then per loop pass (a pass ends at each
+    # rebuild) the rebuild kernels, which exit at once when none is due, and
+    # one k_steps launch.
     if persistent:
-        core = 1 + 2 * (rebuilds + 1)
+        core = 1 + (rebuilds + 1) * (per_rebuild + 1)
     else:
-        core = steps + steps // 32 + steps % 32
-    return int(core + per_rebuild * rebuilds + 2 + per_rebuild + 1)
+        core = steps + steps // 32 + steps % 32 + per_rebuild * rebuilds
+    return int(core + 2 + per_rebuild + 1)
 
 
 def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
