@@ -101,16 +101,12 @@ struct RepState {
 };
 
 // Control block of the persistent step kernel (k_steps), one per engine.
-constexpr int kPersistMaxSm = 1024;    // SM ids the tile order can use
-constexpr int kPersistMaxGrid = 8192;  // blocks the tile order can rank
 struct PersistCtl {
   unsigned long long arrive;  // setup barrier: blocks arrived
   unsigned long long word[2];  // step barriers (alternating): arrivals and the finalizers' tallies
   unsigned gen;     // grid-barrier generation
   int budget;       // steps this graph launch may still run (set by the host)
   int err;          // a grid-barrier wait gave up (reported to the host)
-  unsigned smslot[kPersistMaxSm];  // blocks of this launch seen per SM id
-  unsigned rank[kPersistMaxGrid];  // per block: slot on its SM * nsmid + SM id
 };
 
 struct EngArgs {
