@@ -329,6 +329,12 @@ size_t force_smem(const b2md_engine* e, const EngArgs& a) {
   return (need + 15) & ~(size_t)15;
 }
 
+// Dynamic shared memory of k_steps: the pair table, which stays loaded for
+// the launch, then the reduction scratch.
+size_t persist_smem(const b2md_engine* e, const EngArgs& a) {
+  return (size_t)persist_table_bytes(a) + (size_t)force_red_bytes(e->pb * e->tp);
+}
+
 // Dynamic shared memory of k_rb_build: cut-off table [+ list tile] [+ window scratch].
 size_t build_smem(const b2md_engine* e, const EngArgs& a) {
   const int pb = e->pb;
@@ -786,7 +792,7 @@ int steps_grid(const b2md_engine* e, StepsFn fn, size_t smem) {
 // barrier each instead of a conditional node and a kernel launch.
 void build_persist_graph(b2md_engine* e) {
   EngArgs a = make_args(e);
-  const size_t smem = force_smem(e, a);
+  const size_t smem = persist_smem(e, a);
   force_fn(e, true, false, a);  // checks the shared-memory need
   StepsFn fs = steps_fn(e->tp);
   cudaGraph_t g;
@@ -856,7 +862,7 @@ void ensure_graphs(b2md_engine* e) {
     EngArgs a = make_args(e);
     int per_sm = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)steps_fn(e->tp), e->pb * e->tp,
-                                                     force_smem(e, a)));
+                                                     persist_smem(e, a)));
     e->persist_on = (long long)per_sm * e->nsm >= e->ntiles;
   }
   if (e->persist_on) {

@@ -707,6 +707,11 @@ constexpr int kParSmemFloats = kMaxTypes * kMaxTypes * kParStride;
 __host__ __device__ constexpr int force_red_bytes(int threads) {
   return ((threads + 31) / 32) * kNPart * (int)sizeof(double) + threads * (int)sizeof(double);
 }
+// k_steps keeps the pair table (of the engine's largest type count) at the
+// start of its dynamic shared memory; the reduction scratch follows it.
+__host__ __device__ inline int persist_table_bytes(const EngArgs& a) {
+  return (a.max_types * a.max_types * kParStride * (int)sizeof(float) + 15) & ~15;
+}
 constexpr unsigned kWaitPolls = 1u << 22;
 
 enum { FM_STREAMED = 0, FM_STAGED = 1, FM_WINDOW = 2 };
@@ -758,8 +763,9 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
   unsigned short* s_wl = reinterpret_cast<unsigned short*>(s_win + a.win_cap);  // mode 2: staged window list
   // the block reduction's scratch reuses the start of the dynamic region once
-  // every thread is past the neighbour loop (force_red_bytes)
-  double* s_warp = reinterpret_cast<double*>(s_dyn);
+  // every thread is past the neighbour loop (force_red_bytes); in k_steps it
+  // follows the pair table, which stays loaded for the whole launch
+  double* s_warp = reinterpret_cast<double*>(s_dyn + (PERSIST ? persist_table_bytes(a) : 0));
   double* s_scr = s_warp + (blockDim.x >> 5) * kNPart;
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
@@ -833,7 +839,8 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
     }
     // 3. meanwhile: pair table and this particle's data
     const int nt = R.ntypes;
-    for (int k = threadIdx.x; k < nt * nt * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
+    if (!PERSIST)
+      for (int k = threadIdx.x; k < nt * nt * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
     const int lp = threadIdx.x / TP, lane_t = threadIdx.x % TP;
     const int i = first + lp;
     const bool valid = i < R.n;
@@ -1161,8 +1168,15 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
   __shared__ StepView s_view;
   const int tile = blockIdx.x;
   const bool has_tile = tile < a.ntiles;
-  if (threadIdx.x == 0 && has_tile) load_view(s_view, a.st + a.tile_rep[tile]);
+  if (has_tile) {
+    if (threadIdx.x == 0) load_view(s_view, a.st + a.tile_rep[tile]);
+    // the replica's pair table, once for the launch
+    const RepDev& R = a.rep[a.tile_rep[tile]];
+    float* s_par = reinterpret_cast<float*>(s_dyn);
+    for (int k = threadIdx.x; k < R.ntypes * R.ntypes * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
+  }
   __syncthreads();
+  double* s_red = reinterpret_cast<double*>(s_dyn + persist_table_bytes(a)) + (blockDim.x >> 5) * kNPart;
   for (int step = 0; s_go; ++step) {
     if (threadIdx.x == 0) s_step_tally = 0ull;
     __syncthreads();
@@ -1176,8 +1190,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     if (threadIdx.x == 0) now = step_arrive(a, step);
     // the replica reduction and the step's finish, between the arrival and
     // the barrier's completion
-    if (stepped && post_reduce(a, tile, step & 1, reinterpret_cast<double*>(s_dyn) + (blockDim.x >> 5) * kNPart,
-                               s_tot)) {
+    if (stepped && post_reduce(a, tile, step & 1, s_red, s_tot)) {
       const int rep = a.tile_rep[tile];
       finish_step_persist(a, a.rep[rep], a.st + rep, s_tot);
     }
