@@ -1419,7 +1419,11 @@ __global__ void k_rb_scan_local(EngArgs a) {
   if (threadIdx.x == 0) a.ctot[tile] = s_carry;
 }
 
-// (3b) exclusive prefix of chunk totals over the replica's tiles (block per replica)
+// (3b) exclusive prefix of chunk totals over the replica's tiles (block per
+//      replica): thread t sums a run of consecutive tiles (its loads all in
+//      flight together), the block scans the run sums, and each thread
+//      writes its run's prefixes
+constexpr int kScanRun = 8;  // tiles per thread and pass
 __global__ void k_rb_scan_tiles(EngArgs a) {
   __shared__ int s_w[32];
   __shared__ int s_carry;
@@ -1428,12 +1432,20 @@ __global__ void k_rb_scan_tiles(EngArgs a) {
   const RepDev& R = a.rep[rep];
   if (R.nb_method != NB_CELLS) return;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int* __restrict__ tot = a.ctot + R.tile0;
+  int* __restrict__ pref = a.cpref + R.tile0;
   if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
-  for (int base = 0; base < R.ntiles; base += blockDim.x) {
-    const int t = base + threadIdx.x;
-    const int x = t < R.ntiles ? a.ctot[R.tile0 + t] : 0;
-    int incl = x;
+  for (int base = 0; base < R.ntiles; base += blockDim.x * kScanRun) {
+    const int t0 = base + threadIdx.x * kScanRun;
+    int x[kScanRun];
+    int sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanRun; ++k) {
+      x[k] = t0 + k < R.ntiles ? tot[t0 + k] : 0;
+      sum += x[k];
+    }
+    int incl = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       int y = __shfl_up_sync(0xffffffffu, incl, o);
@@ -1444,12 +1456,17 @@ __global__ void k_rb_scan_tiles(EngArgs a) {
     int woff = 0;
     for (int w = 0; w < wid; ++w) woff += s_w[w];
     const int carry = s_carry;
-    if (t < R.ntiles) a.cpref[R.tile0 + t] = carry + woff + incl - x;
+    int run = carry + woff + incl - sum;
+#pragma unroll
+    for (int k = 0; k < kScanRun; ++k) {
+      if (t0 + k < R.ntiles) pref[t0 + k] = run;
+      run += x[k];
+    }
     __syncthreads();
     if (threadIdx.x == blockDim.x - 1) {
-      int tot = 0;
-      for (int w = 0; w < nw; ++w) tot += s_w[w];
-      s_carry = carry + tot;
+      int t = 0;
+      for (int w = 0; w < nw; ++w) t += s_w[w];
+      s_carry = carry + t;
     }
     __syncthreads();
   }
@@ -1477,6 +1494,7 @@ __global__ void k_rb_scatter(EngArgs a) {
 //     (thrust::sort_by_key on (cellIndex, iota), Sample.h:174-188).  Also
 //     turns cstart into each cell's absolute first slot (cstart + the chunk's
 //     prefix), which the list build reads without a division.
+constexpr int kFixRegs = 8;  // buckets up to this size are sorted in registers
 __global__ void k_rb_fix(EngArgs a) {
   const int tile = blockIdx.x, rep = a.tile_rep[tile];
   if (!rb_active(a, rep)) return;
@@ -1489,6 +1507,24 @@ __global__ void k_rb_fix(EngArgs a) {
     const int b = a.cstart[R.cell0 + c] + pref, m = a.cnt[R.cell0 + c];
     a.cstart[R.cell0 + c] = b;
     unsigned* o = a.order + (size_t)R.p0 + b;
+    if (m <= kFixRegs) {
+      // the bucket in registers (padding sorts last), odd-even transposition
+      unsigned x[kFixRegs];
+#pragma unroll
+      for (int k = 0; k < kFixRegs; ++k) x[k] = k < m ? o[k] : 0xffffffffu;
+#pragma unroll
+      for (int r = 0; r < kFixRegs; ++r)
+#pragma unroll
+        for (int k = r & 1; k + 1 < kFixRegs; k += 2) {
+          const unsigned lo = min(x[k], x[k + 1]), hi = max(x[k], x[k + 1]);
+          x[k] = lo;
+          x[k + 1] = hi;
+        }
+#pragma unroll
+      for (int k = 0; k < kFixRegs; ++k)
+        if (k < m) o[k] = x[k];
+      continue;
+    }
     for (int p = 1; p < m; ++p) {
       unsigned x = o[p];
       int q = p - 1;
