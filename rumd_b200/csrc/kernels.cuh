@@ -757,7 +757,8 @@ __device__ __forceinline__ void load_view(StepView& v, const RepState* S) {
 template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
 __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
                                            double* s_tot, uint64_t& s_bar, unsigned& s_rows,
-                                           const StepView* pv = nullptr, int gpar = 0) {
+                                           const StepView* pv = nullptr, int gpar = 0,
+                                           const RepDev* prep = nullptr) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -768,7 +769,8 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
   double* s_warp = reinterpret_cast<double*>(s_dyn + (PERSIST ? persist_table_bytes(a) : 0));
   double* s_scr = s_warp + (blockDim.x >> 5) * kNPart;
   const int rep = a.tile_rep[tile];
-  const RepDev& R = a.rep[rep];
+  // PERSIST: k_steps' shared-memory copy of the replica's descriptor
+  const RepDev& R = PERSIST ? *prep : a.rep[rep];
   RepState* S = a.st + rep;
   // PERSIST: the block's view of its replica's state, kept by k_steps
   // (the buffer parity, step counters); xi and the momentum come from the
@@ -881,7 +883,7 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
         mbar_wait_bounded(&s_bar, 0, kWaitPolls);
       }
     } else {
-      __syncthreads();  // the pair table
+      if (!PERSIST) __syncthreads();  // the pair table (k_steps loads it once per launch)
       using PosS = typename Pick<PERSIST, PosCoherent, PosGlobal>::type;
       force_loop_any<TP, STRESS, true>(fast, R.potential, nt, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosS{rc}, lane_t, nn, ri, prow, Lx, Ly,
                                  Lz, iLx, iLy, iLz);
@@ -1166,12 +1168,17 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
   // one tile per block (the engine uses k_steps only when every tile has a
   // resident block); the block's view of its replica's state
   __shared__ StepView s_view;
+  // the replica's descriptor and pair table, which no step changes, once for
+  // the launch
+  __shared__ __align__(16) RepDev s_rep;
   const int tile = blockIdx.x;
   const bool has_tile = tile < a.ntiles;
   if (has_tile) {
     if (threadIdx.x == 0) load_view(s_view, a.st + a.tile_rep[tile]);
-    // the replica's pair table, once for the launch
     const RepDev& R = a.rep[a.tile_rep[tile]];
+    static_assert(sizeof(RepDev) % sizeof(int) == 0, "descriptor copied as words");
+    for (int k = threadIdx.x; k < (int)(sizeof(RepDev) / sizeof(int)); k += blockDim.x)
+      reinterpret_cast<int*>(&s_rep)[k] = reinterpret_cast<const int*>(&R)[k];
     float* s_par = reinterpret_cast<float*>(s_dyn);
     for (int k = threadIdx.x; k < R.ntypes * R.ntypes * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
   }
@@ -1183,7 +1190,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     bool stepped = false;
     if (has_tile)
       stepped = force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, &s_view,
-                                                               step & 1);
+                                                               step & 1, &s_rep);
     budget -= 1;
     __syncthreads();  // the tile's partial sums are written
     unsigned long long now = 0ull;
