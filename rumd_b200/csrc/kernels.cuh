@@ -117,10 +117,9 @@ __device__ bool replica_reduce(const EngArgs& a, int rep, const RepDev& R, int l
 // and the replica counter.  Returns true in the replica's last block, which
 // then sums the group totals and finishes the step; the other blocks have
 // gone on to the next step and wait for that only before they integrate.
-__device__ bool post_reduce(const EngArgs& a, int tile, int par, double* s_scr, double* s_tot) {
+__device__ bool post_reduce(const EngArgs& a, int tile, int rep, const RepDev& R, int par, double* s_scr,
+                            double* s_tot) {
   __shared__ int s_last;
-  const int rep = a.tile_rep[tile];
-  const RepDev& R = a.rep[rep];
   const int lt = tile - R.tile0;
   const int g = lt / kGroup;
   const int gfirst = g * kGroup;
@@ -735,7 +734,7 @@ enum { FM_STREAMED = 0, FM_STAGED = 1, FM_WINDOW = 2 };
 // finalizer (on another SM) wrote them, so thread 0 reads them past L1 once
 // per tile and the block shares them through shared memory.
 struct StepView {
-  int overflow, rbuf, abuf, pad_;
+  int overflow, rbuf, abuf, first;  // first: the tile's first slot
   long long steps_left, run_step, steps;
   double M, P[3], xi;
 };
@@ -780,7 +779,7 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
   const bool skip = (SV(overflow) != 0) || (FUSED && SV(steps_left) <= 0) || !R.active;
   if (!skip) {
     const int pb = blockDim.x / TP;
-    const int first = a.tile_first[tile];
+    const int first = PERSIST ? pv->first : a.tile_first[tile];
     const int pitch = a.idx_pitch;
     const int rb = SV(rbuf);
     const float4* rc = a.r[rb] + R.p0;
@@ -1173,8 +1172,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
   __shared__ __align__(16) RepDev s_rep;
   const int tile = blockIdx.x;
   const bool has_tile = tile < a.ntiles;
+  const int rep_id = has_tile ? a.tile_rep[tile] : 0;
   if (has_tile) {
-    if (threadIdx.x == 0) load_view(s_view, a.st + a.tile_rep[tile]);
+    if (threadIdx.x == 0) {
+      load_view(s_view, a.st + a.tile_rep[tile]);
+      s_view.first = a.tile_first[tile];
+    }
     const RepDev& R = a.rep[a.tile_rep[tile]];
     static_assert(sizeof(RepDev) % sizeof(int) == 0, "descriptor copied as words");
     for (int k = threadIdx.x; k < (int)(sizeof(RepDev) / sizeof(int)); k += blockDim.x)
@@ -1197,10 +1200,8 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     if (threadIdx.x == 0) now = step_arrive(a, step);
     // the replica reduction and the step's finish, between the arrival and
     // the barrier's completion
-    if (stepped && post_reduce(a, tile, step & 1, s_red, s_tot)) {
-      const int rep = a.tile_rep[tile];
-      finish_step_persist(a, a.rep[rep], a.st + rep, s_tot);
-    }
+    if (stepped && post_reduce(a, tile, rep_id, s_rep, step & 1, s_red, s_tot))
+      finish_step_persist(a, s_rep, a.st + rep_id, s_tot);
     if (threadIdx.x == 0) {
       s_go = step_decide(a, step, budget, seen, now, h_loop);
       if (stepped) {
