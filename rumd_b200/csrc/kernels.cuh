@@ -753,11 +753,20 @@ __device__ __forceinline__ void load_view(StepView& v, const RepState* S) {
   v.xi = __ldcg(&S->xi);
 }
 
+// Per-thread state that k_steps keeps in registers for a launch (no rebuild,
+// hence no re-sort, happens inside one): the particle's list length and, in
+// its integrating thread, the velocity, image counts and build-time position.
+struct PersistRegs {
+  float4 v, lr;
+  int4 im;
+  unsigned nn;
+};
+
 template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
 __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
                                            double* s_tot, uint64_t& s_bar, unsigned& s_rows,
                                            const StepView* pv = nullptr, int gpar = 0,
-                                           const RepDev* prep = nullptr) {
+                                           const RepDev* prep = nullptr, PersistRegs* pr = nullptr) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -850,7 +859,7 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
     const float4 ri = valid ? (PERSIST ? rc[i] : __ldg(rc + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
     const int ti = valid ? __float_as_int(ri.w) : 0;
     const float* prow = s_par + ti * nt * kParStride;
-    const unsigned nn = valid ? a.nn[R.p0 + i] : 0u;
+    const unsigned nn = valid ? (PERSIST ? pr->nn : a.nn[R.p0 + i]) : 0u;
     const size_t lstride = (size_t)R.nbl_stride;
     const unsigned* lbase = a.nbl + R.nbl0;
     const unsigned short* wbase = a.wl + R.nbl0;
@@ -942,8 +951,8 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
       acc[P_W] = (double)ww;
       if (FUSED) {
         const int ab = SV(abuf);
-        float4 v = a.v[ab][gi];
-        int4 im = a.im[ab][gi];
+        float4 v = PERSIST ? pr->v : a.v[ab][gi];
+        int4 im = PERSIST ? pr->im : a.im[ab][gi];
         const bool do_reset = R.reset_interval > 0 && (SV(run_step) % R.reset_interval) == 0;
         float3 vs = make_float3(0.f, 0.f, 0.f);
         const double M = SVS(M, s_M);
@@ -951,9 +960,14 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
           vs = make_float3((float)(SVS(P[0], s_P[0]) / M), (float)(SVS(P[1], s_P[1]) / M),
                            (float)(SVS(P[2], s_P[2]) / M));
         float4 rn;
-        integrate_one(R, (float)SVS(xi, s_xi), vs, do_reset, ri, fo, v, im, rn, acc, exceed, a.last_r[gi]);
+        integrate_one(R, (float)SVS(xi, s_xi), vs, do_reset, ri, fo, v, im, rn, acc, exceed,
+                      PERSIST ? pr->lr : a.last_r[gi]);
         a.v[ab][gi] = v;
         a.im[ab][gi] = im;
+        if (PERSIST) {
+          pr->v = v;
+          pr->im = im;
+        }
         a.r[rb ^ 1][gi] = rn;
       }
     }
@@ -1147,7 +1161,7 @@ __device__ int step_decide(const EngArgs& a, int step, int budget, unsigned long
 // order that spread each SM's tiles over the box measured 0.3 us per step
 // slower than block order.)
 template <int TP>
-__global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditionalHandle h_loop) {
+__global__ void __maxnreg__(72) k_steps(EngArgs a, cudaGraphConditionalHandle h_loop) {
   extern __shared__ __align__(128) unsigned char s_dyn[];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
   __shared__ __align__(8) uint64_t s_bar;
@@ -1186,6 +1200,19 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     for (int k = threadIdx.x; k < R.ntypes * R.ntypes * kParStride; k += blockDim.x) s_par[k] = a.par[R.par0 + k];
   }
   __syncthreads();
+  PersistRegs pr{};
+  if (has_tile) {
+    const int i = s_view.first + (int)threadIdx.x / TP;
+    if (i < s_rep.n) {
+      const size_t gi = (size_t)s_rep.p0 + i;
+      pr.nn = a.nn[gi];
+      if (threadIdx.x % TP == 0) {
+        pr.v = a.v[s_view.abuf][gi];
+        pr.im = a.im[s_view.abuf][gi];
+        pr.lr = a.last_r[gi];
+      }
+    }
+  }
   double* s_red = reinterpret_cast<double*>(s_dyn + persist_table_bytes(a)) + (blockDim.x >> 5) * kNPart;
   for (int step = 0; s_go; ++step) {
     if (threadIdx.x == 0) s_step_tally = 0ull;
@@ -1193,7 +1220,7 @@ __global__ void __launch_bounds__(kMaxBlock) k_steps(EngArgs a, cudaGraphConditi
     bool stepped = false;
     if (has_tile)
       stepped = force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, &s_view,
-                                                               step & 1, &s_rep);
+                                                               step & 1, &s_rep, &pr);
     budget -= 1;
     __syncthreads();  // the tile's partial sums are written
     unsigned long long now = 0ull;
