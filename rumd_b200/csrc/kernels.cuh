@@ -766,7 +766,8 @@ template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
 __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
                                            double* s_tot, uint64_t& s_bar, unsigned& s_rows,
                                            const StepView* pv = nullptr, int gpar = 0,
-                                           const RepDev* prep = nullptr, PersistRegs* pr = nullptr) {
+                                           const RepDev* prep = nullptr, PersistRegs* pr = nullptr,
+                                           unsigned* wdone = nullptr) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -917,9 +918,10 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
       }
     }
     if constexpr (PERSIST && FUSED) {
-      // wait (bounded) for the previous step's finalizer: it stores the step
-      // count last, with release
-      if (threadIdx.x == 0) {
+      // the block's first warp past its neighbour loop waits (bounded) for
+      // the previous step's finalizer, which stores the step count last, with
+      // release; the other warps are still in their loops meanwhile
+      if ((threadIdx.x & 31u) == 0 && atomicAdd(wdone, 1u) == 0u) {
         const unsigned long long want = (unsigned long long)pv->steps;
         for (unsigned it = 0; ld_acquire_u64(reinterpret_cast<const unsigned long long*>(&S->steps)) < want; ++it) {
           if (it >= kWaitPolls) {
@@ -1184,6 +1186,7 @@ __global__ void __maxnreg__(72) k_steps(EngArgs a, cudaGraphConditionalHandle h_
   // the replica's descriptor and pair table, which no step changes, once for
   // the launch
   __shared__ __align__(16) RepDev s_rep;
+  __shared__ unsigned s_wdone;  // warps of the block past their neighbour loop this step
   const int tile = blockIdx.x;
   const bool has_tile = tile < a.ntiles;
   const int rep_id = has_tile ? a.tile_rep[tile] : 0;
@@ -1215,12 +1218,15 @@ __global__ void __maxnreg__(72) k_steps(EngArgs a, cudaGraphConditionalHandle h_
   }
   double* s_red = reinterpret_cast<double*>(s_dyn + persist_table_bytes(a)) + (blockDim.x >> 5) * kNPart;
   for (int step = 0; s_go; ++step) {
-    if (threadIdx.x == 0) s_step_tally = 0ull;
+    if (threadIdx.x == 0) {
+      s_step_tally = 0ull;
+      s_wdone = 0u;
+    }
     __syncthreads();
     bool stepped = false;
     if (has_tile)
       stepped = force_tile<TP, true, false, FM_STREAMED, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, &s_view,
-                                                               step & 1, &s_rep, &pr);
+                                                               step & 1, &s_rep, &pr, &s_wdone);
     budget -= 1;
     __syncthreads();  // the tile's partial sums are written
     unsigned long long now = 0ull;
