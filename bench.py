@@ -58,6 +58,9 @@ def parse():
                    help="kernel variant: 1 = one cooperative kernel runs the steps between list rebuilds")
     p.add_argument("--profile-launches", action="store_true",
                    help="small plain run only (for the ncu launch list)")
+    p.add_argument("--profile-batched", action="store_true",
+                   help="the 256-replica batch only, eager launches of --steps steps between "
+                        "cudaProfilerStart/Stop (for the ncu launch list)")
     p.add_argument("--lj1m", action="store_true",
                    help="only the HBM-scale plain workload: single-component LJ, N=1,048,576 (one JSON line)")
     return p.parse_args()
@@ -163,6 +166,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as fh:
+            for ln in fh:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -251,66 +266,118 @@ def launches_in_run(steps, rebuilds, per_rebuild=8, persistent=False):
     return int(core + 2 + per_rebuild + 1)
 
 
-def cpu_baseline_sample(e, rid, box, params, seconds=15.0):
-    """The oracle's FP32 step (cell list + full list + forces + NVT) on all host cores."""
-    from oracle import oracle as O
-    n = N_PLAIN
-    pos4 = e.get(rid, "pos", n)
-    vel4 = e.get(rid, "vel", n)
-    im3 = e.get(rid, "images", n)
-    kw = dict(L=box, ntypes=2, params=params, cutoff=O.SF, skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU)
+def _timed_oracle_steps(O, pos4, vel4, im3, kw, seconds):
     t = time.perf_counter()
     O.md_run(pos4, vel4, im3, nsteps=2, **kw)
     one = max((time.perf_counter() - t) / 2, 1e-4)
-    steps = int(max(4, min(2000, seconds / one)))
+    steps = int(max(2, min(2000, seconds / one)))
     t = time.perf_counter()
     O.md_run(pos4, vel4, im3, nsteps=steps, **kw)
-    dt = time.perf_counter() - t
-    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
+    return steps, time.perf_counter() - t
+
+
+def cpu_baseline_sample(e, rid, box, params, seconds=15.0, seconds_1core=5.0):
+    """The oracle's FP32 step (cell list + full list + forces + NVT) on all
+    host cores, and on one core, from the GPU arm's own equilibrated state."""
+    from oracle import oracle as O
+    n = N_PLAIN
+    pos4, vel4, im3 = e.read(rid, n)
+    kw = dict(L=box, ntypes=2, params=params, cutoff=O.SF, skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU)
+    cores = O.num_threads()
+    steps, dt = _timed_oracle_steps(O, pos4, vel4, im3, kw, seconds)
+    O.set_num_threads(1)
+    try:
+        steps1, dt1 = _timed_oracle_steps(O, pos4, vel4, im3, kw, seconds_1core)
+    finally:
+        O.set_num_threads(cores)
+    return {"value": n * steps / dt, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "cpu_model": cpu_model(), "value_1core": n * steps1 / dt1,
             "sample": f"KA N={n} from the equilibrated T=0.45 state, {steps} FP32 steps (cell sort, full list, "
-                      f"SF forces, NVT) with OpenMP over particles"}
+                      f"SF forces, NVT) with OpenMP over particles on {cores} threads; {steps1} steps on 1 thread "
+                      f"for value_1core"}
+
+
+def pinned(a):
+    """A page-locked host copy of numpy array a (the caller's pinned buffers)."""
+    import torch
+    t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    return out, t
 
 
 def e2e_run(capi, device, pb, tp, pos4, vel4, im3, box, params, steps):
-    """Public API end to end: upload (H2D) + Run(steps) + read back (D2H).
-    The engine is created, with pools sized for the system (the way a
-    serving process keeps one), before the timed region."""
+    """Public API end to end: upload (H2D from the caller's pinned arrays) +
+    Run(steps) + read back (D2H) of positions, velocities, images and the
+    energies.  The engine is created, with pools sized for the system (the way
+    a serving process keeps one), before the timed region."""
     n = len(pos4)
+    (p_in, t1), (v_in, t2) = pinned(np.ascontiguousarray(pos4)), pinned(np.ascontiguousarray(vel4))
     e = new_engine(capi, device=device, pb=pb, tp=tp, max_particles=n, max_list_entries=n * 256)
     e.run(0)
     t = time.perf_counter()
-    rid = e.add(pos4, box, params, 2, cutoff="SF", skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU, vel4=vel4, im3=im3)
+    rid = e.add(p_in, box, params, 2, cutoff="SF", skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU, vel4=v_in, im3=im3)
     t_add = time.perf_counter()
     e.run(steps)
     t_run = time.perf_counter()
-    p = e.get(rid, "pos", n)
-    v = e.get(rid, "vel", n)
-    im = e.get(rid, "images", n)
+    p, v, im = e.read(rid, n)
     st = e.stats(rid)
     t_end = time.perf_counter()
     dt = t_end - t
     e.close()
+    del t1, t2
     assert np.isfinite(p).all() and np.isfinite(st["pe"])
-    h2d = n * (16 + 16 + 16 + 16 + 4)          # r, last_r, v, images, ids
-    d2h = n * (3 * (16 + 4) + 4) + 256         # pos, vel, images (+ ids each), list lengths, state
+    h2d = n * (16 + 16 + 16)                   # r, v, images (last_r and ids are made on the device)
+    d2h = n * (4 + 16 + 16 + 16 + 4) + 256     # ids, pos, vel, images, list lengths (stats), state
     return {"value": n * steps / dt, "unit": "particle-steps/s",
             "h2d_bytes_per_step": h2d / steps, "d2h_bytes_per_step": d2h / steps,
             "phases_ms": {"add": 1e3 * (t_add - t), "run": 1e3 * (t_run - t_add), "read_back": 1e3 * (t_end - t_run)}}
 
 
-def batched(capi, device, pb, tp, steps, seed=0):
-    """256 KA replicas, N log-uniform in [512, 8192], T log-spaced 0.45..2.0,
-    advanced together; against sequential plain runs of every 16th replica."""
+def batch_workload(seed=0):
+    """The batching configuration: 256 KA replicas, N = floor(exp(U(ln 512,
+    ln 8192))) (seeded), T log-spaced from 0.45 to 2.0."""
     from rumd_b200 import initconf as I
     rng = np.random.default_rng(seed)
     R = 256
     ns = np.floor(np.exp(rng.uniform(np.log(512), np.log(8192), R))).astype(int)
     Ts = np.exp(np.linspace(np.log(0.45), np.log(2.0), R))
-    params = ka_params()
     confs = [I.ka_config(int(n), T=float(T), seed=seed + k) for k, (n, T) in enumerate(zip(ns, Ts))]
+    return ns, Ts, confs
+
+
+def batch_engine(capi, device, pb, tp, ns, Ts, confs):
+    R = len(ns)
+    params = ka_params()
     e = new_engine(capi, device=device, max_particles=int(ns.sum() + 64 * R), max_replicas=R, pb=pb, tp=tp)
-    ids = [e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(T), tau=TAU,
-                 vel4=c["vel4"]) for c, T in zip(confs, Ts)]
+    for c, T in zip(confs, Ts):
+        e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(T), tau=TAU, vel4=c["vel4"])
+    return e
+
+
+def profile_batched(capi, device, args):
+    """The batch with eager launches (b2md_run_timed) for ncu's launch list."""
+    import torch
+    ns, Ts, confs = batch_workload()
+    e = batch_engine(capi, device, args.pb, args.tp, ns, Ts, confs)
+    e.run(300)
+    torch.cuda.synchronize(device)
+    torch.cuda.profiler.start()
+    ms, nl = e.run_timed(max(args.steps, 1))
+    torch.cuda.synchronize(device)
+    torch.cuda.profiler.stop()
+    print(json.dumps({"profile_batched_steps": args.steps, "particles": int(ns.sum()),
+                      "step_kernel_ms_avg": ms / max(args.steps, 1), "launches": nl}), flush=True)
+    e.close()
+
+
+def batched(capi, device, pb, tp, steps, seed=0):
+    """256 KA replicas, N log-uniform in [512, 8192], T log-spaced 0.45..2.0,
+    advanced together; against sequential plain runs of every 16th replica."""
+    R = 256
+    ns, Ts, confs = batch_workload(seed)
+    params = ka_params()
+    e = batch_engine(capi, device, pb, tp, ns, Ts, confs)
     e.run(500)
     t_b = time_run(capi, e, steps, device)
     rate_b = float(ns.sum()) * steps / t_b
@@ -411,16 +478,19 @@ def lj_hbm_scale(capi, device, args):
     e.close()
 
 
-def config_block(args, world, engine=None):
-    variants = {}
-    if engine is not None:
-        from rumd_b200 import capi
-        variants = {"force_mode": engine.get_variant(capi.VARIANT_FORCE_MODE),
-                    "build_lanes": engine.get_variant(capi.VARIANT_BUILD_LANES),
-                    "persistent": engine.get_variant(capi.VARIANT_PERSISTENT)}
+def kernel_variants(engine):
+    """The GPU arm's kernel variants (reported beside the config, not in it:
+    the reference arm runs the same workload without them)."""
+    from rumd_b200 import capi
+    return {"pb_tp": list(engine.launch()), "force_mode": engine.get_variant(capi.VARIANT_FORCE_MODE),
+            "build_lanes": engine.get_variant(capi.VARIANT_BUILD_LANES),
+            "persistent": engine.get_variant(capi.VARIANT_PERSISTENT)}
+
+
+def config_block(args, world):
     return {"workload": f"Kob-Andersen 80:20 LJ, N={N_PLAIN}, rho=1.2, T=0.45, NVT tau=0.2, dt=0.005, skin 0.3, "
                         "SF cut-off 2.5 sigma_ij (plain method, single large system)",
-            "n_particles": N_PLAIN, "pb": args.pb, "tp": args.tp, **variants,
+            "n_particles": N_PLAIN,
             "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             "precision": "FP32 forces, FP64 reductions/thermostat, int32 images",
             "l2_policy": "L2 flushed (512 MiB write) before the timed Run; inside a Run every step reads the "
@@ -429,16 +499,22 @@ def config_block(args, world, engine=None):
 
 def run_reference(args):
     """The reference arm: the CPU implementation of the path (oracle port) on
-    all host cores, same workload and metric, K steps capped to ~60 s."""
+    all host cores, same workload and metric.  The state is prepared with the
+    GPU arm's recipe (seeded FCC start, 1000 steps at T=2, then 2000 at
+    T=0.45, here on the CPU and untimed), then W warm-up steps and K timed
+    steps (K capped so that the timed part stays near 60 s)."""
     rank, world, local = dist_env()
     if rank != 0:
         return
     from oracle import oracle as O
     from rumd_b200 import initconf as I
-    c = I.ka_config(N_PLAIN, density=KA_DENSITY, T=T_PLAIN, seed=1)
+    c = I.ka_config(N_PLAIN, density=KA_DENSITY, T=2.0, seed=1)
     params = ka_params()
-    kw = dict(L=c["box"], ntypes=2, params=params, cutoff=O.SF, skin=SKIN, dt=DT, T=T_PLAIN, tau=TAU)
-    st = O.md_run(c["pos4"], c["vel4"], c["im3"], nsteps=max(args.warmup, 1), **kw)
+    kw = dict(L=c["box"], ntypes=2, params=params, cutoff=O.SF, skin=SKIN, dt=DT, tau=TAU)
+    st = O.md_run(c["pos4"], c["vel4"], c["im3"], nsteps=1000, T=2.0, **kw)
+    st = O.md_run(st["pos4"], st["vel4"], st["im3"], nsteps=2000, xi=st["xi"], T=T_PLAIN, **kw)
+    kw["T"] = T_PLAIN
+    st = O.md_run(st["pos4"], st["vel4"], st["im3"], nsteps=max(args.warmup, 1), xi=st["xi"], **kw)
     t = time.perf_counter()
     st2 = O.md_run(st["pos4"], st["vel4"], st["im3"], nsteps=2, xi=st["xi"], **kw)
     one = (time.perf_counter() - t) / 2
@@ -447,14 +523,15 @@ def run_reference(args):
     O.md_run(st2["pos4"], st2["vel4"], st2["im3"], nsteps=steps, xi=st2["xi"], **kw)
     dt = time.perf_counter() - t
     v = N_PLAIN * steps / dt
-    sample = (f"KA N={N_PLAIN} from the FCC start at T=0.45, {steps} of the requested {args.steps} steps "
-              "(capped at ~60 s), FP32 reference arithmetic, OpenMP over particles")
+    sample = (f"KA N={N_PLAIN} equilibrated with the GPU arm's recipe (seeded FCC, 1000 steps at T=2, 2000 at "
+              f"T=0.45; untimed, on the CPU), then {steps} of the requested {args.steps} steps (capped at ~60 s), "
+              "FP32 reference arithmetic, OpenMP over particles")
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
             "steps": steps, "warmup": args.warmup, "ms_per_step": dt / steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": config_block(args, world),
             "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": O.num_threads(), "kind": "port",
-                             "sample": sample},
+                             "cpu_model": cpu_model(), "sample": sample},
             "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -475,6 +552,10 @@ def main():
     device = local
     if args.lj1m:
         lj_hbm_scale(capi, device, args)
+        dist.close()
+        return
+    if args.profile_batched:
+        profile_batched(capi, device, args)
         dist.close()
         return
     if args.profile_launches:
@@ -532,10 +613,11 @@ def main():
                 "bytes_per_launch_alg": bytes_alg, "mean_list_length": st2["mean_nbrs"],
                 "step_share_of_run": per_launch_s * args.steps / t}
     extra = {}
-    cfg = config_block(args, world, e)
-    per_rebuild = 9 if cfg.get("force_mode") == capi.FORCE_WINDOW else 8
+    cfg = config_block(args, world)
+    variants = kernel_variants(e)
+    per_rebuild = 9 if variants.get("force_mode") == capi.FORCE_WINDOW else 8
     if rank == 0:
-        pos4, vel4, im3 = e.get(rid, "pos", N_PLAIN), e.get(rid, "vel", N_PLAIN), e.get(rid, "images", N_PLAIN)
+        pos4, vel4, im3 = e.read(rid, N_PLAIN)
         e2e = e2e_run(capi, device, args.pb, args.tp, pos4, vel4, im3, box, params, args.steps)
         if not args.no_cpu_baseline:
             extra["cpu_baseline"] = cpu_baseline_sample(e, rid, box, params)
@@ -549,7 +631,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps * 1e3,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic (seeded FCC start, melted and equilibrated untimed)",
-                "config": cfg, "clocks": clk, "e2e": e2e,
+                "config": cfg, "variants": variants, "clocks": clk, "e2e": e2e,
                 "gpu_launches": launches_in_run(args.steps, rebuilds, per_rebuild, persistent_active), "rebuilds": rebuilds,
                 "roofline": roofline}
         line.update(extra)

@@ -118,9 +118,15 @@ typedef struct {
 B2MD_API int b2md_engine_create(int device, long long max_particles, int max_replicas,
                        long long max_list_entries, int pb, int tp, b2md_engine** out);
 B2MD_API int b2md_engine_destroy(b2md_engine* e);
-/* Sample::SetPB_TP (Sample.h:96).  tp in {1,2,4,8}; pb a multiple of 32;
- * pb*tp <= 512. */
+/* Sample::SetPB_TP (Sample.h:96).  Accepts RUMD's shapes (pb 1..1024, tp
+ * 1..64; Autotune.py:156-158 tries pb 16..192 and tp up to 64) and maps them
+ * onto the engine's: pb rounded up to a multiple of 32 (at most 512), tp the
+ * largest of 1, 2, 4, 8 not above the request, halved until pb*tp <= 512.
+ * The same mapping applies to b2md_engine_create. */
 B2MD_API int b2md_engine_set_launch(b2md_engine* e, int pb, int tp);
+/* The launch shape in effect after that mapping (Sample::GetKernelPlan,
+ * Sample.h:160-163). */
+B2MD_API int b2md_engine_get_launch(b2md_engine* e, int* pb, int* tp);
 /* Device bytes currently allocated by the engine. */
 B2MD_API int b2md_engine_memory(b2md_engine* e, long long* bytes);
 /* Chooses CUDA-graph conditional rebuild nodes (1, default) or unconditional
@@ -189,6 +195,11 @@ B2MD_API int b2md_replica_remove(b2md_engine* e, int id);
 /* Copies a field out in original order (ParticleData::Copy*FromDevice,
  * ParticleData.cu:383-470).  out: n*4 floats, or n*3 ints for images. */
 B2MD_API int b2md_replica_get(b2md_engine* e, int id, int field, void* out);
+/* Positions, velocities and images together, in original order, with one
+ * read of the sort permutation (ParticleData::CopyPosFromDevice +
+ * CopyVelFromDevice, ParticleData.cu:383-420).  Any output may be NULL:
+ * pos4 and vel4 n*4 floats, im3 n*3 ints. */
+B2MD_API int b2md_replica_read(b2md_engine* e, int id, float* pos4, float* vel4, int* im3);
 /* Replaces positions, velocities or images (ParticleData::CopyPosToDevice
  * with reset_sorting, ParticleData.cu:333-355).  Setting positions forces a
  * neighbour-list rebuild before the next force evaluation. */
@@ -289,7 +300,10 @@ B2MD_API int b2md_probe_cell(const float* x, int n, float box, int nc, int* out)
  * call, so calls that overlap on the GPU race; order them on one stream.  The
  * first call on each device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. */
+ * before any stream capture.  A later call in another CUDA context of the
+ * device (after cudaDeviceReset, say) looks it up again.  Every cut-off must
+ * be at most half of every box length (the minimum-image sum counts one
+ * image per pair); larger ones return B2MD_ERR_ARG. */
 B2MD_API int b2md_forces_noalloc(const float* pos4, int n, const float* box, int ntypes, const float* params,
                                  int cutoff_method, float* force4, double* sums, void* stream);
 

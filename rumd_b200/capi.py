@@ -29,9 +29,10 @@ NSTAT = len(STAT_NAMES)
 NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
 
 EXPORTS = [
-    "b2md_engine_create", "b2md_engine_destroy", "b2md_engine_set_launch", "b2md_engine_memory",
+    "b2md_engine_create", "b2md_engine_destroy", "b2md_engine_set_launch", "b2md_engine_get_launch",
+    "b2md_engine_memory",
     "b2md_engine_set_graph_mode", "b2md_engine_set_variant", "b2md_engine_get_variant", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
-    "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_set_integrator",
+    "b2md_replica_read", "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_set_integrator",
     "b2md_replica_set_xi", "b2md_replica_set_reset_interval", "b2md_replica_set_nb_method",
     "b2md_replica_stats", "b2md_replica_set_energy_log", "b2md_replica_energy_log", "b2md_replica_stress", "b2md_calc_f",
     "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
@@ -71,6 +72,7 @@ def lib():
             "b2md_engine_create": [i, ll, i, ll, i, i, ctypes.POINTER(P)],
             "b2md_engine_destroy": [P],
             "b2md_engine_set_launch": [P, i, i],
+            "b2md_engine_get_launch": [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
             "b2md_engine_memory": [P, ctypes.POINTER(ll)],
             "b2md_engine_set_graph_mode": [P, i],
             "b2md_engine_set_variant": [P, i, i],
@@ -78,6 +80,7 @@ def lib():
             "b2md_replica_add": [P, ctypes.POINTER(ReplicaDesc), P, P, P, ctypes.POINTER(i)],
             "b2md_replica_remove": [P, i],
             "b2md_replica_get": [P, i, i, P],
+            "b2md_replica_read": [P, i, P, P, P],
             "b2md_replica_set": [P, i, i, P],
             "b2md_replica_set_potential": [P, i, i, P, i, f, i],
             "b2md_replica_set_integrator": [P, i, f, d, d, d, u],
@@ -168,7 +171,7 @@ class Engine:
         check(lib().b2md_engine_create(device, max_particles, max_replicas, max_list_entries, pb, tp,
                                        ctypes.byref(h)))
         self._h = h
-        self.pb, self.tp = pb, tp
+        self.pb, self.tp = self.launch()
 
     def close(self):
         if getattr(self, "_h", None):
@@ -186,8 +189,15 @@ class Engine:
         return self._h
 
     def set_launch(self, pb, tp):
+        """Sets (pb, tp); RUMD's shapes are mapped onto the engine's (see launch())."""
         check(lib().b2md_engine_set_launch(self._h, pb, tp))
-        self.pb, self.tp = pb, tp
+        self.pb, self.tp = self.launch()
+
+    def launch(self):
+        """The (pb, tp) in effect after the engine's mapping of the requested shape."""
+        p, t = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().b2md_engine_get_launch(self._h, ctypes.byref(p), ctypes.byref(t)))
+        return p.value, t.value
 
     def set_graph_mode(self, conditional):
         check(lib().b2md_engine_set_graph_mode(self._h, int(bool(conditional))))
@@ -243,6 +253,14 @@ class Engine:
             out = np.zeros((n, 4), np.float32)
         check(lib().b2md_replica_get(self._h, rid, FIELD[field], _ptr(out)))
         return out
+
+    def read(self, rid, n, pos=True, vel=True, images=True):
+        """Positions, velocities and images in original order, one id read-back."""
+        p = np.zeros((n, 4), np.float32) if pos else None
+        v = np.zeros((n, 4), np.float32) if vel else None
+        im = np.zeros((n, 3), np.int32) if images else None
+        check(lib().b2md_replica_read(self._h, rid, _ptr(p), _ptr(v), _ptr(im)))
+        return p, v, im
 
     def set(self, rid, field, arr):
         dt = np.int32 if field == "images" else np.float32

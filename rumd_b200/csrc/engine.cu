@@ -141,6 +141,8 @@ struct b2md_engine {
   bool persist_on = false;     // the current graphs are the persistent ones
   PersistCtl* pctl = nullptr;  // k_steps control block
   int* h_budget = nullptr;     // pinned: the step budget written before each persistent launch
+  void* h_stage = nullptr;     // pinned staging for particle uploads and read-backs (grown on demand)
+  size_t h_stage_bytes = 0;
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
   float4* r[2] = {nullptr, nullptr};
   float4* v[2] = {nullptr, nullptr};
@@ -194,6 +196,33 @@ void dev_grow(b2md_engine* e, T*& p, long long old_n, long long new_n, bool zero
     CK(cudaFree(p));
   }
   p = np;
+}
+
+// Pinned host staging of at least `bytes` (kept for the engine's life), so
+// that particle uploads and read-backs are DMA copies.
+void* host_stage(b2md_engine* e, size_t bytes) {
+  if (bytes > e->h_stage_bytes) {
+    if (e->h_stage) {
+      CK(cudaStreamSynchronize(e->stream));
+      CK(cudaFreeHost(e->h_stage));
+      e->h_stage = nullptr;
+      e->h_stage_bytes = 0;
+    }
+    const size_t b = std::max(bytes, (size_t)1 << 20);
+    CK(cudaMallocHost(&e->h_stage, b));
+    e->h_stage_bytes = b;
+  }
+  return e->h_stage;
+}
+
+// Page-locked host memory (cudaMallocHost / cudaHostRegister): DMA-able as is.
+bool is_pinned(const void* p) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeHost;
 }
 
 void invalidate_graphs(b2md_engine* e) {
@@ -978,6 +1007,24 @@ int guarded(F&& fn) {
   }
 }
 
+// RUMD's launch shapes mapped onto the engine's: tiles are whole warps (pb
+// rounded up to a multiple of 32, at most 512) and tp is a power of two up
+// to 8 (the largest one <= the request), halved until pb * tp <= 512.  RUMD's
+// autotuner tries pb in {16, 32, 48, 64, 96, 128, 192} and tp up to 64
+// (Autotune.py:156-158); e.g. (16, 4) -> (32, 4), (48, 1) -> (64, 1),
+// (192, 8) -> (192, 2), (64, 64) -> (64, 8).  False for pb < 1 or tp < 1 or
+// sizes far outside those ranges.
+bool map_launch(int pb, int tp, int* pb_out, int* tp_out) {
+  if (pb < 1 || pb > 1024 || tp < 1 || tp > 64) return false;
+  int p = std::min((pb + 31) / 32 * 32, kMaxBlock);
+  int t = 8;
+  while (t > tp) t >>= 1;
+  while (t > 1 && p * t > kMaxBlock) t >>= 1;
+  *pb_out = p;
+  *tp_out = t;
+  return true;
+}
+
 void launch_momentum(b2md_engine* e) {
   if (e->ntiles == 0) return;
   EngArgs a = make_args(e);
@@ -1005,8 +1052,7 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
                        int pb, int tp, b2md_engine** out) {
   if (!out) return fail(B2MD_ERR_ARG, "out is null");
   *out = nullptr;
-  if (tp != 1 && tp != 2 && tp != 4 && tp != 8) return fail(B2MD_ERR_ARG, "tp must be 1, 2, 4 or 8");
-  if (pb < 32 || pb % 32 || pb * tp > kMaxBlock) return fail(B2MD_ERR_ARG, "pb must be a multiple of 32 with pb*tp <= 512");
+  if (!map_launch(pb, tp, &pb, &tp)) return fail(B2MD_ERR_ARG, "pb must be 1..1024 and tp 1..64 (got %d, %d)", pb, tp);
   b2md_engine* e = new b2md_engine();
   int rc = guarded([&] {
     CK(cudaSetDevice(device));
@@ -1061,6 +1107,7 @@ int b2md_engine_destroy(b2md_engine* e) {
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->h_budget) cudaFreeHost(e->h_budget);
+  if (e->h_stage) cudaFreeHost(e->h_stage);
   if (e->stream) cudaStreamDestroy(e->stream);
   if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
   delete e;
@@ -1069,8 +1116,7 @@ int b2md_engine_destroy(b2md_engine* e) {
 
 int b2md_engine_set_launch(b2md_engine* e, int pb, int tp) {
   if (!e) return fail(B2MD_ERR_ARG, "null engine");
-  if (tp != 1 && tp != 2 && tp != 4 && tp != 8) return fail(B2MD_ERR_ARG, "tp must be 1, 2, 4 or 8");
-  if (pb < 32 || pb % 32 || pb * tp > kMaxBlock) return fail(B2MD_ERR_ARG, "pb must be a multiple of 32 with pb*tp <= 512");
+  if (!map_launch(pb, tp, &pb, &tp)) return fail(B2MD_ERR_ARG, "pb must be 1..1024 and tp 1..64 (got %d, %d)", pb, tp);
   return guarded([&] {
     CK(cudaSetDevice(e->device));
     CK(cudaStreamSynchronize(e->stream));
@@ -1078,6 +1124,13 @@ int b2md_engine_set_launch(b2md_engine* e, int pb, int tp) {
     e->tp = tp;
     relayout(e);
   });
+}
+
+int b2md_engine_get_launch(b2md_engine* e, int* pb, int* tp) {
+  if (!e || !pb || !tp) return fail(B2MD_ERR_ARG, "null argument");
+  *pb = e->pb;
+  *tp = e->tp;
+  return B2MD_OK;
 }
 
 int b2md_engine_memory(b2md_engine* e, long long* bytes) {
@@ -1229,22 +1282,38 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
       h.d.energy_cap = 0;
     }
     h.active = true;
-    // upload particle data (slot order = original order until the first sort)
-    std::vector<int4> imv(h.n);
-    std::vector<unsigned> ids(h.n);
-    std::vector<float4> vv(h.n);
-    for (int i = 0; i < h.n; ++i) {
-      imv[i] = im3 ? make_int4(im3[3 * i], im3[3 * i + 1], im3[3 * i + 2], 0) : make_int4(0, 0, 0, 0);
-      ids[i] = (unsigned)i;
-      vv[i] = vel4 ? make_float4(vel4[4 * i], vel4[4 * i + 1], vel4[4 * i + 2], vel4[4 * i + 3])
-                   : make_float4(0.f, 0.f, 0.f, 1.f);
-      if (!(vv[i].w > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass (vel4[.,3]) must be positive");
+    // upload particle data (slot order = original order until the first
+    // sort): one pinned staging area holds r, v and the images as the device
+    // stores them, so each is one DMA copy; last_r and the ids are made on
+    // the device
+    if (vel4)
+      for (int i = 0; i < h.n; ++i)
+        if (!(vel4[4 * i + 3] > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass (vel4[.,3]) must be positive");
+    const size_t nb = (size_t)h.n * sizeof(float4);
+    char* stage = static_cast<char*>(host_stage(e, 3 * nb));
+    const float4* sr = reinterpret_cast<const float4*>(pos4);
+    const float4* sv = reinterpret_cast<const float4*>(vel4);
+    int4* si = reinterpret_cast<int4*>(stage + 2 * nb);
+    // arrays the caller already pinned are copied from directly
+    if (!is_pinned(pos4)) {
+      std::memcpy(stage, pos4, nb);
+      sr = reinterpret_cast<const float4*>(stage);
     }
-    CK(cudaMemcpyAsync(e->r[0] + p0, pos4, h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
-    CK(cudaMemcpyAsync(e->last_r + p0, pos4, h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
-    CK(cudaMemcpyAsync(e->v[0] + p0, vv.data(), h.n * sizeof(float4), cudaMemcpyHostToDevice, e->stream));
-    CK(cudaMemcpyAsync(e->im[0] + p0, imv.data(), h.n * sizeof(int4), cudaMemcpyHostToDevice, e->stream));
-    CK(cudaMemcpyAsync(e->uidx[0] + p0, ids.data(), h.n * sizeof(unsigned), cudaMemcpyHostToDevice, e->stream));
+    if (!vel4 || !is_pinned(vel4)) {
+      float4* v = reinterpret_cast<float4*>(stage + nb);
+      if (vel4) std::memcpy(v, vel4, nb);
+      else
+        for (int i = 0; i < h.n; ++i) v[i] = make_float4(0.f, 0.f, 0.f, 1.f);
+      sv = v;
+    }
+    for (int i = 0; i < h.n; ++i)
+      si[i] = im3 ? make_int4(im3[3 * i], im3[3 * i + 1], im3[3 * i + 2], 0) : make_int4(0, 0, 0, 0);
+    CK(cudaMemcpyAsync(e->r[0] + p0, sr, nb, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->v[0] + p0, sv, nb, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->im[0] + p0, si, nb, cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->last_r + p0, e->r[0] + p0, nb, cudaMemcpyDeviceToDevice, e->stream));
+    k_iota<<<(h.n + 255) / 256, 256, 0, e->stream>>>(e->uidx[0] + p0, h.n);
+    check_launch();
     CK(cudaMemsetAsync(e->f + p0, 0, h.np * sizeof(float4), e->stream));
     CK(cudaMemsetAsync(e->w + p0, 0, h.np * sizeof(float4), e->stream));
     CK(cudaMemsetAsync(e->sts + p0, 0, h.np * sizeof(float4), e->stream));
@@ -1312,6 +1381,37 @@ int b2md_replica_get(b2md_engine* e, int id, int field, void* out) {
     CK(cudaStreamSynchronize(e->stream));
     float4* o = static_cast<float4*>(out);
     for (int k = 0; k < h.n; ++k) o[ids[k]] = tmp[k];
+  });
+}
+
+int b2md_replica_read(b2md_engine* e, int id, float* pos4, float* vel4, int* im3) {
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    RepState s = read_state(e, id);
+    const size_t n = (size_t)h.n;
+    char* stage = static_cast<char*>(host_stage(e, n * (sizeof(unsigned) + 3 * sizeof(float4))));
+    unsigned* ids = reinterpret_cast<unsigned*>(stage);
+    float4* sr = reinterpret_cast<float4*>(stage + ((n * sizeof(unsigned) + 15) & ~(size_t)15));
+    float4* sv = sr + n;
+    int4* si = reinterpret_cast<int4*>(sv + n);
+    CK(cudaMemcpyAsync(ids, e->uidx[s.abuf] + h.p0, n * sizeof(unsigned), cudaMemcpyDeviceToHost, e->stream));
+    if (pos4) CK(cudaMemcpyAsync(sr, e->r[s.rbuf] + h.p0, n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    if (vel4) CK(cudaMemcpyAsync(sv, e->v[s.abuf] + h.p0, n * sizeof(float4), cudaMemcpyDeviceToHost, e->stream));
+    if (im3) CK(cudaMemcpyAsync(si, e->im[s.abuf] + h.p0, n * sizeof(int4), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaStreamSynchronize(e->stream));
+    float4* po = reinterpret_cast<float4*>(pos4);
+    float4* vo = reinterpret_cast<float4*>(vel4);
+    for (size_t k = 0; k < n; ++k) {
+      const unsigned i = ids[k];
+      if (pos4) po[i] = sr[k];
+      if (vel4) vo[i] = sv[k];
+      if (im3) {
+        im3[3 * (size_t)i] = si[k].x;
+        im3[3 * (size_t)i + 1] = si[k].y;
+        im3[3 * (size_t)i + 2] = si[k].z;
+      }
+    }
   });
 }
 

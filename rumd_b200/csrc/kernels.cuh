@@ -1345,6 +1345,12 @@ __global__ void k_apply_zero_momentum(EngArgs a) {
   a.v[S->abuf][gi] = v;
 }
 
+// Original particle ids 0..n-1 (a replica's slot order before its first sort).
+__global__ void k_iota(unsigned* ids, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) ids[i] = (unsigned)i;
+}
+
 // Sets the queued step counts of all replicas (lock-step run start).
 __global__ void k_set_steps(EngArgs a, long long nsteps, int reset_run_step) {
   const int rep = blockIdx.x * blockDim.x + threadIdx.x;

@@ -17,9 +17,22 @@
 // one stream or with events.  The completion counter is cleared at the start
 // of every call; the partial sums are overwritten before they are read.
 //
+// Host code cannot use the array's name as a device address (it names a
+// host-side stand-in).  The first call on a device, with that device current,
+// looks the address up with cudaGetSymbolAddress and keeps it together with
+// the device's current CUDA context; a later call in another context (after
+// cudaDeviceReset, say, which unloads the module and so moves the array)
+// looks it up again.  Make the first call on a device before any stream
+// capture, since the lookup is not a stream operation.
+//
+// The pair sum uses the minimum-image convention, which counts each pair once;
+// that equals the periodic sum only while every cut-off is at most half of
+// every box length, so larger cut-offs are rejected.
+//
 // Its results match b2md_calc_f for the same configuration: the same pair
 // function (shifted-force / shifted-potential / plain LJ), all pairs within
 // the cut-off under the minimum-image convention, per-particle energies halved.
+#include <cstdio>
 #include <mutex>
 
 #include "../../include/rumd_b200.h"
@@ -45,9 +58,11 @@ struct PairTable {
   float p[kNoAllocMaxTypes * kNoAllocMaxTypes * kRow];
 };
 
-// Device address of g_noalloc_scratch per device, looked up once per device.
+// Device address of g_noalloc_scratch per device, looked up once per device
+// and context (the context the address was found in is kept beside it).
 std::mutex g_mu;
 NoAllocScratch* g_scratch_ptr[64] = {};
+void* g_scratch_ctx[64] = {};
 
 __global__ void __launch_bounds__(kNoAllocBlock)
     k_forces_noalloc(const float4* __restrict__ pos, int n, float3 L, float3 iL, int ntypes, PairTable tab,
@@ -136,22 +151,45 @@ __global__ void __launch_bounds__(kNoAllocBlock)
   }
 }
 
-// Looks up (once per device, with that device current) the device address of
-// the scratch array; host code may not use the symbol itself as a pointer.
+// The current CUDA context (driver call cuCtxGetCurrent, fetched through the
+// runtime so that the library needs no link to the driver library); null
+// when it cannot be read.
+void* current_context() {
+  typedef int (*CtxGetCurrent)(void**);
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
+
+// Looks up (once per device and context, with that device current) the
+// device address of the scratch array; host code may not use the symbol
+// itself as a pointer.
 NoAllocScratch* scratch_for_current_device(int* err) {
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
     *err = B2MD_ERR_CUDA;
     return nullptr;
   }
+  void* ctx = current_context();
   std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_scratch_ptr[dev]) {
+  if (!g_scratch_ptr[dev] || !ctx || ctx != g_scratch_ctx[dev]) {
+    // the lookup also makes the device's primary context current on this
+    // thread when none was, so the context is read again after it
     NoAllocScratch* p = nullptr;
     if (cudaGetSymbolAddress((void**)&p, g_noalloc_scratch) != cudaSuccess || !p) {
       *err = B2MD_ERR_CUDA;
       return nullptr;
     }
     g_scratch_ptr[dev] = p;
+    g_scratch_ctx[dev] = current_context();
   }
   return g_scratch_ptr[dev];
 }
@@ -180,6 +218,20 @@ extern "C" int b2md_forces_noalloc(const float* pos4, int n, const float* box, i
     return noalloc_fail(B2MD_ERR_ARG, "b2md_forces_noalloc: cutoff method must be NS, SP or SF");
   if (!(box[0] > 0.f) || !(box[1] > 0.f) || !(box[2] > 0.f))
     return noalloc_fail(B2MD_ERR_ARG, "b2md_forces_noalloc: box lengths must be positive");
+  // minimum image counts one image per pair: exact only for rc <= L/2
+  float rcmax = 0.f;
+  for (int k = 0; k < ntypes * ntypes; ++k) rcmax = params[k * 12] > rcmax ? params[k * 12] : rcmax;
+  const float lmin = fminf(box[0], fminf(box[1], box[2]));
+  if (rcmax > 0.5f * lmin) {
+    char msg[200];
+    snprintf(msg, sizeof(msg),
+             "b2md_forces_noalloc: cut-off %g exceeds half the smallest box length %g (the minimum-image sum "
+             "would miss periodic images)", (double)rcmax, (double)lmin);
+    return noalloc_fail(B2MD_ERR_ARG, msg);
+  }
+  // an error left by an earlier runtime call on this thread is not this
+  // call's: clear it so that the launch check below sees only this launch
+  (void)cudaGetLastError();
   int err = B2MD_OK;
   NoAllocScratch* scr = scratch_for_current_device(&err);
   if (!scr) return noalloc_fail(err, "b2md_forces_noalloc: cannot find the device address of the scratch array");
@@ -199,13 +251,24 @@ extern "C" int b2md_forces_noalloc(const float* pos4, int n, const float* box, i
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // the completion counter must start at zero for every call
-  if (cudaMemsetAsync(&scr->counter, 0, sizeof(unsigned), s) != cudaSuccess)
-    return noalloc_fail(B2MD_ERR_CUDA, "b2md_forces_noalloc: clearing the scratch counter failed");
+  const cudaError_t me = cudaMemsetAsync(&scr->counter, 0, sizeof(unsigned), s);
+  if (me != cudaSuccess) {
+    char msg[200];
+    snprintf(msg, sizeof(msg), "b2md_forces_noalloc: clearing the scratch counter failed: %s",
+             cudaGetErrorName(me));
+    return noalloc_fail(B2MD_ERR_CUDA, msg);
+  }
   const float3 L = make_float3(box[0], box[1], box[2]);
   const float3 iL = make_float3(1.f / box[0], 1.f / box[1], 1.f / box[2]);
   const int blocks = (n + kNoAllocBlock - 1) / kNoAllocBlock;
   k_forces_noalloc<<<blocks, kNoAllocBlock, 0, s>>>(reinterpret_cast<const float4*>(pos4), n, L, iL, ntypes, tab,
                                                      reinterpret_cast<float4*>(force4), sums, scr);
-  if (cudaGetLastError() != cudaSuccess) return noalloc_fail(B2MD_ERR_CUDA, "b2md_forces_noalloc: launch failed");
+  const cudaError_t le = cudaGetLastError();
+  if (le != cudaSuccess) {
+    char msg[200];
+    snprintf(msg, sizeof(msg), "b2md_forces_noalloc: launch failed: %s (%s)", cudaGetErrorName(le),
+             cudaGetErrorString(le));
+    return noalloc_fail(B2MD_ERR_CUDA, msg);
+  }
   return B2MD_OK;
 }

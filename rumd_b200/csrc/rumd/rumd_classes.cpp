@@ -339,17 +339,30 @@ void Sample::ChooseLaunch() {
   // Defaults by size, as Sample(pb=0, tp=0) does (Sample.cu:208-215), with
   // B200 shapes: tp = 4 threads per particle, 64 particles per block.
   unsigned n = GetNumberOfParticles();
+  // RUMD's shapes (pb 16..192, tp up to 64) are accepted; the engine maps
+  // them onto whole-warp tiles and tp in {1, 2, 4, 8} (b2md_engine_set_launch)
+  // and GetParticlesPerBlock / GetThreadsPerParticle report what it runs.
   pb = user_pb ? user_pb : (n > 10000 ? 64 : 32);
   tp = user_tp ? user_tp : 4;
-  if (pb % 32 || pb * tp > 512 || (tp != 1 && tp != 2 && tp != 4 && tp != 8))
-    throw RUMD_cudaResourceError("Sample", "SetPB_TP", "pb must be a multiple of 32, tp in {1,2,4,8}, pb*tp <= 512");
+  if (pb < 1 || pb > 1024 || tp < 1 || tp > 64)
+    throw RUMD_cudaResourceError("Sample", "SetPB_TP", "pb must be 1..1024 and tp 1..64");
+}
+
+void Sample::SyncLaunch() {
+  int p = 0, t = 0;
+  Check(b2md_engine_get_launch(eng, &p, &t), "GetKernelPlan");
+  pb = (unsigned)p;
+  tp = (unsigned)t;
 }
 
 void Sample::SetPB_TP(unsigned pb_, unsigned tp_) {
   user_pb = pb_;
   user_tp = tp_;
   ChooseLaunch();
-  if (eng) Check(b2md_engine_set_launch(eng, (int)pb, (int)tp), "SetPB_TP");
+  if (eng) {
+    Check(b2md_engine_set_launch(eng, (int)pb, (int)tp), "SetPB_TP");
+    SyncLaunch();
+  }
 }
 
 void Sample::SetConfiguration(const std::vector<float>& pos3, const std::vector<int>& types,
@@ -434,7 +447,10 @@ void Sample::EnsureReplica() {
   if (type.empty()) throw RUMD_Error("Sample", "CalcF", "No configuration has been read");
   if (!pot) throw RUMD_Error("Sample", "CalcF", "No potential has been set");
   ChooseLaunch();
-  if (!eng) Check(b2md_engine_create(0, (long long)type.size(), 1, 0, (int)pb, (int)tp, &eng), "Sample");
+  if (!eng) {
+    Check(b2md_engine_create(0, (long long)type.size(), 1, 0, (int)pb, (int)tp, &eng), "Sample");
+    SyncLaunch();
+  }
   std::vector<float> table = pot->ParamTable(GetNumberOfTypes());
   b2md_replica_desc d;
   std::memset(&d, 0, sizeof(d));

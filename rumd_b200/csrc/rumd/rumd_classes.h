@@ -259,6 +259,7 @@ class Sample {
   std::vector<float> GetBoxLengths() const { return box; }
   double GetVolume() const { return (double)box[0] * box[1] * box[2]; }
   void SetPB_TP(unsigned pb, unsigned tp);
+  // pb and tp in effect (after the engine's mapping of RUMD shapes)
   unsigned GetParticlesPerBlock() const { return pb; }
   unsigned GetThreadsPerParticle() const { return tp; }
   void SetVerbose(bool v) { verbose = v; }
@@ -291,6 +292,7 @@ class Sample {
   void ChooseLaunch();
 
   unsigned pb, tp, user_pb, user_tp;
+  void SyncLaunch();
   b2md_engine* eng = nullptr;
   int rid = -1;
   std::vector<float> pos, vel, box, mass;  // host copies until the replica exists

@@ -10,7 +10,7 @@ reference's golden vectors for the pair force path.  This script parses them
 line 173) and stores compact ``.npz`` fixtures so that the tests do not need
 the reference tree.
 
-Usage:  python tests/golden/make_golden.py [RUMD_SOURCE_TREE]
+Usage:  python tests/golden/make_golden.py RUMD_SOURCE_TREE
 """
 import gzip
 import os
@@ -64,7 +64,9 @@ def parse(path):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py RUMD_SOURCE_TREE")
+    root = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     for name in FILES:
         d = parse(os.path.join(root, "Conf", "KobAndersen", name))

@@ -39,10 +39,12 @@ def test_error_reporting_without_gpu():
     from rumd_b200 import capi
     lib = capi.lib()
     h = ctypes.c_void_p()
-    rc = lib.b2md_engine_create(0, 0, 1, 0, 48, 4, ctypes.byref(h))  # pb not a multiple of 32
+    # RUMD's shapes (pb 16..192, tp up to 64) are mapped, not refused; only
+    # shapes outside pb 1..1024, tp 1..64 are rejected
+    rc = lib.b2md_engine_create(0, 0, 1, 0, 0, 4, ctypes.byref(h))
     assert rc == capi.B2MD_ERR_ARG
     assert b"pb" in lib.b2md_last_error()
-    rc = lib.b2md_engine_create(0, 0, 1, 0, 64, 3, ctypes.byref(h))  # tp not a power of two
+    rc = lib.b2md_engine_create(0, 0, 1, 0, 64, 65, ctypes.byref(h))
     assert rc == capi.B2MD_ERR_ARG
     assert lib.b2md_version().startswith(b"rumd_b200")
     # a null engine is rejected before any device work

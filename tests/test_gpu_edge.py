@@ -91,3 +91,25 @@ def test_rejected_inputs(capi, oracle):
     with pytest.raises(Exception):
         e.stats(rid)  # removed replica
     e.close()
+
+
+@pytest.mark.parametrize("req,eff", [((16, 4), (32, 4)), ((48, 1), (64, 1)), ((96, 3), (96, 2)),
+                                     ((192, 8), (192, 2)), ((64, 64), (64, 8)), ((128, 16), (128, 4))])
+def test_rumd_launch_shapes_are_mapped(capi, oracle, req, eff):
+    """RUMD's autotuner shapes (pb 16..192, tp up to 64; Autotune.py:156-158)
+    run: pb becomes whole warps and tp one of 1, 2, 4, 8 with pb*tp <= 512,
+    and the forces meet the FP64 tolerance."""
+    from rumd_b200 import initconf as I
+    c = I.ka_config(2000, T=1.0, seed=9)
+    params = oracle.lj_params(2, oracle.ka_table())
+    e = capi.Engine(device=0, pb=req[0], tp=req[1])
+    assert e.launch() == eff
+    rid = e.add(c["pos4"], c["box"], params, 2, cutoff="SF")
+    e.calc_f()
+    f = e.get(rid, "force", 2000)
+    e.set_launch(64, 4)
+    e.set_launch(*req)
+    assert e.launch() == eff
+    e.close()
+    ref, _, _ = oracle.forces_f64(c["pos4"][:, :3].astype(np.float64), c["types"], c["box"], 2, params, 2)
+    assert rms_rel(f[:, :3].astype(np.float64), ref) < 1e-5

@@ -78,7 +78,7 @@ def test_errors_map_to_python_exceptions(rumd, tmp_path):
     with pytest.raises(RuntimeError):
         s.CalcF()  # no configuration
     with pytest.raises(ValueError):
-        s.SetPB_TP(48, 4)  # pb not a multiple of 32
+        s.SetPB_TP(2048, 4)  # beyond any launch shape (RUMD's 16..192 are mapped)
     pot = rumd.Pot_LJ_12_6(rumd.ShiftedForce)
     with pytest.raises(RuntimeError):
         pot.SetNB_Method("cells")
