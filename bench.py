@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--profile-batched", action="store_true",
                    help="the 256-replica batch only, eager launches of --steps steps between "
                         "cudaProfilerStart/Stop (for the ncu launch list)")
+    p.add_argument("--batched-only", action="store_true",
+                   help="only the 256-replica batch (one JSON line, not the headline)")
     p.add_argument("--lj1m", action="store_true",
                    help="only the HBM-scale plain workload: single-component LJ, N=1,048,576 (one JSON line)")
     return p.parse_args()
@@ -556,6 +558,10 @@ def main():
         return
     if args.profile_batched:
         profile_batched(capi, device, args)
+        dist.close()
+        return
+    if args.batched_only:
+        print(json.dumps({"batched": batched(capi, device, args.pb, args.tp, args.batch_steps)}), flush=True)
         dist.close()
         return
     if args.profile_launches:

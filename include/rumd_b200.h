@@ -145,11 +145,14 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *                                tile, made with the list -- copied to shared
  *                                memory (one TMA bulk copy per segment), with
  *                                a 16-bit list of window offsets.
- *   B2MD_VARIANT_BUILD_LANES   lanes per particle in the list build: 1,2,4,8;
- *                              32: one warp per cell, the cell's candidates
- *                              staged in shared memory and shared by its
- *                              particles (with force mode 2 the lane build
- *                              runs instead, with min(8, 512/pb) lanes).
+ *   B2MD_VARIANT_BUILD_LANES   the list build: 0 (default) one warp per
+ *                              cell, each lane testing a contiguous run of
+ *                              the cell's candidates against up to four of
+ *                              its particles at once; 1,2,4,8 lanes per
+ *                              particle; 32: one warp per cell, 32
+ *                              candidates per round staged in shared memory
+ *                              (with force mode 2 the lane build runs for 0
+ *                              and 32, with min(8, 512/pb) lanes).
  *   B2MD_VARIANT_BUILD_SMEM    1: the list build assembles a tile's list in
  *                              shared memory and writes it with bulk stores;
  *                              0: it stores entries straight to the list.
@@ -245,8 +248,12 @@ B2MD_API int b2md_zero_momentum(b2md_engine* e);
  * decided on the device; list overflow is repaired on the host (capacity
  * doubled, NeighborList.cu:657-676) and the run resumed. */
 B2MD_API int b2md_run(b2md_engine* e, long long nsteps);
-/* b2md_run with eager launches instead of graphs, for measurement: CUDA
- * events on the engine's stream bracket every fused step kernel, and the host
+/* b2md_run with eager launches instead of graphs, for measurement (a
+ * profiler can follow eager launches, not conditional graph nodes).  With the
+ * persistent step kernel in effect, the loop of the persistent graph runs
+ * from the host: the rebuild kernels, then one cooperative k_steps launch
+ * that runs steps until a rebuild is due; CUDA events bracket each k_steps
+ * launch.  Otherwise events bracket every fused step kernel and the host
  * reads the rebuild decision before each step (one small kernel and a 4-byte
  * copy), launching the rebuild kernels only when a list is due, as the step
  * graph's conditional node does.  Returns the summed step-kernel time and the
@@ -282,6 +289,12 @@ B2MD_API int b2md_probe_dist2(const float* a4, const float* b4, const float* box
 /* Same for the cell coordinate (int)(nc * (x / L + 0.5f)) of n coordinates:
  * out 2*n ints (reference expression, explicit form). */
 B2MD_API int b2md_probe_cell(const float* x, int n, float box, int nc, int* out);
+/* integrateNVTAlgorithm's velocity/position update and wrap as the reference
+ * source writes them (IntegratorNVT.cu:385-399, SimulationBox.h:140-155),
+ * compiled with default nvcc flags, next to the engine's explicit forms:
+ * ref9 / eng9 receive (v, r, image) per particle. */
+B2MD_API int b2md_probe_nvt(const float* r4, const float* v4, const float* f4, const float* xi, float dt,
+                            const float* box, int n, float* ref9, float* eng9);
 
 /* LJ forces, per-particle energies, total potential energy and virial of one
  * configuration, for callers that cannot allocate device memory during the

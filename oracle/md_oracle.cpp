@@ -343,9 +343,23 @@ static void pair_f64(int kind, double d2, const float* p, double* s, double* u) 
 // Uses a cell list with cells >= max cutoff, or all pairs for small boxes.
 // The cut-off terms (fij, PairPotential.h:1208-1221) use s(rc), u(rc) of the
 // same pair function in double.
+// The same sum with the per-particle stress of fij's STR branch
+// (PairPotential.h:1232-1241): sts6[6 i + (xx, yy, zz, yz, xz, xy)] =
+// -sum_j d_a d_b s over the pairs within the cut-off (RUMD keeps xx, yy, zz,
+// yz in sts and xz, xy in w.y, w.z).  sts6 may be null.
+ORC_API void orc_forces_stress_f64_pot(int n, const double* pos3, const int* type, const double* L,
+                                       int ntypes, const float* params, int cutoff, int potential,
+                                       double* f3, double* u, double* w, double* sts6);
+
 ORC_API void orc_forces_f64_pot(int n, const double* pos3, const int* type, const double* L,
                                 int ntypes, const float* params, int cutoff, int potential,
                                 double* f3, double* u, double* w) {
+  orc_forces_stress_f64_pot(n, pos3, type, L, ntypes, params, cutoff, potential, f3, u, w, nullptr);
+}
+
+ORC_API void orc_forces_stress_f64_pot(int n, const double* pos3, const int* type, const double* L,
+                                       int ntypes, const float* params, int cutoff, int potential,
+                                       double* f3, double* u, double* w, double* sts6) {
   double invL[3] = {1. / L[0], 1. / L[1], 1. / L[2]};
   double maxc = 0;
   for (int k = 0; k < ntypes * ntypes; ++k) maxc = std::max(maxc, (double)params[k * NP]);
@@ -377,6 +391,7 @@ ORC_API void orc_forces_f64_pot(int n, const double* pos3, const int* type, cons
 #pragma omp parallel for schedule(dynamic, 64)
   for (int i = 0; i < n; ++i) {
     double fx = 0, fy = 0, fz = 0, ui = 0, wi = 0;
+    double sxx = 0, syy = 0, szz = 0, syz = 0, sxz = 0, sxy = 0;
     auto pair = [&](int j) {
       if (j == i) return;
       double dx = pos3[3 * i] - pos3[3 * j];
@@ -404,6 +419,8 @@ ORC_API void orc_forces_f64_pot(int n, const double* pos3, const int* type, cons
         }
         fx += dx * s; fy += dy * s; fz += dz * s;
         ui += uu; wi += d2 * s;
+        sxx -= dx * dx * s; syy -= dy * dy * s; szz -= dz * dz * s;
+        syz -= dy * dz * s; sxz -= dx * dz * s; sxy -= dx * dy * s;
       }
     };
     if (use_cells) {
@@ -420,6 +437,10 @@ ORC_API void orc_forces_f64_pot(int n, const double* pos3, const int* type, cons
     }
     f3[3 * i] = fx; f3[3 * i + 1] = fy; f3[3 * i + 2] = fz;
     u[i] = 0.5 * ui; w[i] = wi;
+    if (sts6) {
+      double* o = sts6 + 6 * (size_t)i;
+      o[0] = sxx; o[1] = syy; o[2] = szz; o[3] = syz; o[4] = sxz; o[5] = sxy;
+    }
   }
 }
 
@@ -701,9 +722,15 @@ static int md_run(int n, float* pos4, float* vel4, int* im3, const float* L, int
     }
     md_forces(S);
     double pe = 0, W = 0, ke_t = 0, ke2 = 0;
-    R factor = thermostat_on ? (R)(0.5f * (float)xi * dt) : R(0);
-    if (sizeof(R) == 8 && thermostat_on) factor = (R)(0.5 * xi * (double)dt);
+    R factor = thermostat_on ? (R)(0.5 * xi * (double)dt) : R(0);
     R plus = R(1) / (R(1) + factor), minus = R(1) - factor;
+    if (sizeof(R) == 4) {
+      // as the device build contracts it: factor = (xi/2) dt is fused into
+      // both sums, plus = 1 / fma(xi/2, dt, 1), minus = fma(-xi/2, dt, 1)
+      const float h = thermostat_on ? 0.5f * (float)xi : 0.f;
+      plus = (R)(1.f / std::fmaf(h, dt, 1.f));
+      minus = (R)std::fmaf(-h, dt, 1.f);
+    }
 #pragma omp parallel for schedule(static) reduction(+ : pe, W, ke_t, ke2)
     for (int i = 0; i < n; ++i) {
       pe += (double)S.u[i];
@@ -715,9 +742,9 @@ static int md_run(int n, float* pos4, float* vel4, int* im3, const float* L, int
         R vn, x, k;
         if (sizeof(R) == 4) {
           // integrateNVTAlgorithm as the device build contracts it:
-          // v = plus*fma(minus, v, (1/m * f) * dt);  r = fma(v, dt, r)
-          float t = ((float)im_ * (float)S.f[3 * i + d]) * dt;
-          vn = (R)((float)plus * std::fmaf((float)minus, (float)vo, t));
+          // v = plus * fma((1/m) f, dt, minus v);  r = fma(v, dt, r)
+          const float mf = (float)im_ * (float)S.f[3 * i + d];
+          vn = (R)((float)plus * std::fmaf(mf, dt, (float)minus * (float)vo));
           x = (R)std::fmaf((float)vn, dt, (float)S.r[3 * i + d]);
           k = (R)std::rintf((float)x * (float)S.invL[d]);
           x = (R)std::fmaf(-(float)S.L[d], (float)k, (float)x);

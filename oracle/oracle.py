@@ -49,6 +49,7 @@ def lib():
         L.orc_max_nbrs_estimate.restype = u
         L.orc_forces_f64.argtypes = [i, P, P, P, i, P, i, P, P, P]
         L.orc_forces_f64_pot.argtypes = [i, P, P, P, i, P, i, i, P, P, P]
+        L.orc_forces_stress_f64_pot.argtypes = [i, P, P, P, i, P, i, i, P, P, P, P]
         L.orc_smooth_set_params.argtypes = [i, P, i, i, f, f, f]
         L.orc_ipl_n_set_params.argtypes = [i, P, i, i, f, f, f, f]
         L.orc_forces_f32.argtypes = [i, P, P, i, P, i, P, P, i, P, P]
@@ -177,6 +178,33 @@ def forces_f64(pos3, types, L, ntypes, params, cutoff, potential="LJ_12_6"):
     lib().orc_forces_f64_pot(n, _p(pos3), _p(types), _p(np.asarray(L, np.float64)), ntypes,
                              _p(params), cutoff, POTENTIAL[potential], _p(f), _p(u), _p(w))
     return f, u, w
+
+
+def stress_f64(pos3, types, L, ntypes, params, cutoff, potential="LJ_12_6"):
+    """FP64 per-particle pair stress of fij's STR branch (PairPotential.h:1232-1241):
+    [n, 6] = (xx, yy, zz, yz, xz, xy), each -sum_j d_a d_b s."""
+    pos3 = np.ascontiguousarray(pos3, np.float64)
+    types = np.ascontiguousarray(types, np.int32)
+    n = len(pos3)
+    f = np.zeros((n, 3)); u = np.zeros(n); w = np.zeros(n); sts = np.zeros((n, 6))
+    lib().orc_forces_stress_f64_pot(n, _p(pos3), _p(types), _p(np.asarray(L, np.float64)), ntypes,
+                                    _p(params), cutoff, POTENTIAL[potential], _p(f), _p(u), _p(w), _p(sts))
+    return sts
+
+
+def sample_stress(sts6, vel4, L, include_kinetic=True):
+    """Sample::GetStress (Sample.cu:393-444): 0.5 * (sum of the particles'
+    pair stresses, minus 2 m v_a v_b per particle when the kinetic part is
+    included) / V, in FP64, order (xx, yy, zz, yz, xz, xy)."""
+    st = np.asarray(sts6, np.float64).sum(axis=0)
+    if include_kinetic:
+        v = np.asarray(vel4, np.float64)
+        m2 = 2.0 / v[:, 3]
+        vx, vy, vz = v[:, 0], v[:, 1], v[:, 2]
+        st = st - np.array([(m2 * vx * vx).sum(), (m2 * vy * vy).sum(), (m2 * vz * vz).sum(),
+                            (m2 * vy * vz).sum(), (m2 * vx * vz).sum(), (m2 * vx * vy).sum()])
+    V = float(np.prod(np.asarray(L, np.float64)))
+    return 0.5 * st / V
 
 
 def forces_f32(pos4, L, ntypes, params, cutoff, counts, nbl):

@@ -10,8 +10,8 @@ knobs are the engine's:
 and, in a second stage at the winning shape, the kernel variants
   force_mode    neighbours streamed (0), list tile staged (1) or position
                 window staged (2) in shared memory
-  build_lanes   lanes per particle in the list build: 1, 2, 4, 8, or 32 (one
-                warp per cell)
+  build_lanes   lanes per particle in the list build: 0 (row scan, one thread
+                per particle), 1, 2, 4, 8, or 32 (one warp per cell)
   sm_tiles      streamed mode: blocks claim tiles from their SM's region (1)
                 or one block per tile (0)
   persistent    streamed mode, one block per tile: the steps between list
@@ -34,7 +34,7 @@ VARIANT_KEYS = ("force_mode", "build_lanes", "sm_tiles", "persistent")
 # kernel-variant candidates: (force_mode, sm_tiles, persistent) x build_lanes
 VARIANTS = tuple(dict(force_mode=fm, sm_tiles=st, persistent=ps, build_lanes=bl)
                  for (fm, st, ps), bl in itertools.product(((0, 0, 1), (0, 0, 0), (0, 1, 0), (1, 0, 0), (2, 0, 0)),
-                                                           (1, 2, 4, 8, 32)))
+                                                           (0, 1, 2, 4, 8, 32)))
 
 
 def candidates(pbs=DEFAULT_PB, tps=DEFAULT_TP, skins=DEFAULT_SKIN, max_block=512):

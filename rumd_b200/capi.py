@@ -38,6 +38,7 @@ EXPORTS = [
     "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
     "b2md_run_queued", "b2md_nbl_export", "b2md_sort_export", "b2md_cell_grid", "b2md_sync",
     "b2md_stream", "b2md_last_error", "b2md_version", "b2md_probe_dist2", "b2md_probe_cell",
+    "b2md_probe_nvt",
     "b2md_forces_noalloc", "b2md_f64_create", "b2md_f64_destroy", "b2md_f64_set_state",
     "b2md_f64_set_integrator", "b2md_f64_set_xi", "b2md_f64_calc_f", "b2md_f64_run", "b2md_f64_get",
     "b2md_f64_stats",
@@ -104,6 +105,7 @@ def lib():
             "b2md_sync": [P],
             "b2md_probe_dist2": [P, P, P, i, P],
             "b2md_probe_cell": [P, i, f, i, P],
+            "b2md_probe_nvt": [P, P, P, P, f, P, i, P, P],
             "b2md_forces_noalloc": [P, i, P, i, P, i, P, P, P],
             "b2md_f64_create": [i, i, i, P, P, i, d, i, ctypes.POINTER(P)],
             "b2md_f64_destroy": [P],
@@ -368,6 +370,18 @@ def probe_cell(x, box, nc):
     out = np.zeros((len(x), 2), np.int32)
     check(lib().b2md_probe_cell(_ptr(x), len(x), float(box), int(nc), _ptr(out)))
     return out
+
+
+def probe_nvt(r4, v4, f4, xi, dt, box):
+    """(reference expressions, engine forms) of the leap-frog update: [n, 9] each."""
+    r4, v4, f4 = (np.ascontiguousarray(x, np.float32) for x in (r4, v4, f4))
+    xi = np.ascontiguousarray(xi, np.float32)
+    box = np.ascontiguousarray(box, np.float32)
+    ref = np.zeros((len(r4), 9), np.float32)
+    eng = np.zeros((len(r4), 9), np.float32)
+    check(lib().b2md_probe_nvt(_ptr(r4), _ptr(v4), _ptr(f4), _ptr(xi), float(dt), _ptr(box), len(r4), _ptr(ref),
+                               _ptr(eng)))
+    return ref, eng
 
 
 F64_STAT_NAMES = ["pe", "virial", "ke", "ke2", "xi", "rebuilds", "steps"]

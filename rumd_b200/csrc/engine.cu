@@ -135,7 +135,7 @@ struct b2md_engine {
   unsigned* smctr = nullptr;   // SM-region claim counters (nsm + 1)
   int win_cap = 2560;          // FM_WINDOW: window capacity in particles
   int wl_rows_cap = 128;       // FM_WINDOW: window-list rows staged in shared memory (0 = stream)
-  int build_lanes = 32;        // list build: lanes per particle (32: one warp per cell)
+  int build_lanes = 0;         // list build: 0 contiguous candidate runs per lane, else lanes per particle (32: one warp per cell)
   bool build_smem = false;     // list build: tile assembled in shared memory
   bool persist = true;         // runs: many steps per launch of k_steps between list rebuilds
   bool persist_on = false;     // the current graphs are the persistent ones
@@ -199,7 +199,9 @@ void dev_grow(b2md_engine* e, T*& p, long long old_n, long long new_n, bool zero
 }
 
 // Pinned host staging of at least `bytes` (kept for the engine's life), so
-// that particle uploads and read-backs are DMA copies.
+// that particle uploads and read-backs are DMA copies.  Sized per particle
+// for the largest use (read-back: id + r + v + images, plus alignment).
+constexpr size_t kStagePerParticle = 64;
 void* host_stage(b2md_engine* e, size_t bytes) {
   if (bytes > e->h_stage_bytes) {
     if (e->h_stage) {
@@ -622,6 +624,11 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   // list build: build_lanes lanes per particle (fewer when pb*lanes would
   // exceed a block), the list either assembled in shared memory or stored
   // straight to global memory
+  if (e->build_lanes == 0 && !a.win_on) {
+    // one warp per cell, contiguous candidate runs per lane
+    k_rb_build_runs<<<T, kRunWarps * 32, 0, s>>>(a);
+    return;
+  }
   if (e->build_lanes == 32 && !a.win_on) {
     // one warp per cell, candidates staged in shared memory
     const size_t cw = (size_t)kCs2Floats * sizeof(float) + (size_t)kCwWarps * kCwCand * (sizeof(float4) + sizeof(int));
@@ -631,7 +638,8 @@ void launch_rebuild(b2md_engine* e, cudaStream_t s, const EngArgs& a) {
   const size_t smem = build_smem(e, a);
   if (smem > kMaxDynSmemBytes)
     api_fail(B2MD_ERR_NOMEM, "neighbour-list tile does not fit in shared memory: use a smaller pb");
-  const int lanes = std::min(e->build_lanes, kMaxBlock / e->pb);
+  // (position windows need the lane build: the warp builds run it with 8 lanes)
+  const int lanes = std::min(e->build_lanes == 0 || e->build_lanes == 32 ? 8 : e->build_lanes, kMaxBlock / e->pb);
 #define LB(LPV)                                                                    \
   if (lanes >= LPV) {                                                              \
     if (a.win_on) {                                                                \
@@ -1072,6 +1080,9 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
     grow_params(e, 1024);
     grow_elog(e, 16);
     grow_reps(e, std::max(max_replicas, 1));
+    // pinned staging for the expected particles, so that admissions and
+    // read-backs do not allocate it later
+    if (max_particles > 0) host_stage(e, (size_t)max_particles * kStagePerParticle);
     init_func_attrs(device);
     CK(cudaMalloc(&e->fctr, sizeof(unsigned)));
     CK(cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device));
@@ -1177,8 +1188,10 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
       e->win_cap = value;
       break;
     case B2MD_VARIANT_BUILD_LANES:
-      if (value != 1 && value != 2 && value != 4 && value != 8 && value != 32)
-        return fail(B2MD_ERR_ARG, "build lanes must be 1, 2, 4, 8 or 32 (one warp per cell) (got %d)", value);
+      if (value != 0 && value != 1 && value != 2 && value != 4 && value != 8 && value != 32)
+        return fail(B2MD_ERR_ARG,
+                    "build lanes must be 0 (row scan, one thread per particle), 1, 2, 4, 8 or 32 (one warp per "
+                    "cell) (got %d)", value);
       e->build_lanes = value;
       break;
     case B2MD_VARIANT_BUILD_SMEM:
@@ -1290,7 +1303,7 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
       for (int i = 0; i < h.n; ++i)
         if (!(vel4[4 * i + 3] > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass (vel4[.,3]) must be positive");
     const size_t nb = (size_t)h.n * sizeof(float4);
-    char* stage = static_cast<char*>(host_stage(e, 3 * nb));
+    char* stage = static_cast<char*>(host_stage(e, (size_t)h.n * kStagePerParticle));
     const float4* sr = reinterpret_cast<const float4*>(pos4);
     const float4* sv = reinterpret_cast<const float4*>(vel4);
     int4* si = reinterpret_cast<int4*>(stage + 2 * nb);
@@ -1390,7 +1403,7 @@ int b2md_replica_read(b2md_engine* e, int id, float* pos4, float* vel4, int* im3
     CK(cudaSetDevice(e->device));
     RepState s = read_state(e, id);
     const size_t n = (size_t)h.n;
-    char* stage = static_cast<char*>(host_stage(e, n * (sizeof(unsigned) + 3 * sizeof(float4))));
+    char* stage = static_cast<char*>(host_stage(e, n * kStagePerParticle));
     unsigned* ids = reinterpret_cast<unsigned*>(stage);
     float4* sr = reinterpret_cast<float4*>(stage + ((n * sizeof(unsigned) + 15) & ~(size_t)15));
     float4* sv = sr + n;
@@ -1712,6 +1725,58 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     long long nl = 2;
+    if (persist_mode(e) && e->reps.size() < (1u << 20)) {
+      // the persistent graph's launch sequence with the host taking the loop
+      // decision: rebuild kernels (they exit at once when no rebuild is due),
+      // then one cooperative k_steps launch that runs steps until a rebuild is
+      // due or the budget is spent; each launch is timed with its steps
+      const StepsFn fs = steps_fn(e->tp);
+      const size_t psmem = persist_smem(e, a);
+      force_fn(e, true, false, a);  // checks the shared-memory need
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fs, e->pb * e->tp, psmem));
+      if ((long long)per_sm * e->nsm >= e->ntiles) {
+        const int grid = steps_grid(e, fs, psmem);
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        int* h_left = nullptr;
+        CK(cudaMallocHost(&h_left, sizeof(int)));
+        int budget = (int)std::min<long long>(nsteps, 1 << 30);
+        *e->h_budget = budget;
+        CK(cudaMemcpyAsync(&e->pctl->budget, e->h_budget, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        double tot = 0.0;
+        cudaGraphConditionalHandle none = 0;
+        while (budget > 0) {
+          launch_rebuild(e, e->stream, a);
+          nl += rebuild_launches(e);
+          CK(cudaMemsetAsync(&e->pctl->arrive, 0, sizeof(unsigned long long), e->stream));
+          CK(cudaEventRecord(e0, e->stream));
+          void* args[] = {&a, &none};
+          CK(cudaLaunchCooperativeKernel((const void*)fs, dim3(grid), dim3(e->pb * e->tp), args, psmem, e->stream));
+          CK(cudaEventRecord(e1, e->stream));
+          CK(cudaMemcpyAsync(h_left, &e->pctl->budget, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+          CK(cudaStreamSynchronize(e->stream));
+          check_persist(e);
+          float ms = 0.f;
+          CK(cudaEventElapsedTime(&ms, e0, e1));
+          tot += ms;
+          nl += 1;
+          const int ran = budget - *h_left;
+          budget = *h_left;
+          if (ran <= 0 || max_steps_left(e) == 0) break;  // no replica has steps left
+        }
+        cudaFreeHost(h_left);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (repair_overflow(e)) run_steps(e, nsteps);
+        calc_f(e, false);
+        CK(cudaStreamSynchronize(e->stream));
+        *step_kernel_ms = tot;
+        *launches = nl + rebuild_launches(e) + 1;
+        return;
+      }
+    }
     const size_t smem = force_smem(e, a);
     ForceFn fstep = force_fn(e, true, false, a);
     std::vector<cudaEvent_t> ev(2 * nsteps);

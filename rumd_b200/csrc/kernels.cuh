@@ -234,17 +234,15 @@ __device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float
   const bool thermo = (R.thermo_mask >> ti) & 1u;
   if (do_reset) { v.x -= vshift.x; v.y -= vshift.y; v.z -= vshift.z; }
   const float xs = thermo ? xi_f : 0.f;
-  const float factor = 0.5f * xs * R.dt;
-  const float plus = 1.f / (1.f + factor);
-  const float minus = 1.f - factor;
   const float dt = R.dt;
+  const NvtCoef c = nvt_coef(xs, dt);
   const double vb = (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z;
-  float vx = plus * __fmaf_rn(minus, v.x, __fmul_rn(__fmul_rn(v.w, f.x), dt));
-  float vy = plus * __fmaf_rn(minus, v.y, __fmul_rn(__fmul_rn(v.w, f.y), dt));
-  float vz = plus * __fmaf_rn(minus, v.z, __fmul_rn(__fmul_rn(v.w, f.z), dt));
-  float x = __fmaf_rn(vx, dt, r.x), y = __fmaf_rn(vy, dt, r.y), z = __fmaf_rn(vz, dt, r.z);
-  float kx = rintf(__fmul_rn(x, R.invL[0])), ky = rintf(__fmul_rn(y, R.invL[1])), kz = rintf(__fmul_rn(z, R.invL[2]));
-  x = __fmaf_rn(-R.L[0], kx, x); y = __fmaf_rn(-R.L[1], ky, y); z = __fmaf_rn(-R.L[2], kz, z);
+  float vx = nvt_velocity(c, v.x, v.w, f.x, dt);
+  float vy = nvt_velocity(c, v.y, v.w, f.y, dt);
+  float vz = nvt_velocity(c, v.z, v.w, f.z, dt);
+  float x = nvt_position(r.x, vx, dt), y = nvt_position(r.y, vy, dt), z = nvt_position(r.z, vz, dt);
+  float kx = wrap_image(x, R.invL[0]), ky = wrap_image(y, R.invL[1]), kz = wrap_image(z, R.invL[2]);
+  x = wrap_apply(x, R.L[0], kx); y = wrap_apply(y, R.L[1], ky); z = wrap_apply(z, R.L[2], kz);
   im.x += (int)kx; im.y += (int)ky; im.z += (int)kz;
   v.x = vx; v.y = vy; v.z = vz;
   rn = make_float4(x, y, z, r.w);
@@ -362,10 +360,14 @@ __device__ void finish_step_persist(const EngArgs& a, const RepDev& R, RepState*
 // Pair force (+ fused integration).  FUSED = one MD step: forces from r[rbuf],
 // integrate, write r[rbuf^1].  Otherwise Sample::CalcF only.
 // ---------------------------------------------------------------------------
-// Per-thread force accumulators of one particle.
+// Per-thread force accumulators of one particle.  The stress terms are
+// fij's FP32 products (PairPotential.h:1232-1241) summed in FP64: a
+// particle's six components cancel strongly over its neighbours, and FP32
+// sums of them lose about 1e-5 (stresses are computed only on request,
+// never in the fused step).
 struct PairAcc {
   float fx = 0.f, fy = 0.f, fz = 0.f, uu = 0.f, ww = 0.f;
-  float sxx = 0.f, syy = 0.f, szz = 0.f, syz = 0.f, sxz = 0.f, sxy = 0.f;
+  double sxx = 0.0, syy = 0.0, szz = 0.0, syz = 0.0, sxz = 0.0, sxy = 0.0;
 };
 
 // The pair rows of particle i's type, looked up by the neighbour's type.
@@ -479,8 +481,8 @@ __device__ __forceinline__ void lj_pair(PairAcc& A, const float4& ri, const floa
   A.ww = __fmaf_rn(d2, s, A.ww);
   A.uu += u;
   if (STRESS) {
-    A.sxx -= dx * dx * s; A.syy -= dy * dy * s; A.szz -= dz * dz * s;
-    A.syz -= dy * dz * s; A.sxz -= dx * dz * s; A.sxy -= dx * dy * s;
+    A.sxx -= (double)(dx * dx * s); A.syy -= (double)(dy * dy * s); A.szz -= (double)(dz * dz * s);
+    A.syz -= (double)(dy * dz * s); A.sxz -= (double)(dx * dz * s); A.sxy -= (double)(dx * dy * s);
   }
 }
 
@@ -898,7 +900,7 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
                                  Lz, iLx, iLy, iLz);
     }
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
-    float sxx = A.sxx, syy = A.syy, szz = A.szz, syz = A.syz, sxz = A.sxz, sxy = A.sxy;
+    double sxx = A.sxx, syy = A.syy, szz = A.szz, syz = A.syz, sxz = A.sxz, sxy = A.sxy;
     if (TP > 1) {
 #pragma unroll
       for (int o = TP / 2; o > 0; o >>= 1) {
@@ -947,8 +949,8 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
       const float4 fo = make_float4(fx, fy, fz, 0.5f * uu);
       const size_t gi = (size_t)R.p0 + i;
       a.f[gi] = fo;
-      a.w[gi] = make_float4(0.f, sxz, sxy, ww);
-      if (STRESS) a.sts[gi] = make_float4(sxx, syy, szz, syz);
+      a.w[gi] = make_float4(0.f, (float)sxz, (float)sxy, ww);
+      if (STRESS) a.sts[gi] = make_float4((float)sxx, (float)syy, (float)szz, (float)syz);
       acc[P_PE] = (double)fo.w;
       acc[P_W] = (double)ww;
       if (FUSED) {
@@ -1070,6 +1072,12 @@ __device__ __forceinline__ unsigned long long atom_add_acq_rel_u64(unsigned long
   return old;
 }
 
+// The persistent loop's condition, when k_steps runs inside the step graph;
+// an eager (profiling) launch passes a zero handle and the host decides.
+__device__ __forceinline__ void set_loop(cudaGraphConditionalHandle h, unsigned v) {
+  if (h) cudaGraphSetConditional(h, v);
+}
+
 // Waits (bounded) until the grid barrier of generation gen is released;
 // false when the wait gave up (recorded, and the graph's loop ended).
 __device__ bool barrier_wait(PersistCtl* c, unsigned gen, cudaGraphConditionalHandle h_loop) {
@@ -1077,7 +1085,7 @@ __device__ bool barrier_wait(PersistCtl* c, unsigned gen, cudaGraphConditionalHa
     if (ld_acquire_u32(&c->gen) != gen) break;
     if (it >= kBarrierPolls) {
       atomicExch(&c->err, 1);
-      cudaGraphSetConditional(h_loop, 0u);
+      set_loop(h_loop, 0u);
       return false;
     }
     __nanosleep(64);
@@ -1135,7 +1143,7 @@ __device__ int step_decide(const EngArgs& a, int step, int budget, unsigned long
       if (((now - base) & kTallyArriveMask) == gridDim.x) break;
       if (it >= kBarrierPolls) {
         atomicExch(&c->err, 1);
-        cudaGraphSetConditional(h_loop, 0u);
+        set_loop(h_loop, 0u);
         return 0;
       }
       __nanosleep(32);
@@ -1149,7 +1157,7 @@ __device__ int step_decide(const EngArgs& a, int step, int budget, unsigned long
   const int go = any == 0 && more > 0 && budget > 0 && step + 1 < cap;
   if (last && !go) {
     c->budget = budget;  // for the launch after the rebuild
-    cudaGraphSetConditional(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
+    set_loop(h_loop, (more > 0 && budget > 0) ? 1u : 0u);
   }
   return go;
 }
@@ -1172,7 +1180,7 @@ __global__ void __maxnreg__(72) k_steps(EngArgs a, cudaGraphConditionalHandle h_
   PersistCtl* c = a.pctl;
   if (threadIdx.x == 0) {
     s_go = __ldcg(&c->err) == 0;
-    if (!s_go && blockIdx.x == 0) cudaGraphSetConditional(h_loop, 0u);
+    if (!s_go && blockIdx.x == 0) set_loop(h_loop, 0u);
     if (s_go) s_go = setup_barrier(a, h_loop);
   }
   __syncthreads();
@@ -2242,5 +2250,266 @@ __global__ void __launch_bounds__(kCwWarps * 32) k_rb_build_cw(EngArgs a) {
   }
 }
 
+// (7'') The same list with one warp per cell and contiguous candidate runs:
+//       the cell's candidates (its 25 row parts, numbered in the reference's
+//       order) are cut into chunks of up to 32 * kRunMax, and lane l of the
+//       warp takes the consecutive run [l K, (l + 1) K) of a chunk (K <= 16).
+//       For two of the cell's particles at a time, a lane tests its run with
+//       no cross-lane traffic, keeping one accept bit per candidate; one
+//       exclusive scan of the lanes' accept counts then gives each lane the
+//       list position of its first accepted candidate, and the lane writes its
+//       accepted ones in run order.  Runs follow one another in candidate
+//       order, so the list is the reference's entry for entry.  Only the
+//       candidates' slots are staged (in shared memory, lane-major with an odd
+//       stride so that a warp's reads are bank-conflict free); their
+//       positions are read through L1, where the cell's other particles and
+//       the neighbouring cells' warps find them again.
+constexpr int kRunWarps = 4;                 // warps (cells in flight) per block
+constexpr int kRunMax = 16;                  // candidates per lane per chunk
+constexpr int kRunStride = kRunMax + 1;      // odd: conflict-free lane-major slots
+constexpr int kRunChunk = 32 * kRunMax;      // candidates per chunk
+
+struct Cs2One {
+  float c0;
+  __device__ __forceinline__ float operator()(int) const { return c0; }
+};
+struct Cs2Two {
+  float c0, c1;
+  __device__ __forceinline__ float operator()(int tj) const { return tj ? c1 : c0; }
+};
+struct Cs2Table {
+  const float* row;
+  __device__ __forceinline__ float operator()(int tj) const { return row[tj]; }
+};
+
+// Accept bits of a lane's run for up to four of the cell's particles (a
+// missing one repeats the last; its bits are unused): each candidate's
+// position is read once and tested against all four.
+template <bool WRAP, class CS2>
+__device__ __forceinline__ void run_tests4(const int* __restrict__ run, int nrun, const float4* __restrict__ rc,
+                                           const float4 (&rp)[4], const int (&ip)[4], const CS2 (&cs)[4],
+                                           float Lx, float Ly, float Lz, float iLx, float iLy, float iLz,
+                                           unsigned (&bits)[4]) {
+#pragma unroll
+  for (int q = 0; q < 4; ++q) bits[q] = 0u;
+#pragma unroll 2
+  for (int k = 0; k < kRunMax; ++k) {
+    if (k < nrun) {
+      const int j = run[k];
+      const float4 rj = __ldg(rc + j);
+      const int tj = __float_as_int(rj.w);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        float dx = rp[q].x - rj.x, dy = rp[q].y - rj.y, dz = rp[q].z - rj.z;
+        if (WRAP) {
+          dx = mi_comp(dx, Lx, iLx);
+          dy = mi_comp(dy, Ly, iLy);
+          dz = mi_comp(dz, Lz, iLz);
+        }
+        if (dist2_ref(dx, dy, dz) < cs[q](tj) && j != ip[q]) bits[q] |= 1u << k;
+      }
+    }
+  }
+}
+
+// Writes particle p's accepted candidates of this chunk: `bits` of the lane's
+// run, after `cnt` entries already in p's list (32-bit offsets from the
+// replica's list: entry k of slot p at (k/8) 8 stride + 8 p + k%8).
+// Returns the chunk's total for p.
+__device__ __forceinline__ int run_store(unsigned bits, const int* __restrict__ run, int cnt, int maxn,
+                                         unsigned* __restrict__ lbase, unsigned p, unsigned stride8) {
+  const int lane = threadIdx.x & 31;
+  const int c = __popc(bits);
+  int incl = c;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  unsigned pos = (unsigned)(cnt + incl - c);
+  const unsigned pb = p << 3;
+  while (bits) {
+    const int k = __ffs(bits) - 1;
+    bits &= bits - 1u;
+    if (pos < (unsigned)maxn) lbase[(pos >> 3) * stride8 + pb + (pos & 7u)] = (unsigned)run[k];
+    ++pos;
+  }
+  return __shfl_sync(0xffffffffu, incl, 31);
+}
+
+__global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ float s_cs2[kCs2Floats];
+  __shared__ int s_run[kRunWarps][32 * kRunStride];
+  __shared__ int s_max;
+  const int tile = blockIdx.x, rep = a.tile_rep[tile];
+  if (!rb_active(a, rep)) return;
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  const int nt = R.ntypes;
+  for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
+  if (threadIdx.x == 0) s_max = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int first = a.tile_first[tile];
+  const int last = (tile + 1 < R.tile0 + R.ntiles) ? a.tile_first[tile + 1] : R.n;
+  const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
+  const int maxn = R.max_nbrs;
+  const unsigned stride8 = 8u * (unsigned)R.nbl_stride;
+  unsigned* __restrict__ lbase = a.nbl + R.nbl0;
+  int* wrun = s_run[warp];
+  const int* run = wrun + lane * kRunStride;
+  const bool cells = R.nb_method == NB_CELLS;
+  const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
+  const int* __restrict__ cbeg = a.cstart + R.cell0;  // absolute first slot (k_rb_fix)
+  const int* __restrict__ ccnt = a.cnt + R.cell0;
+  // units of work: the cells from the first to the last particle's (keys
+  // ascend along the slots), or one unit for all pairs
+  int k0 = 0, k1 = 0;
+  if (cells && last > first) {
+    const float4 rf = rc[first], rl = rc[last - 1];
+    const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
+    k0 = cell_coord(rf.x, iLx, nx) + cell_coord(rf.y, iLy, ny) * nx + cell_coord(rf.z, iLz, nz) * nx * ny;
+    k1 = cell_coord(rl.x, iLx, nx) + cell_coord(rl.y, iLy, ny) * nx + cell_coord(rl.z, iLz, nz) * nx * ny;
+  }
+  int wmax = 0;
+  for (int c = k0 + warp; c <= k1; c += kRunWarps) {
+    const int p0 = cells ? max(cbeg[c], first) : first;
+    const int p1 = cells ? min(cbeg[c] + ccnt[c], last) : last;
+    if (p0 >= p1) continue;  // no particle of this tile in the cell
+    // lane r < 25: row (dz, dy) = (r/5 - 2, r%5 - 2) as one or two slot parts
+    int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
+    bool wrap = true;
+    if (cells) {
+      const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+      // no wrapped cell among the 5x5x5 and at least 7 cells a side: the
+      // minimum-image step is exactly the identity
+      wrap = !(nx >= 7 && ny >= 7 && nz >= 7 && cx >= 2 && cx < nx - 2 && cy >= 2 && cy < ny - 2 && cz >= 2 &&
+               cz < nz - 2);
+      if (lane < 25) {
+        const int dz = lane / 5 - 2, dy = lane % 5 - 2;
+        int oz = cz + dz;
+        oz += ((oz < 0) - (oz >= nz)) * nz;
+        int oy = cy + dy;
+        oy += ((oy < 0) - (oy >= ny)) * ny;
+        const int row = oy * nx + oz * nx * ny;
+        const int lo = cx - 2, hi = cx + 2;
+        if (lo >= 0 && hi < nx) {
+          b0 = cbeg[row + lo];
+          e0 = cbeg[row + hi] + ccnt[row + hi];
+        } else {
+          // the row wraps: cells from the far end first (dx < 0), as the
+          // reference's dx loop visits them
+          const int cw = row + nx - 1;
+          const int ca = lo < 0 ? row + nx + lo : row + lo;
+          const int cb = lo < 0 ? row + hi : row + hi - nx;
+          b0 = cbeg[ca];
+          e0 = cbeg[cw] + ccnt[cw];
+          b1 = cbeg[row];
+          e1 = cbeg[cb] + ccnt[cb];
+        }
+      }
+    } else if (lane == 0) {
+      e0 = R.n;
+    }
+    const int l0 = e0 - b0, len = l0 + (e1 - b1);
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int off = incl - len;                 // this lane's first candidate number
+    const int M = __shfl_sync(FULL, incl, 31);  // candidates of the unit
+    for (int pg = p0; pg < p1; pg += 32) {
+      const int pe = min(p1, pg + 32);
+      int cnt_reg = 0;  // lane k: list length so far of particle pg + k
+      for (int ch = 0; ch < M; ch += kRunChunk) {
+        const int mc = min(kRunChunk, M - ch);
+        const int K = (mc + 31) >> 5;  // run length of every lane but the last ones
+        __syncwarp();
+        // candidate number v of the chunk goes to lane v / K, place v % K:
+        // each row lane writes its own parts' candidates, stepping the
+        // (lane, place) pair instead of dividing per candidate
+        {
+          const int v0 = max(off, ch), v1 = min(off + len, ch + mc);
+          if (v0 < v1) {
+            int qk = (v0 - ch) / K, rk = (v0 - ch) - qk * K;
+            for (int v = v0; v < v1; ++v) {
+              wrun[qk * kRunStride + rk] = v - off < l0 ? b0 + (v - off) : b1 + (v - off - l0);
+              if (++rk == K) {
+                rk = 0;
+                ++qk;
+              }
+            }
+          }
+        }
+        __syncwarp();
+        const int nrun = min(K, max(0, mc - lane * K));
+        for (int p = pg; p < pe; p += 4) {
+          // up to four of the cell's particles against the chunk
+          float4 rp[4];
+          int ip[4];
+          const float* crow[4];
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            ip[q] = min(p + q, pe - 1);
+            rp[q] = rc[ip[q]];
+            crow[q] = s_cs2 + __float_as_int(rp[q].w) * nt;
+          }
+          unsigned bits[4];
+#define RUNS(W, T, MK)                                                                                    \
+  {                                                                                                       \
+    const T cs[4] = {MK(crow[0]), MK(crow[1]), MK(crow[2]), MK(crow[3])};                                 \
+    run_tests4<W>(run, nrun, rc, rp, ip, cs, R.L[0], R.L[1], R.L[2], R.invL[0], R.invL[1], R.invL[2], bits); \
+  }
+#define ONE(c) Cs2One{(c)[0]}
+#define TWO(c) Cs2Two{(c)[0], (c)[1]}
+#define TAB(c) Cs2Table{(c)}
+          if (nt == 1) {
+            if (wrap) RUNS(true, Cs2One, ONE) else RUNS(false, Cs2One, ONE)
+          } else if (nt == 2) {
+            if (wrap) RUNS(true, Cs2Two, TWO) else RUNS(false, Cs2Two, TWO)
+          } else {
+            if (wrap) RUNS(true, Cs2Table, TAB) else RUNS(false, Cs2Table, TAB)
+          }
+#undef RUNS
+#undef ONE
+#undef TWO
+#undef TAB
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            if (p + q < pe) {
+              const int cq = __shfl_sync(FULL, cnt_reg, p + q - pg);
+              const int tot = run_store(bits[q], run, cq, maxn, lbase, (unsigned)(p + q), stride8);
+              if (lane == p + q - pg) cnt_reg = cq + tot;
+            }
+          }
+        }
+      }
+      if (pg + lane < pe) {
+        const int p = pg + lane;
+        a.nn[(size_t)R.p0 + p] = (unsigned)min(cnt_reg, maxn);
+        a.last_r[(size_t)R.p0 + p] = rc[p];
+        wmax = max(wmax, cnt_reg);
+      }
+    }
+  }
+  wmax = __reduce_max_sync(FULL, wmax);
+  if (lane == 0) atomicMax(&s_max, wmax);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int s_max_v = s_max;
+    atomicMax(&S->actual_max_nbrs, s_max_v);
+    if (s_max_v > R.max_nbrs) atomicExch(&S->overflow, 1);
+    __threadfence();
+    const unsigned cdone = atomicAdd(&a.rctr[rep], 1u);
+    if (cdone == (unsigned)(R.ntiles - 1)) {
+      a.rctr[rep] = 0u;
+      S->rebuild = 0;
+      S->nrebuilds += 1;
+    }
+  }
+}
 
 }  // namespace b2md

@@ -38,6 +38,36 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
   return y;
 }
 
+// Nose-Hoover leap-frog of one particle (integrateNVTAlgorithm,
+// IntegratorNVT.cu:385-399, with applyBoundaryCondition, SimulationBox.h:140-155):
+//   factor = xi dt / 2, plus = 1 / (1 + factor), minus = 1 - factor
+//   v <- plus (minus v + (1/m) f dt);  r <- r + v dt;  k = rint(r / L);  r <- r - L k
+// with the multiply-add contractions nvcc makes of those expressions written
+// out, so that the result is the reference's bit for bit (checked by the
+// parity probe against the expressions compiled as written).
+struct NvtCoef {
+  float plus, minus;
+};
+// factor = (0.5 xi) dt is never rounded on its own: nvcc fuses it into the
+// two sums that use it, 1 + factor and 1 - factor.
+__device__ __forceinline__ NvtCoef nvt_coef(float xi, float dt) {
+  const float h = __fmul_rn(0.5f, xi);
+  NvtCoef c;
+  c.plus = __fdiv_rn(1.f, __fmaf_rn(h, dt, 1.f));
+  c.minus = __fmaf_rn(-h, dt, 1.f);
+  return c;
+}
+// One component: new velocity, position before the wrap, then the wrap.
+// In minus * v + (1/m) f dt nvcc fuses the second product, ((1/m) f) dt,
+// into the sum, not the first (2^20 random states: 0 mismatches this way,
+// about 30 % the other way).
+__device__ __forceinline__ float nvt_velocity(const NvtCoef& c, float v, float im, float f, float dt) {
+  return __fmul_rn(c.plus, __fmaf_rn(__fmul_rn(im, f), dt, __fmul_rn(c.minus, v)));
+}
+__device__ __forceinline__ float nvt_position(float r, float vn, float dt) { return __fmaf_rn(vn, dt, r); }
+__device__ __forceinline__ float wrap_image(float x, float invL) { return rintf(__fmul_rn(x, invL)); }
+__device__ __forceinline__ float wrap_apply(float x, float L, float k) { return __fmaf_rn(-L, k, x); }
+
 __device__ __forceinline__ int cell_coord(float x, float invL, int nc) {
   // calculateCellCoordinates (NeighborList.cu:1106-1133)
   float scaled = __fmaf_rn(x, invL, 0.5f);

@@ -110,6 +110,9 @@ PYBIND11_MODULE(_rumd, m) {
       .def(py::init<float, double, double>(), py::arg("timeStep"), py::arg("targetTemperature"),
            py::arg("thermostatRelaxationTime"))
       .def(py::init<float>(), py::arg("timeStep"))
+      .def("GetInfoString", &IntegratorNVT::GetInfoString, py::arg("precision") = 6)
+      .def("InitializeFromInfoString", &IntegratorNVT::InitializeFromInfoString, py::arg("infoStr"),
+           py::arg("verbose") = true)
       .def("SetRelaxationTime", &IntegratorNVT::SetRelaxationTime)
       .def("SetTargetTemperature", &IntegratorNVT::SetTargetTemperature, py::arg("T"), py::arg("reset") = false)
       .def("SetThermostatState", &IntegratorNVT::SetThermostatState)
@@ -124,7 +127,7 @@ PYBIND11_MODULE(_rumd, m) {
 
   py::class_<Sample>(m, "Sample")
       .def(py::init<unsigned, unsigned>(), py::arg("pb") = 0, py::arg("tp") = 0)
-      .def("ReadConf", &Sample::ReadConf)
+      .def("ReadConf", &Sample::ReadConf, py::arg("filename"), py::arg("init_itg") = false)
       .def("WriteConf", [](Sample& s, const std::string& f, const std::string&) { s.WriteConf(f); }, py::arg("filename"),
            py::arg("mode") = "w")
       .def("SetConfiguration",

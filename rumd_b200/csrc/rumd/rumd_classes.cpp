@@ -6,6 +6,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <iomanip>
+#include <iostream>
 #include <sstream>
 
 #include "rumd_b200.h"
@@ -21,6 +23,22 @@ std::vector<std::string> split(const std::string& s, char sep) {
   std::istringstream is(s);
   while (std::getline(is, cur, sep)) out.push_back(cur);
   return out;
+}
+
+// "Class,p1,p2,..." -> class name and the parameters as floats (the format
+// of RUMD's info strings, ParseInfoString.cc:6-34).
+std::string parse_info(const std::string& info, std::vector<float>& params) {
+  params.clear();
+  std::vector<std::string> parts = split(info, ',');
+  if (parts.empty()) return "";
+  for (size_t k = 1; k < parts.size(); ++k) {
+    if (parts[k].empty()) continue;
+    char* end = nullptr;
+    const float v = std::strtof(parts[k].c_str(), &end);
+    if (end == parts[k].c_str()) throw RUMD_Error("[None]", "ParseInfoString", "Failed to read parameter from infoStr " + info);
+    params.push_back(v);
+  }
+  return parts[0];
 }
 }  // namespace
 
@@ -224,6 +242,34 @@ void IntegratorNVT::PushSettings() {
 void IntegratorNVT::SetTimeStep(float dt) {
   Integrator::SetTimeStep(dt);
   PushSettings();
+}
+
+std::string IntegratorNVT::GetInfoString(unsigned precision) const {
+  std::ostringstream o;
+  o << std::setprecision((int)precision);
+  if (thermostatOn)
+    o << "IntegratorNVT," << GetTimeStep() << "," << GetTargetTemperature() << "," << GetRelaxationTime() << ","
+      << GetThermostatState();
+  else
+    o << "IntegratorNVE," << GetTimeStep();
+  return o.str();
+}
+
+void IntegratorNVT::InitializeFromInfoString(const std::string& infoStr, bool verbose) {
+  std::vector<float> p;
+  const std::string cls = parse_info(infoStr, p);
+  const bool nvt = cls == "IntegratorNVT";
+  if (!nvt && cls != "IntegratorNVE")
+    throw RUMD_Error("IntegratorNVT", "InitializeFromInfoString", "Expected IntegratorNVT or IntegratorNVE");
+  if (p.size() != (nvt ? 4u : 1u))
+    throw RUMD_Error("IntegratorNVT", "InitializeFromInfoString", "Wrong number of parameters in infoStr");
+  if (verbose) std::cout << "[Info] Initializing " << cls << ". time step:" << p[0] << std::endl;
+  SetTimeStep(p[0]);
+  if (nvt) {
+    SetTargetTemperature(p[1]);
+    SetRelaxationTime(p[2]);
+    SetThermostatState(p[3]);
+  }
 }
 
 void IntegratorNVT::SetRelaxationTime(float tau) {
@@ -600,7 +646,7 @@ std::vector<unsigned> Sample::ExportSortIndex() const {
 // key=value header line and a columns= list.
 // ---------------------------------------------------------------------------
 
-void Sample::ReadConf(const std::string& filename) {
+void Sample::ReadConf(const std::string& filename, bool init_itg) {
   gzFile fp = gzopen(filename.c_str(), "rb");
   if (!fp) throw RUMD_Error("Sample", "ReadConf", "cannot open " + filename);
   std::vector<char> buf(1 << 16);
@@ -615,29 +661,62 @@ void Sample::ReadConf(const std::string& filename) {
       }
     }
   };
+  auto fail = [&](const std::string& msg) {
+    gzclose(fp);
+    throw RUMD_Error("Sample", "ReadConf", msg);
+  };
   std::string line;
-  if (!getline(line)) { gzclose(fp); throw RUMD_Error("Sample", "ReadConf", "empty file"); }
+  if (!getline(line)) fail("empty file");
   long n = std::strtol(line.c_str(), nullptr, 10);
-  if (n < 2) { gzclose(fp); throw RUMD_Error("Sample", "ReadConf", "bad particle count"); }
+  if (n < 2) fail("bad particle count");
   getline(line);
   std::map<std::string, std::string> meta;
   for (const std::string& tok : split(line, ' ')) {
     auto eq = tok.find('=');
     if (eq != std::string::npos) meta[tok.substr(0, eq)] = tok.substr(eq + 1);
   }
-  if (!meta.count("boxLengths") || !meta.count("columns")) {
-    gzclose(fp);
-    throw RUMD_Error("Sample", "ReadConf", "header needs boxLengths= and columns=");
+  // ConfigurationMetaData::ReadMetaData (ConfigurationMetaData.cc:166-214):
+  // ioformat 1 carries dt, boxLengths and Nose-Hoover-Ps; ioformat 2 carries
+  // integrator=Class,params and sim_box=Class,params
+  if (!meta.count("ioformat")) fail("Did not find ioformat");
+  const int iof = std::atoi(meta["ioformat"].c_str());
+  if (iof != 1 && iof != 2) fail("ioformat must be 1 or 2");
+  std::string box_info, itg_info;
+  bool found_itg = false;
+  file_xi = 0.0;
+  file_dt = 0.f;
+  if (iof == 1) {
+    if (meta.count("boxLengths")) box_info = "RectangularSimulationBox," + meta["boxLengths"];
+    if (meta.count("Nose-Hoover-Ps")) {
+      file_xi = std::stod(meta["Nose-Hoover-Ps"]);
+      found_itg = true;
+    }
+    if (meta.count("dt")) file_dt = std::stof(meta["dt"]);
+  } else {
+    if (meta.count("sim_box")) box_info = meta["sim_box"];
+    if (meta.count("integrator")) {
+      itg_info = meta["integrator"];
+      found_itg = true;
+      std::vector<float> ip;
+      const std::string cls = parse_info(itg_info, ip);
+      if (!ip.empty()) file_dt = ip[0];  // ConfigurationMetaData.cc:209-212
+      if (cls == "IntegratorNVT" && ip.size() == 4) file_xi = ip[3];
+    }
   }
+  if (box_info.empty()) fail("Did not find box information");
   std::vector<float> L;
-  for (auto& s : split(meta["boxLengths"], ',')) L.push_back(std::stof(s));
+  if (parse_info(box_info, L) != "RectangularSimulationBox")
+    fail("only RectangularSimulationBox is supported (file has " + box_info.substr(0, box_info.find(',')) + ")");
+  if (L.size() == 1) L.assign(3, L[0]);
+  if (L.size() != 3) fail("RectangularSimulationBox needs 3 lengths");
+  if (!meta.count("columns")) fail("header needs columns=");
+  file_ioformat = iof;
+  file_integrator = itg_info;
   std::vector<std::string> cols = split(meta["columns"], ',');
   std::vector<float> masses;
   if (meta.count("mass"))
     for (auto& s : split(meta["mass"], ',')) masses.push_back(std::stof(s));
   if (meta.count("numTypes")) masses.resize(std::max<size_t>(masses.size(), std::stoul(meta["numTypes"])), 1.f);
-  file_xi = meta.count("Nose-Hoover-Ps") ? std::stod(meta["Nose-Hoover-Ps"]) : 0.0;
-  file_dt = meta.count("dt") ? std::stof(meta["dt"]) : 0.f;
   auto col = [&](const char* name) -> int {
     for (size_t k = 0; k < cols.size(); ++k)
       if (cols[k] == name) return (int)k;
@@ -645,18 +724,18 @@ void Sample::ReadConf(const std::string& filename) {
   };
   int ct = col("type"), cx = col("x"), cy = col("y"), cz = col("z");
   int cvx = col("vx"), cvy = col("vy"), cvz = col("vz"), cix = col("imx"), ciy = col("imy"), ciz = col("imz");
-  if (ct < 0 || cx < 0 || cy < 0 || cz < 0) { gzclose(fp); throw RUMD_Error("Sample", "ReadConf", "missing columns"); }
+  if (ct < 0 || cx < 0 || cy < 0 || cz < 0) fail("missing columns");
   std::vector<float> p3(3 * n), v3, i3f;
   std::vector<int> types(n), i3;
   if (cvx >= 0) v3.assign(3 * n, 0.f);
   if (cix >= 0) i3.assign(3 * n, 0);
   for (long i = 0; i < n; ++i) {
-    if (!getline(line)) { gzclose(fp); throw RUMD_Error("Sample", "ReadConf", "file ends early"); }
+    if (!getline(line)) fail("file ends early");
     std::istringstream is(line);
     std::vector<double> v;
     double x;
     while (is >> x) v.push_back(x);
-    if ((int)v.size() < (int)cols.size()) { gzclose(fp); throw RUMD_Error("Sample", "ReadConf", "short particle line"); }
+    if ((int)v.size() < (int)cols.size()) fail("short particle line");
     types[i] = (int)v[ct];
     p3[3 * i] = (float)v[cx]; p3[3 * i + 1] = (float)v[cy]; p3[3 * i + 2] = (float)v[cz];
     if (cvx >= 0) { v3[3 * i] = (float)v[cvx]; v3[3 * i + 1] = (float)v[cvy]; v3[3 * i + 2] = (float)v[cvz]; }
@@ -664,7 +743,14 @@ void Sample::ReadConf(const std::string& filename) {
   }
   gzclose(fp);
   SetConfiguration(p3, types, L, masses, v3, i3);
-  if (auto* nvt = dynamic_cast<IntegratorNVT*>(itg)) nvt->SetThermostatState(file_xi);
+  // Sample::ReadConf(filename, init_itg) (Sample.cu:584-600)
+  if (itg && init_itg && found_itg) {
+    if (iof == 1) {
+      if (auto* nvt = dynamic_cast<IntegratorNVT*>(itg)) nvt->SetThermostatState(file_xi);
+    } else {
+      itg->InitializeFromInfoString(itg_info);
+    }
+  }
 }
 
 void Sample::WriteConf(const std::string& filename) {
@@ -673,13 +759,19 @@ void Sample::WriteConf(const std::string& filename) {
   std::vector<int> imgs = GetImages();
   gzFile fp = gzopen(filename.c_str(), "wb");
   if (!fp) throw RUMD_Error("Sample", "WriteConf", "cannot open " + filename);
-  double xi = 0.0;
-  if (auto* nvt = dynamic_cast<IntegratorNVT*>(itg)) xi = nvt->GetThermostatState();
-  float dt = itg ? itg->GetTimeStep() : file_dt;
+  // ConfigurationWriterReader::Write_ioformat2 (ConfigurationWriterReader.cu:90-141):
+  // info strings with precision + 2 significant figures, the rest with
+  // `precision` decimals (9, the restart writer's)
+  const int precision = 9;
   std::ostringstream h;
-  h.precision(9);
-  h << std::fixed << type.size() << "\nioformat=2 dt=" << dt << " boxLengths=" << box[0] << "," << box[1] << ","
-    << box[2] << " numTypes=" << mass.size() << " Nose-Hoover-Ps=" << xi << " Barostat-Pv=0.000000000 mass=";
+  h << type.size() << "\nioformat=2 numTypes=" << mass.size();
+  if (itg) h << " integrator=" << itg->GetInfoString(precision + 2);
+  {
+    std::ostringstream b;
+    b << std::setprecision(precision + 2) << "RectangularSimulationBox," << box[0] << "," << box[1] << "," << box[2];
+    h << " sim_box=" << b.str();
+  }
+  h << std::fixed << std::setprecision(precision) << " mass=";
   for (size_t t = 0; t < mass.size(); ++t) h << (t ? "," : "") << mass[t];
   h << " columns=type,x,y,z,imx,imy,imz,vx,vy,vz,fx,fy,fz,pe,vir\n";
   gzputs(fp, h.str().c_str());

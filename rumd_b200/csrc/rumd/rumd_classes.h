@@ -170,6 +170,9 @@ class Integrator {
   virtual void SetTimeStep(float dt);
   bool RequiresStress() const { return false; }
   const std::string& GetID_String() const { return id; }
+  // "Class,p1,p2,..." as written to ioformat=2 files (IntegratorNVT.cu:252-290)
+  virtual std::string GetInfoString(unsigned precision) const = 0;
+  virtual void InitializeFromInfoString(const std::string& infoStr, bool verbose = false) = 0;
 
  protected:
   Sample* sample = nullptr;
@@ -187,6 +190,8 @@ class IntegratorNVT : public Integrator {
   double GetKineticEnergy(bool copy = true) const override;
   void SetMomentumToZero() override;
   void SetTimeStep(float dt) override;
+  std::string GetInfoString(unsigned precision) const override;
+  void InitializeFromInfoString(const std::string& infoStr, bool verbose = false) override;
 
   void SetRelaxationTime(float tau);
   void SetTargetTemperature(double T, bool reset = false);
@@ -227,7 +232,10 @@ class Sample {
   Sample& operator=(const Sample&) = delete;
 
   // Configuration I/O (ConfigurationWriterReader.cu:90-343).
-  void ReadConf(const std::string& filename);
+  // ConfigurationWriterReader::Read + ConfigurationMetaData::ReadMetaData
+  // (Sample.cu:584-600, ConfigurationMetaData.cc:166-214): ioformat 1 or 2;
+  // with init_itg the file's integrator state goes to the integrator.
+  void ReadConf(const std::string& filename, bool init_itg = false);
   void WriteConf(const std::string& filename);
   // Direct configuration set-up (positions xyz, types, box, masses per type).
   void SetConfiguration(const std::vector<float>& pos3, const std::vector<int>& types, const std::vector<float>& box,
@@ -302,6 +310,8 @@ class Sample {
   bool include_kinetic_stress = false;
   bool verbose = true;
   double file_xi = 0.0;
+  int file_ioformat = 0;
+  std::string file_integrator;  // ioformat=2 integrator info string
   int elog_interval = 0, elog_capacity = 0;
   float file_dt = 0.f;
 };

@@ -8,7 +8,8 @@ potential (SP) cut-off at 2.5 sigma_ij and the KA parameters.  They are the
 reference's golden vectors for the pair force path.  This script parses them
 (format written by src/ConfigurationWriterReader.cu:90-180; ``vir`` is w.w/2,
 line 173) and stores compact ``.npz`` fixtures so that the tests do not need
-the reference tree.
+the reference tree.  Two of the files are also copied unchanged into conf/
+for the configuration-reader tests.
 
 Usage:  python tests/golden/make_golden.py RUMD_SOURCE_TREE
 """
@@ -63,6 +64,16 @@ def parse(path):
     return out
 
 
+# RUMD's own configuration files, copied unchanged for the reader tests: one
+# in ioformat=1 (dt, boxLengths, Nose-Hoover-Ps) and one in ioformat=2
+# (integrator=IntegratorNVT,dt,T,tau,xi and sim_box=RectangularSimulationBox,
+# two types of unequal mass)
+RAW = [
+    ("Conf/KobAndersen", "KA_N256_L6.0_T0.50.xyz.gz"),
+    ("Conf/SingleComponentLiquid", "MgCu_equil_0.051_0.055.xyz.gz"),
+]
+
+
 def main():
     if len(sys.argv) != 2:
         sys.exit("usage: python tests/golden/make_golden.py RUMD_SOURCE_TREE")
@@ -73,6 +84,11 @@ def main():
         stem = name.replace(".xyz.gz", "")
         np.savez_compressed(os.path.join(here, f"ka_{stem}.npz"), **d)
         print(stem, len(d["type"]), "vir" in d)
+    import shutil
+    os.makedirs(os.path.join(here, "conf"), exist_ok=True)
+    for sub, name in RAW:
+        shutil.copyfile(os.path.join(root, sub, name), os.path.join(here, "conf", name))
+        print("copied", name)
 
 
 if __name__ == "__main__":

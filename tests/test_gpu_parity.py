@@ -98,6 +98,33 @@ def test_cell_coordinate_explicit_form_equals_reference_expression(capi):
     assert np.array_equal(out[:, 0], out[:, 1])
 
 
+@pytest.mark.parametrize("dt", [0.005, 0.004, 0.0025])
+def test_nvt_update_explicit_form_equals_nvcc_contraction_of_reference_expression(capi, dt):
+    """integrateNVTAlgorithm's velocity and position update and the periodic
+    wrap (IntegratorNVT.cu:385-399, SimulationBox.h:140-155), compiled as
+    written with default nvcc flags, against the engine's explicit forms
+    (nvt_coef / nvt_velocity / nvt_position / wrap_*), bit for bit, on 2^20
+    random states: thermostat states across and beyond the range runs reach
+    (xi = 0 included), forces up to the r^-13 wall, particles that leave the
+    box on any face."""
+    rng = np.random.default_rng(5)
+    n = 1 << 20
+    L = np.array([37.94, 9.41, 107.49], np.float32)
+    r = np.zeros((n, 4), np.float32)
+    v = np.zeros((n, 4), np.float32)
+    f = np.zeros((n, 4), np.float32)
+    r[:, :3] = rng.uniform(-L / 2, L / 2, (n, 3))
+    r[: n // 8, :3] = (L / 2) * np.sign(rng.normal(size=(n // 8, 3))) * rng.uniform(0.999, 1.0, (n // 8, 3))
+    v[:, :3] = rng.normal(size=(n, 3)) * rng.uniform(0.3, 3.0, (n, 1))
+    v[:, 3] = rng.choice(np.array([1.0, 0.5, 1.0 / 3.0], np.float32), n)
+    f[:, :3] = rng.normal(size=(n, 3)) * np.exp(rng.uniform(0, 8, (n, 1)))
+    xi = rng.normal(size=n).astype(np.float32) * 2.0
+    xi[::16] = 0.0
+    ref, eng = capi.probe_nvt(r, v, f, xi, dt, L)
+    bad = (ref.view(np.uint32) != eng.view(np.uint32)).sum(axis=0)
+    assert bad.sum() == 0, dict(zip(["vx", "vy", "vz", "x", "y", "z", "kx", "ky", "kz"], bad.tolist()))
+
+
 def test_explicit_dist2_matches_oracle_restatement(capi, oracle):
     """The oracle (fmaf on the CPU) and the GPU agree bit for bit."""
     rng = np.random.default_rng(3)
@@ -206,7 +233,7 @@ def test_neighbour_list_and_permutation_bit_exact(capi, oracle, ka_params, n):
     e.close()
 
 
-@pytest.mark.parametrize("lanes", [2, 32])
+@pytest.mark.parametrize("lanes", [0, 2, 32])
 def test_n2_and_sort_methods_give_same_sets(capi, oracle, ka_params, lanes):
     n = 5000
     m = melted_ka(capi, ka_params, n, steps=100, seed=7)
@@ -293,7 +320,7 @@ def test_fused_run_equals_separate_calcf_integrate(capi, ka_params):
 VARIANTS = [  # (force_mode, build_lanes, build_smem, sm_tiles)
     (1, 8, 1, 0), (0, 8, 1, 0), (1, 1, 0, 0), (0, 1, 0, 0), (0, 2, 0, 0), (0, 4, 0, 0), (0, 8, 0, 0),
     (0, 1, 1, 0), (2, 2, 0, 0), (2, 8, 1, 0), (2, 1, 0, 0), (2, 4, 0, 0), (0, 32, 0, 0), (1, 32, 0, 0),
-    (2, 32, 0, 0), (0, 32, 0, 1), (0, 2, 0, 1), (2, 32, 0, 1)]
+    (2, 32, 0, 0), (0, 32, 0, 1), (0, 2, 0, 1), (2, 32, 0, 1), (0, 0, 0, 0), (1, 0, 0, 0), (0, 0, 0, 1), (2, 0, 0, 0)]
 
 
 @pytest.mark.parametrize("tp", [1, 4])
@@ -441,4 +468,37 @@ def test_stress_tensor_trace_equals_virial(capi, ka_params):
     W = e.stats(rid)["virial"]
     # configurational stress: -tr(sigma)/3 * V == W  (Sample.cu:393-444 sign convention)
     assert abs(-(s[0] + s[1] + s[2]) / 3 * V - W) < 1e-4 * abs(W) + 1e-3
+    e.close()
+
+
+@pytest.mark.parametrize("cutoff,tp", [("SF", 4), ("SP", 1), ("NS", 2)])
+def test_stress_tensor_against_fp64_oracle(capi, oracle, ka_params, cutoff, tp):
+    """All six components of the pair stress (fij's STR branch,
+    PairPotential.h:1232-1241) per particle against the FP64 oracle (rms
+    relative 1e-5 over the components), and Sample::GetStress
+    (Sample.cu:393-444) with and without the kinetic part: the diagonal to
+    1e-5 relative, the off-diagonal (which fluctuate around zero) to 1e-5 of
+    the diagonal's size.  Non-cubic box, every cut-off method."""
+    n = 4000
+    m = melted_ka(capi, ka_params, n, steps=80, seed=33, cutoff=cutoff)
+    stretch = np.array([1.2, 0.9, 1.0 / 1.08], np.float32)
+    box = (m["box"] * stretch).astype(np.float32)
+    pos4 = m["pos4"].copy()
+    pos4[:, :3] *= stretch
+    e = new_engine(capi, tp=tp)
+    rid = e.add(pos4, box, ka_params, 2, cutoff=cutoff, vel4=m["vel4"])
+    e.calc_f(stress=True)
+    sts = e.get(rid, "stress", n).astype(np.float64)
+    w = e.get(rid, "virial", n).astype(np.float64)
+    g6 = np.stack([sts[:, 0], sts[:, 1], sts[:, 2], sts[:, 3], w[:, 1], w[:, 2]], 1)
+    types = pos4[:, 3].view(np.int32)
+    o6 = oracle.stress_f64(pos4[:, :3].astype(np.float64), types, box, 2, ka_params, capi.CUTOFF[cutoff])
+    assert rms_rel(g6, o6) <= 1e-5
+    vel = e.get(rid, "vel", n)
+    for kin in (False, True):
+        s = e.stress(rid, include_kinetic=kin)
+        ref = oracle.sample_stress(o6, vel, box, include_kinetic=kin)
+        scale = abs(ref[:3]).mean()
+        assert np.all(np.abs(s[:3] - ref[:3]) <= 1e-5 * np.abs(ref[:3])), (kin, s, ref)
+        assert np.all(np.abs(s[3:] - ref[3:]) <= 1e-5 * scale), (kin, s, ref)
     e.close()

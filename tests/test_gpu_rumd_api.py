@@ -92,10 +92,26 @@ def test_write_read_round_trip(rumd, tmp_path):
     out = tmp_path / "end.xyz.gz"
     s.WriteConf(str(out))
     t = rumd.Sample(0, 0)
-    t.ReadConf(str(out))
+    t2 = rumd.IntegratorNVT(0.001, 1.0, 1.0)
+    t.SetIntegrator(t2)
+    t.ReadConf(str(out), True)
     assert np.allclose(t.GetPositions(), s.GetPositions(), atol=1e-8)
     assert np.array_equal(t.GetImages(), s.GetImages())
     assert np.allclose(t.GetVelocities(), s.GetVelocities(), atol=1e-8)
+    # RUMD's ioformat=2 header (ConfigurationWriterReader.cu:90-141): the box
+    # and integrator as info strings, no ioformat=1 keys
+    import gzip
+    with gzip.open(out, "rt") as fh:
+        fh.readline()
+        meta = dict(tok.split("=", 1) for tok in fh.readline().split())
+    assert meta["ioformat"] == "2" and "boxLengths" not in meta and "dt" not in meta
+    assert meta["sim_box"].startswith("RectangularSimulationBox,")
+    assert [np.float32(x) for x in meta["sim_box"].split(",")[1:]] == [np.float32(x) for x in g["L"]]
+    assert meta["integrator"].split(",")[0] == "IntegratorNVT"
+    assert t2.GetTimeStep() == np.float32(0.005) and t2.GetTargetTemperature() == 0.5
+    # info-string parameters are read as float (ParseInfoString.cc:22)
+    xi = s.GetIntegrator().GetThermostatState()
+    assert abs(t2.GetThermostatState() - xi) <= 1e-6 * max(1.0, abs(xi))
 
 
 def test_pb_tp_do_not_change_physics(rumd, tmp_path):

@@ -3,6 +3,7 @@
 Parameter mapping, configuration files and error behaviour run entirely on
 the host until the first force evaluation creates the device replica."""
 import gzip
+import os
 
 import numpy as np
 import pytest
@@ -71,6 +72,78 @@ def test_readconf_host_side(rumd, tmp_path):
     assert np.allclose(s.GetVelocities(), g["vel"], atol=1e-6)
     assert s.GetNumberOfDOFs() == 3 * 1000 - 3
     assert abs(s.GetVolume() - float(np.prod(g["L"]))) < 1e-3
+
+
+CONF = os.path.join(os.path.dirname(__file__), "golden", "conf")
+
+
+def test_read_rumd_ioformat1_file(rumd):
+    """RUMD's own Conf/KobAndersen/KA_N256_L6.0_T0.50.xyz.gz (ioformat=1:
+    dt, boxLengths, Nose-Hoover-Ps).  Without init_itg the integrator keeps
+    its state; with it the thermostat state comes from the file
+    (Sample.cu:584-600)."""
+    g = load_golden([p for p in golden_files() if "KA_N256_L6.0_T0.50" in p][0])
+    path = os.path.join(CONF, "KA_N256_L6.0_T0.50.xyz.gz")
+    s = rumd.Sample(0, 0)
+    itg = rumd.IntegratorNVT(timeStep=0.005, targetTemperature=0.5, thermostatRelaxationTime=0.2)
+    s.SetIntegrator(itg)
+    s.ReadConf(path)
+    assert itg.GetThermostatState() == 0.0
+    s.ReadConf(path, True)
+    assert abs(itg.GetThermostatState() - 0.568610489) < 1e-6
+    assert s.GetNumberOfParticles() == 256 and s.GetNumberOfTypes() == 2
+    assert abs(s.GetVolume() - 216.0) < 1e-3
+    assert np.allclose(s.GetPositions(), g["pos"], atol=1e-6)
+    assert np.allclose(s.GetVelocities(), g["vel"], atol=1e-6)
+    assert np.array_equal(np.asarray(s.GetImages()).reshape(-1, 3), g["im"])
+
+
+def test_read_rumd_ioformat2_file(rumd):
+    """RUMD's own Conf/SingleComponentLiquid/MgCu_equil_0.051_0.055.xyz.gz
+    (ioformat=2: integrator=IntegratorNVT,dt,T,tau,xi and
+    sim_box=RectangularSimulationBox,Lx,Ly,Lz; masses 24.305 and 63.54).
+    With init_itg the integrator takes the file's info string
+    (IntegratorNVT::InitializeFromInfoString, IntegratorNVT.cu:265-290)."""
+    path = os.path.join(CONF, "MgCu_equil_0.051_0.055.xyz.gz")
+    with gzip.open(path, "rt") as fh:
+        n = int(fh.readline())
+        header = fh.readline().split()
+        rows = np.array([fh.readline().split() for _ in range(n)], np.float64)
+    meta = dict(t.split("=", 1) for t in header)
+    assert meta["ioformat"] == "2"
+    s = rumd.Sample(0, 0)
+    itg = rumd.IntegratorNVT(timeStep=0.001, targetTemperature=1.0, thermostatRelaxationTime=0.2)
+    s.SetIntegrator(itg)
+    s.ReadConf(path, True)
+    assert s.GetNumberOfParticles() == 1000 and s.GetNumberOfTypes() == 2
+    L = np.float32(26.9322929)
+    assert abs(s.GetVolume() - float(L) ** 3) < 1e-2
+    assert np.allclose(s.GetPositions(), rows[:, 1:4], atol=1e-6)
+    assert np.allclose(s.GetVelocities(), rows[:, 7:10], atol=1e-6)
+    assert itg.GetTimeStep() == np.float32(0.5)
+    assert abs(itg.GetTargetTemperature() - 0.0551250086) < 1e-7
+    assert itg.GetRelaxationTime() == np.float32(5.0)
+    assert abs(itg.GetThermostatState() - 0.0240456783) < 1e-8
+    assert abs(s.GetMass(0) - 24.305) < 1e-4 and abs(s.GetMass(1) - 63.54) < 1e-4
+    info = itg.GetInfoString(11)
+    assert info.startswith("IntegratorNVT,0.5,")
+
+
+def test_readconf_rejects_files_without_rumd_metadata(rumd, tmp_path):
+    """ConfigurationMetaData::ReadMetaData's checks: ioformat is required,
+    ioformat=2 takes the box from sim_box= (boxLengths= is an ioformat=1 key),
+    and only the rectangular box is supported here."""
+    cases = {
+        "noioformat": "boxLengths=5,5,5 columns=type,x,y,z",
+        "format2_boxlengths": "ioformat=2 boxLengths=5,5,5 columns=type,x,y,z",
+        "lees_edwards": "ioformat=2 sim_box=LeesEdwardsSimulationBox,5,5,5,0.1 columns=type,x,y,z",
+    }
+    for name, header in cases.items():
+        path = tmp_path / f"{name}.xyz.gz"
+        with gzip.open(path, "wt") as fh:
+            fh.write(f"2\n{header}\n0 0.0 0.0 0.0\n0 1.0 0.0 0.0\n")
+        with pytest.raises(RuntimeError):
+            rumd.Sample(0, 0).ReadConf(str(path))
 
 
 def test_errors_map_to_python_exceptions(rumd, tmp_path):
