@@ -293,6 +293,11 @@ B2MD_API int b2md_probe_cell(const float* x, int n, float box, int nc, int* out)
  * source writes them (IntegratorNVT.cu:385-399, SimulationBox.h:140-155),
  * compiled with default nvcc flags, next to the engine's explicit forms:
  * ref9 / eng9 receive (v, r, image) per particle. */
+/* Measured peaks of the current device for the roofline fractions: L2 read
+ * bandwidth (GB/s, a 48 MiB buffer read past L1) and FP32 FMA throughput
+ * (TFLOP/s, independent FMA chains), best of `trials`, CUDA-event timed.
+ * No counterpart in the reference (measurement only). */
+B2MD_API int b2md_measure_peaks(int trials, double* l2_gbs, double* fma_tflops);
 B2MD_API int b2md_probe_nvt(const float* r4, const float* v4, const float* f4, const float* xi, float dt,
                             const float* box, int n, float* ref9, float* eng9);
 

@@ -347,19 +347,27 @@ static void pair_f64(int kind, double d2, const float* p, double* s, double* u) 
 // (PairPotential.h:1232-1241): sts6[6 i + (xx, yy, zz, yz, xz, xy)] =
 // -sum_j d_a d_b s over the pairs within the cut-off (RUMD keeps xx, yy, zz,
 // yz in sts and xz, xy in w.y, w.z).  sts6 may be null.
+// fp32_cut: a pair is in the sum when the reference's FP32 arithmetic puts
+// it inside the cut-off (dist.w < param[0]*param[0] in float, fij,
+// PairPotential.h:1206-1207) rather than when the FP64 distance does.  With
+// the NS and SP cut-offs the pair force does not vanish at rc, so a pair
+// within a rounding error of rc changes the sum; this option makes the FP64
+// oracle sum exactly the pairs the reference sums.
 ORC_API void orc_forces_stress_f64_pot(int n, const double* pos3, const int* type, const double* L,
                                        int ntypes, const float* params, int cutoff, int potential,
-                                       double* f3, double* u, double* w, double* sts6);
+                                       double* f3, double* u, double* w, double* sts6, int fp32_cut);
 
 ORC_API void orc_forces_f64_pot(int n, const double* pos3, const int* type, const double* L,
                                 int ntypes, const float* params, int cutoff, int potential,
                                 double* f3, double* u, double* w) {
-  orc_forces_stress_f64_pot(n, pos3, type, L, ntypes, params, cutoff, potential, f3, u, w, nullptr);
+  orc_forces_stress_f64_pot(n, pos3, type, L, ntypes, params, cutoff, potential, f3, u, w, nullptr, 0);
 }
 
 ORC_API void orc_forces_stress_f64_pot(int n, const double* pos3, const int* type, const double* L,
                                        int ntypes, const float* params, int cutoff, int potential,
-                                       double* f3, double* u, double* w, double* sts6) {
+                                       double* f3, double* u, double* w, double* sts6, int fp32_cut) {
+  const float Lf[3] = {(float)L[0], (float)L[1], (float)L[2]};
+  const float iLf[3] = {1.f / Lf[0], 1.f / Lf[1], 1.f / Lf[2]};
   double invL[3] = {1. / L[0], 1. / L[1], 1. / L[2]};
   double maxc = 0;
   for (int k = 0; k < ntypes * ntypes; ++k) maxc = std::max(maxc, (double)params[k * NP]);
@@ -403,7 +411,14 @@ ORC_API void orc_forces_stress_f64_pot(int n, const double* pos3, const int* typ
       double d2 = dx * dx + dy * dy + dz * dz;
       const float* p = &params[(type[i] * ntypes + type[j]) * NP];
       double rc = p[0];
-      if (d2 < rc * rc) {
+      bool in = d2 < rc * rc;
+      if (fp32_cut) {
+        const float fx = mi_f32((float)pos3[3 * i] - (float)pos3[3 * j], Lf[0], iLf[0]);
+        const float fy = mi_f32((float)pos3[3 * i + 1] - (float)pos3[3 * j + 1], Lf[1], iLf[1]);
+        const float fz = mi_f32((float)pos3[3 * i + 2] - (float)pos3[3 * j + 2], Lf[2], iLf[2]);
+        in = dist2_ref(fx, fy, fz) < p[0] * p[0];
+      }
+      if (in) {
         double s, uu;
         pair_f64(potential, d2, p, &s, &uu);
         if (cutoff != ORC_NS) {

@@ -49,7 +49,7 @@ def lib():
         L.orc_max_nbrs_estimate.restype = u
         L.orc_forces_f64.argtypes = [i, P, P, P, i, P, i, P, P, P]
         L.orc_forces_f64_pot.argtypes = [i, P, P, P, i, P, i, i, P, P, P]
-        L.orc_forces_stress_f64_pot.argtypes = [i, P, P, P, i, P, i, i, P, P, P, P]
+        L.orc_forces_stress_f64_pot.argtypes = [i, P, P, P, i, P, i, i, P, P, P, P, i]
         L.orc_smooth_set_params.argtypes = [i, P, i, i, f, f, f]
         L.orc_ipl_n_set_params.argtypes = [i, P, i, i, f, f, f, f]
         L.orc_forces_f32.argtypes = [i, P, P, i, P, i, P, P, i, P, P]
@@ -180,15 +180,17 @@ def forces_f64(pos3, types, L, ntypes, params, cutoff, potential="LJ_12_6"):
     return f, u, w
 
 
-def stress_f64(pos3, types, L, ntypes, params, cutoff, potential="LJ_12_6"):
+def stress_f64(pos3, types, L, ntypes, params, cutoff, potential="LJ_12_6", fp32_cut=True):
     """FP64 per-particle pair stress of fij's STR branch (PairPotential.h:1232-1241):
-    [n, 6] = (xx, yy, zz, yz, xz, xy), each -sum_j d_a d_b s."""
+    [n, 6] = (xx, yy, zz, yz, xz, xy), each -sum_j d_a d_b s.  fp32_cut: the
+    pairs summed are those the reference's FP32 cut-off test admits."""
     pos3 = np.ascontiguousarray(pos3, np.float64)
     types = np.ascontiguousarray(types, np.int32)
     n = len(pos3)
     f = np.zeros((n, 3)); u = np.zeros(n); w = np.zeros(n); sts = np.zeros((n, 6))
     lib().orc_forces_stress_f64_pot(n, _p(pos3), _p(types), _p(np.asarray(L, np.float64)), ntypes,
-                                    _p(params), cutoff, POTENTIAL[potential], _p(f), _p(u), _p(w), _p(sts))
+                                    _p(params), cutoff, POTENTIAL[potential], _p(f), _p(u), _p(w), _p(sts),
+                                    int(bool(fp32_cut)))
     return sts
 
 

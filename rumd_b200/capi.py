@@ -38,7 +38,7 @@ EXPORTS = [
     "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
     "b2md_run_queued", "b2md_nbl_export", "b2md_sort_export", "b2md_cell_grid", "b2md_sync",
     "b2md_stream", "b2md_last_error", "b2md_version", "b2md_probe_dist2", "b2md_probe_cell",
-    "b2md_probe_nvt",
+    "b2md_probe_nvt", "b2md_measure_peaks",
     "b2md_forces_noalloc", "b2md_f64_create", "b2md_f64_destroy", "b2md_f64_set_state",
     "b2md_f64_set_integrator", "b2md_f64_set_xi", "b2md_f64_calc_f", "b2md_f64_run", "b2md_f64_get",
     "b2md_f64_stats",
@@ -106,6 +106,7 @@ def lib():
             "b2md_probe_dist2": [P, P, P, i, P],
             "b2md_probe_cell": [P, i, f, i, P],
             "b2md_probe_nvt": [P, P, P, P, f, P, i, P, P],
+            "b2md_measure_peaks": [i, ctypes.POINTER(d), ctypes.POINTER(d)],
             "b2md_forces_noalloc": [P, i, P, i, P, i, P, P, P],
             "b2md_f64_create": [i, i, i, P, P, i, d, i, ctypes.POINTER(P)],
             "b2md_f64_destroy": [P],
@@ -382,6 +383,13 @@ def probe_nvt(r4, v4, f4, xi, dt, box):
     check(lib().b2md_probe_nvt(_ptr(r4), _ptr(v4), _ptr(f4), _ptr(xi), float(dt), _ptr(box), len(r4), _ptr(ref),
                                _ptr(eng)))
     return ref, eng
+
+
+def measure_peaks(trials=5):
+    """(L2 read GB/s, FP32 FMA TFLOP/s) of the current device."""
+    l2, fma = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    check(lib().b2md_measure_peaks(int(trials), ctypes.byref(l2), ctypes.byref(fma)))
+    return l2.value, fma.value
 
 
 F64_STAT_NAMES = ["pe", "virial", "ke", "ke2", "xi", "rebuilds", "steps"]

@@ -2,6 +2,8 @@
 // with nvcc's default floating-point flags (multiply-add contraction on, IEEE
 // division/sqrt), the same as the reference's device build, and evaluates
 // the reference's expressions as written next to the engine's explicit forms.
+#include <algorithm>
+
 #include "../../include/rumd_b200.h"
 #include "pbc_math.cuh"
 
@@ -80,7 +82,88 @@ __global__ void k_probe_nvt(const float4* r, const float4* v, const float4* f, c
   }
 }
 
+// ---- peak microbenchmarks (the denominators of the L2 and FP32 fractions) ----
+
+// Reads an L2-resident buffer of float4 past L1 (ld.global.cg), every block
+// striding over all of it, `reps` times.  One sum per thread is written so
+// the loads are not removed.
+__global__ void k_peak_l2(const float4* __restrict__ buf, size_t n4, int reps, float* sink) {
+  float acc = 0.f;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (int r = 0; r < reps; ++r) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride * 4) {
+      float4 v0 = __ldcg(buf + i);
+      float4 v1 = i + stride < n4 ? __ldcg(buf + i + stride) : make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 v2 = i + 2 * stride < n4 ? __ldcg(buf + i + 2 * stride) : make_float4(0.f, 0.f, 0.f, 0.f);
+      float4 v3 = i + 3 * stride < n4 ? __ldcg(buf + i + 3 * stride) : make_float4(0.f, 0.f, 0.f, 0.f);
+      acc += (v0.x + v1.y) + (v2.z + v3.w);
+    }
+  }
+  if (acc == 1.2345f) sink[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+}
+
+// Eight independent FP32 FMA chains per thread, `iters` rounds: 16 flops per
+// round per thread.
+__global__ void k_peak_fma(float a, float b, int iters, float* sink) {
+  float x0 = threadIdx.x, x1 = x0 + 1.f, x2 = x0 + 2.f, x3 = x0 + 3.f, x4 = x0 + 4.f, x5 = x0 + 5.f, x6 = x0 + 6.f,
+        x7 = x0 + 7.f;
+  for (int i = 0; i < iters; ++i) {
+    x0 = __fmaf_rn(x0, a, b); x1 = __fmaf_rn(x1, a, b); x2 = __fmaf_rn(x2, a, b); x3 = __fmaf_rn(x3, a, b);
+    x4 = __fmaf_rn(x4, a, b); x5 = __fmaf_rn(x5, a, b); x6 = __fmaf_rn(x6, a, b); x7 = __fmaf_rn(x7, a, b);
+  }
+  const float r = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+  if (r == 1.2345f) sink[blockIdx.x * blockDim.x + threadIdx.x] = r;
+}
+
 }  // namespace
+
+// L2 read bandwidth (GB/s) and FP32 FMA throughput (TFLOP/s) of the current
+// device, best of `trials`, timed with CUDA events.  The L2 buffer is 48 MiB
+// (well inside the 126 MB L2, so after the first pass every read hits L2).
+extern "C" int b2md_measure_peaks(int trials, double* l2_gbs, double* fma_tflops) {
+  if (!l2_gbs || !fma_tflops || trials < 1) return B2MD_ERR_ARG;
+  int dev = 0, nsm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return B2MD_ERR_CUDA;
+  const size_t bytes = (size_t)48 << 20, n4 = bytes / sizeof(float4);
+  float4* buf = nullptr;
+  float* sink = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  int rc = B2MD_OK;
+  const int grid = nsm * 8, block = 256, reps = 20, iters = 1 << 14;
+  if (cudaMalloc(&buf, bytes) != cudaSuccess || cudaMalloc(&sink, (size_t)grid * block * sizeof(float)) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    rc = B2MD_ERR_NOMEM;
+  } else {
+    cudaMemset(buf, 0, bytes);
+    k_peak_l2<<<grid, block>>>(buf, n4, 1, sink);  // warm: bring the buffer into L2
+    k_peak_fma<<<grid, block>>>(1.0001f, 0.5f, 64, sink);
+    double best_l2 = 0.0, best_fma = 0.0;
+    for (int t = 0; t < trials; ++t) {
+      float ms = 0.f;
+      cudaEventRecord(e0);
+      k_peak_l2<<<grid, block>>>(buf, n4, reps, sink);
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms > 0.f) best_l2 = std::max(best_l2, (double)bytes * reps / (ms * 1e-3) / 1e9);
+      cudaEventRecord(e0);
+      k_peak_fma<<<grid, block>>>(1.0001f, 0.5f, iters, sink);
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms > 0.f) best_fma = std::max(best_fma, 16.0 * iters * (double)grid * block / (ms * 1e-3) / 1e12);
+    }
+    if (cudaGetLastError() != cudaSuccess) rc = B2MD_ERR_CUDA;
+    *l2_gbs = best_l2;
+    *fma_tflops = best_fma;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(buf);
+  cudaFree(sink);
+  return rc;
+}
 
 extern "C" int b2md_probe_nvt(const float* r4, const float* v4, const float* f4, const float* xi, float dt,
                               const float* box, int n, float* ref9, float* eng9) {

@@ -478,7 +478,10 @@ def test_stress_tensor_against_fp64_oracle(capi, oracle, ka_params, cutoff, tp):
     relative 1e-5 over the components), and Sample::GetStress
     (Sample.cu:393-444) with and without the kinetic part: the diagonal to
     1e-5 relative, the off-diagonal (which fluctuate around zero) to 1e-5 of
-    the diagonal's size.  Non-cubic box, every cut-off method."""
+    the diagonal's size.  Non-cubic box, every cut-off method.  The oracle
+    sums the pairs the reference's FP32 cut-off test admits (with NS and SP
+    the pair force does not vanish at rc, so one pair within a rounding
+    error of rc would otherwise differ between FP32 and FP64)."""
     n = 4000
     m = melted_ka(capi, ka_params, n, steps=80, seed=33, cutoff=cutoff)
     stretch = np.array([1.2, 0.9, 1.0 / 1.08], np.float32)
