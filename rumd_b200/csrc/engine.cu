@@ -137,8 +137,11 @@ struct b2md_engine {
   int wl_rows_cap = 128;       // FM_WINDOW: window-list rows staged in shared memory (0 = stream)
   int build_lanes = 0;         // list build: 0 contiguous candidate runs per lane, else lanes per particle (32: one warp per cell)
   bool build_smem = false;     // list build: tile assembled in shared memory
-  bool persist = true;         // runs: many steps per launch of k_steps between list rebuilds
-  bool persist_on = false;     // the current graphs are the persistent ones
+  int persist = 1;             // runs: 0 one launch per step; 1 persistent (k_steps when every tile has a
+                               // resident block, else k_batch); 2 k_batch whenever it applies
+  bool persist_on = false;     // the current graphs are persistent ones (kind below)
+  int persist_kind = 0;        // 1 k_steps, 2 k_batch
+  int* flist = nullptr;        // k_batch rebuild lists (2 x rcap)
   PersistCtl* pctl = nullptr;  // k_steps control block
   int* h_budget = nullptr;     // pinned: the step budget written before each persistent launch
   void* h_stage = nullptr;     // pinned staging for particle uploads and read-backs (grown on demand)
@@ -304,6 +307,7 @@ void grow_reps(b2md_engine* e, int need) {
   dev_grow(e, e->rep, e->rcap, nc, true);
   dev_grow(e, e->st, e->rcap, nc, true);
   dev_grow(e, e->rctr, 2LL * e->rcap, 2LL * nc, true);  // two halves (k_steps: by step parity)
+  dev_grow(e, e->flist, 2LL * e->rcap, 2LL * nc, true);  // two halves (k_batch: by step parity)
   e->rcap = nc;
   invalidate_graphs(e);
 }
@@ -341,6 +345,8 @@ EngArgs make_args(b2md_engine* e) {
   a.smctr = e->smctr;
   a.win_cap = e->win_cap;
   a.wl_rows = e->force_mode == FM_WINDOW ? std::min(list_rows(a.idx_rows), e->wl_rows_cap & ~7) : 0;
+  a.flist = e->flist;
+  a.bshared_off = 0;
   return a;
 }
 
@@ -804,10 +810,40 @@ StepsFn steps_fn(int tp) {
   }
 }
 
-// Runs may use the persistent step graph: streamed force mode, one block
-// per tile, conditional graph nodes.
+// Runs may use a persistent step graph: streamed force mode, no SM-region
+// tile claiming, conditional graph nodes.
 bool persist_mode(const b2md_engine* e) {
-  return e->persist && e->cond_mode && e->force_mode == FM_STREAMED && !e->sm_tiles;
+  return e->persist != 0 && e->cond_mode && e->force_mode == FM_STREAMED && !e->sm_tiles;
+}
+
+typedef void (*BatchFn)(EngArgs, cudaGraphConditionalHandle);
+
+BatchFn batch_fn(int tp) {
+  switch (tp) {
+    case 1: return k_batch<1>;
+    case 2: return k_batch<2>;
+    case 4: return k_batch<4>;
+    default: return k_batch<8>;
+  }
+}
+
+// k_batch applies when one block can hold a replica's sort and the step's
+// rebuild list: at most kBatchMaxRep replicas of at most kBatchMaxN
+// particles each.
+bool batch_eligible(const b2md_engine* e) {
+  if ((int)e->reps.size() > kBatchMaxRep) return false;
+  for (const auto& h : e->reps)
+    if (h.active && h.n > kBatchMaxN) return false;
+  return true;
+}
+
+// Dynamic shared memory of k_batch: the larger of the force tile's region and
+// the list build's, then the per-block rebuild-list tables.
+size_t batch_smem(const b2md_engine* e, EngArgs& a) {
+  const size_t build = (size_t)kCs2Floats * sizeof(float) + (size_t)(e->pb * e->tp / 32) * 32 * kRunStride * sizeof(int);
+  const size_t tile = std::max(force_smem(e, a), build);
+  a.bshared_off = (int)((tile + 15) & ~(size_t)15);
+  return (size_t)a.bshared_off + sizeof(BatchShared);
 }
 
 // Grid of k_steps: every block resident at once (the launch is cooperative),
@@ -886,6 +922,77 @@ void build_persist_graph(b2md_engine* e) {
   e->gexec[2] = ex;
 }
 
+// The batched persistent graph:
+//   gate_loop -> WHILE(loop) { k_batch }
+// k_batch runs whole steps -- the list rebuilds of the replicas whose lists
+// are due included -- with one grid barrier per step, until the budget is
+// spent, no replica has steps left or a list overflows (the host repairs it
+// and launches again).
+void build_batch_graph(b2md_engine* e) {
+  EngArgs a = make_args(e);
+  const size_t smem = batch_smem(e, a);
+  force_fn(e, true, false, a);  // checks the shared-memory need
+  BatchFn fb = batch_fn(e->tp);
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fb, e->pb * e->tp, smem));
+  if (per_sm < 1) api_fail(B2MD_ERR_NOMEM, "the batched step kernel does not fit on an SM: use a smaller pb*tp");
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  cudaGraphConditionalHandle hl;
+  CK(cudaGraphConditionalHandleCreate(&hl, g, 0, cudaGraphCondAssignDefault));
+  cudaGraphNode_t gate;
+  {
+    cudaKernelNodeParams kp = {};
+    void* args[] = {&a, &hl};
+    kp.func = (void*)k_gate_loop;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(256);
+    kp.kernelParams = args;
+    CK(cudaGraphAddKernelNode(&gate, g, nullptr, 0, &kp));
+  }
+  cudaGraphNodeParams wp = {};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = hl;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  CK(cudaGraphAddNode(&wnode, g, &gate, 1, &wp));
+  cudaGraph_t body = wp.conditional.phGraph_out[0];
+  {
+    cudaKernelNodeParams kp = {};
+    void* args[] = {&a, &hl};
+    kp.func = (void*)fb;
+    kp.gridDim = dim3(std::max(1, per_sm * e->nsm));
+    kp.blockDim = dim3(e->pb * e->tp);
+    kp.sharedMemBytes = (unsigned)smem;
+    kp.kernelParams = args;
+    cudaGraphNode_t knode;
+    CK(cudaGraphAddKernelNode(&knode, body, nullptr, 0, &kp));
+    cudaKernelNodeAttrValue av = {};
+    av.cooperative = 1;
+    CK(cudaGraphKernelNodeSetAttribute(knode, cudaKernelNodeAttributeCooperative, &av));
+  }
+  cudaGraphExec_t ex;
+  CK(cudaGraphInstantiate(&ex, g, 0));
+  e->graph[2] = g;
+  e->gexec[2] = ex;
+}
+
+// Which persistent kernel runs the steps: 1 k_steps (every tile has a
+// resident block), 2 k_batch (more tiles than resident blocks, or asked for
+// with persistent = 2), 0 none (one launch per step).
+int persist_kind_for(b2md_engine* e) {
+  if (!persist_mode(e) || e->ntiles == 0 || e->reps.size() >= (1u << 20)) return 0;  // the barrier tally fields
+  if (e->persist == 1) {
+    EngArgs a = make_args(e);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)steps_fn(e->tp), e->pb * e->tp,
+                                                     persist_smem(e, a)));
+    if ((long long)per_sm * e->nsm >= e->ntiles) return 1;
+  }
+  return batch_eligible(e) ? 2 : 0;
+}
+
 // The persistent graph is used when the whole tile set is resident at once
 // (one tile per block): with several tiles per block its fixed tile order
 // balances worse than the hardware's block scheduling (2.12e9 vs 2.26e9
@@ -894,16 +1001,12 @@ void build_persist_graph(b2md_engine* e) {
 void ensure_graphs(b2md_engine* e) {
   if (e->graphs_valid) return;
   invalidate_graphs(e);
-  e->persist_on = false;
-  if (persist_mode(e) && e->ntiles > 0 && e->reps.size() < (1u << 20)) {  // the barrier word's tally fields
-    EngArgs a = make_args(e);
-    int per_sm = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)steps_fn(e->tp), e->pb * e->tp,
-                                                     persist_smem(e, a)));
-    e->persist_on = (long long)per_sm * e->nsm >= e->ntiles;
-  }
-  if (e->persist_on) {
+  e->persist_kind = persist_kind_for(e);
+  e->persist_on = e->persist_kind != 0;
+  if (e->persist_kind == 1) {
     build_persist_graph(e);
+  } else if (e->persist_kind == 2) {
+    build_batch_graph(e);
   } else {
     build_graph(e, 0, 1);
     build_graph(e, 1, kChunk);
@@ -1114,7 +1217,7 @@ int b2md_engine_destroy(b2md_engine* e) {
   void* ptrs[] = {e->r[0], e->r[1], e->v[0], e->v[1], e->im[0], e->im[1], e->uidx[0], e->uidx[1], e->f, e->w,
                   e->sts, e->last_r, e->nn, e->order, e->key, e->slot, e->nbl, e->cnt, e->cstart, e->par, e->elog,
                   e->rep, e->st, e->rctr, e->tile_rep, e->tile_first, e->ctot, e->cpref, e->tpart, e->gpart,
-                  e->gctr, e->fctr, e->any_rebuild, e->wl, e->wseg, e->wmeta, e->smctr, e->pctl};
+                  e->gctr, e->fctr, e->any_rebuild, e->wl, e->wseg, e->wmeta, e->smctr, e->pctl, e->flist};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (e->h_budget) cudaFreeHost(e->h_budget);
@@ -1199,8 +1302,8 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
       e->build_smem = value != 0;
       break;
     case B2MD_VARIANT_PERSISTENT:
-      if (value != 0 && value != 1) return fail(B2MD_ERR_ARG, "persistent must be 0 or 1");
-      e->persist = value != 0;
+      if (value < 0 || value > 2) return fail(B2MD_ERR_ARG, "persistent must be 0, 1 or 2");
+      e->persist = value;
       break;
     case B2MD_VARIANT_PERSISTENT_ACTIVE:
       return fail(B2MD_ERR_ARG, "persistent_active is read-only");
@@ -1220,8 +1323,8 @@ int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
     case B2MD_VARIANT_WINDOW_CAP: *value = e->win_cap; break;
     case B2MD_VARIANT_BUILD_LANES: *value = e->build_lanes; break;
     case B2MD_VARIANT_BUILD_SMEM: *value = e->build_smem ? 1 : 0; break;
-    case B2MD_VARIANT_PERSISTENT: *value = e->persist ? 1 : 0; break;
-    case B2MD_VARIANT_PERSISTENT_ACTIVE: *value = (e->graphs_valid && e->persist_on) ? 1 : 0; break;
+    case B2MD_VARIANT_PERSISTENT: *value = e->persist; break;
+    case B2MD_VARIANT_PERSISTENT_ACTIVE: *value = (e->graphs_valid && e->persist_on) ? e->persist_kind : 0; break;
     default: return fail(B2MD_ERR_ARG, "unknown variant %d", which);
   }
   return B2MD_OK;
@@ -1725,7 +1828,58 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);
     long long nl = 2;
-    if (persist_mode(e) && e->reps.size() < (1u << 20)) {
+    const int kind = persist_kind_for(e);
+    if (kind == 2) {
+      // the batched graph's loop from the host: k_batch launches (each runs
+      // whole steps, rebuilds included) until the budget is spent
+      const BatchFn fb = batch_fn(e->tp);
+      const size_t bsmem = batch_smem(e, a);
+      force_fn(e, true, false, a);
+      int per_sm = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)fb, e->pb * e->tp, bsmem));
+      if (per_sm < 1) api_fail(B2MD_ERR_NOMEM, "the batched step kernel does not fit on an SM: use a smaller pb*tp");
+      cudaEvent_t e0, e1;
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      int* h_left = nullptr;
+      CK(cudaMallocHost(&h_left, sizeof(int)));
+      int budget = (int)std::min<long long>(nsteps, 1 << 30);
+      double tot = 0.0;
+      cudaGraphConditionalHandle none = 0;
+      for (int guard = 0; budget > 0 && guard < 1 << 20; ++guard) {
+        *e->h_budget = budget;
+        CK(cudaMemcpyAsync(&e->pctl->budget, e->h_budget, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        CK(cudaMemsetAsync(&e->pctl->arrive, 0, sizeof(unsigned long long), e->stream));
+        CK(cudaEventRecord(e0, e->stream));
+        void* args[] = {&a, &none};
+        CK(cudaLaunchCooperativeKernel((const void*)fb, dim3(per_sm * e->nsm), dim3(e->pb * e->tp), args, bsmem,
+                                       e->stream));
+        CK(cudaEventRecord(e1, e->stream));
+        CK(cudaMemcpyAsync(h_left, &e->pctl->budget, sizeof(int), cudaMemcpyDeviceToHost, e->stream));
+        CK(cudaStreamSynchronize(e->stream));
+        check_persist(e);
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        tot += ms;
+        nl += 1;
+        budget = *h_left;
+        if (repair_overflow(e)) {
+          a = make_args(e);  // the repaired list moved
+          batch_smem(e, a);
+          continue;
+        }
+        if (max_steps_left(e) == 0) break;
+      }
+      cudaFreeHost(h_left);
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      calc_f(e, false);
+      CK(cudaStreamSynchronize(e->stream));
+      *step_kernel_ms = tot;
+      *launches = nl + rebuild_launches(e) + 1;
+      return;
+    }
+    if (kind == 1) {
       // the persistent graph's launch sequence with the host taking the loop
       // decision: rebuild kernels (they exit at once when no rebuild is due),
       // then one cooperative k_steps launch that runs steps until a rebuild is

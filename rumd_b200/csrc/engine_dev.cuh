@@ -97,7 +97,7 @@ struct RepState {
   int overflow, nrebuilds;
   int actual_max_nbrs, nlog;
   int err;               // a bounded device wait gave up (reported to the host)
-  int pad_;
+  unsigned sort_done;    // k_batch: epoch of the replica's last in-launch sort
 };
 
 // Control block of the persistent step kernel (k_steps), one per engine.
@@ -107,6 +107,10 @@ struct PersistCtl {
   unsigned gen;     // grid-barrier generation
   int budget;       // steps this graph launch may still run (set by the host)
   int err;          // a grid-barrier wait gave up (reported to the host)
+  unsigned ticket;  // k_batch: work-item tickets claimed in this launch
+  unsigned readers; // k_batch: blocks that have read the step's rebuild list
+  int fcnt[2];      // k_batch: replicas on the rebuild list of steps of each parity
+  int ftiles[2];    // k_batch: their tiles
 };
 
 struct EngArgs {
@@ -157,6 +161,8 @@ struct EngArgs {
   int wl_rows;         // window-list rows k_force stages in shared memory (multiple of 8; 0 = none)
   int nreg;            // SM regions for k_force tile claiming (0 = one tile per block)
   unsigned* smctr;     // per-region claim counters [nreg] + tiles claimed [nreg]
+  int* flist;          // k_batch: rebuild lists, two halves by step parity (replica ids)
+  int bshared_off;     // k_batch: offset of its per-block tables in dynamic shared memory
 };
 
 }  // namespace b2md

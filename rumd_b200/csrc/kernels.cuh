@@ -266,8 +266,11 @@ constexpr unsigned long long kTallyArriveMask = (1ull << kTallyMoreShift) - 1ull
 constexpr unsigned long long kTallyField = (1ull << 20) - 1ull;
 
 // Replica bookkeeping after an integration step (last block only).
+// bpar >= 0 (k_batch): the replica tallies "steps left" with the block's
+// barrier arrival and, when its list is due and it has steps left, joins the
+// rebuild list of the next step (parity bpar).
 __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState* S, const double* tot,
-                            bool with_forces) {
+                            bool with_forces, int bpar = -1) {
   if (threadIdx.x != 0) return;
   // the state is read past L1 (in k_steps the previous step's finalizer may
   // have run on another SM), all loads at once: this runs on the step's
@@ -299,6 +302,15 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
   if (ex > 0) atomicAdd(a.any_rebuild, 1);
+  if (bpar >= 0 && left > 1) {
+    s_step_tally += 1ull << kTallyMoreShift;
+    if (ex > 0) {
+      PersistCtl* c = a.pctl;
+      const int pos = atomicAdd(&c->fcnt[bpar], 1);
+      a.flist[(size_t)bpar * a.rctr_half + pos] = rep;
+      atomicAdd(&c->ftiles[bpar], R.ntiles);
+    }
+  }
   // energies at run steps i with i % interval == 0, as Simulation.Run's
   // energies output schedule (Simulation.py:44, 587-589)
   if (R.energy_interval > 0 && (run_idx % R.energy_interval) == 0 && R.energy_cap > 0) {
@@ -553,6 +565,50 @@ struct IdxStreamed {
                       one(lane_entry<TP>(q + 3, t)));
   }
 };
+// Streamed through L2 only (ld.global.cg): for kernels that rewrite the
+// list while they run (k_batch builds lists and reads them in one launch),
+// where the read-only path may not see those writes.
+__device__ __forceinline__ unsigned ld_cg_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint2 ld_cg_v2(const unsigned* p) {
+  uint2 v;
+  asm volatile("ld.global.cg.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ uint4 ld_cg_v4(const unsigned* p) {
+  uint4 v;
+  asm volatile("ld.global.cg.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p));
+  return v;
+}
+struct IdxStreamedCg {
+  const unsigned* base;
+  unsigned i;
+  size_t stride;
+  __device__ __forceinline__ unsigned one(unsigned k) const { return ld_cg_u32(base + lpos(k, i, stride)); }
+  template <int TP>
+  __device__ __forceinline__ uint4 group(unsigned q, unsigned t) const {
+    constexpr unsigned E = 8 / TP;
+    if (E >= 4) return ld_cg_v4(base + lpos(lane_entry<TP>(q, t), i, stride));
+    if (E == 2) {
+      const uint2 a = ld_cg_v2(base + lpos(lane_entry<TP>(q, t), i, stride));
+      const uint2 b = ld_cg_v2(base + lpos(lane_entry<TP>(q + 2, t), i, stride));
+      return make_uint4(a.x, a.y, b.x, b.y);
+    }
+    return make_uint4(one(lane_entry<TP>(q, t)), one(lane_entry<TP>(q + 1, t)), one(lane_entry<TP>(q + 2, t)),
+                      one(lane_entry<TP>(q + 3, t)));
+  }
+};
+// A position through L1 with a plain (coherent) load, for data the running
+// kernel itself rewrites.
+__device__ __forceinline__ float4 ld_ca_f4(const float4* p) {
+  float4 v;
+  asm volatile("ld.global.ca.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+  return v;
+}
+
 // Staged: the tile's list blocks copied to shared memory, block b of slot lp
 // at p[(b * pb + lp) * 8]; p points at this particle's first block.
 struct IdxStaged {
@@ -764,12 +820,15 @@ struct PersistRegs {
   unsigned nn;
 };
 
-template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST>
+// COH (k_batch): positions and lists that the same launch rewrites are read
+// with coherent loads (no read-only path); bpar: the batch rebuild-list parity
+// passed to finish_step.
+template <int TP, bool FUSED, bool STRESS, int MODE, bool PERSIST, bool COH = false>
 __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned char* s_dyn, double* s_blk,
                                            double* s_tot, uint64_t& s_bar, unsigned& s_rows,
                                            const StepView* pv = nullptr, int gpar = 0,
                                            const RepDev* prep = nullptr, PersistRegs* pr = nullptr,
-                                           unsigned* wdone = nullptr) {
+                                           unsigned* wdone = nullptr, int bpar = -1) {
   float* s_par = reinterpret_cast<float*>(s_dyn);
   unsigned* s_idx = reinterpret_cast<unsigned*>(s_dyn + kParSmemFloats * sizeof(float));
   float4* s_win = reinterpret_cast<float4*>(s_dyn + kParSmemFloats * sizeof(float));
@@ -859,7 +918,7 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
     const bool valid = i < R.n;
     const float Lx = R.L[0], Ly = R.L[1], Lz = R.L[2];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
-    const float4 ri = valid ? (PERSIST ? rc[i] : __ldg(rc + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 ri = valid ? ((PERSIST || COH) ? rc[i] : __ldg(rc + i)) : make_float4(0.f, 0.f, 0.f, 0.f);
     const int ti = valid ? __float_as_int(ri.w) : 0;
     const float* prow = s_par + ti * nt * kParStride;
     const unsigned nn = valid ? (PERSIST ? pr->nn : a.nn[R.p0 + i]) : 0u;
@@ -895,9 +954,10 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
       }
     } else {
       if (!PERSIST) __syncthreads();  // the pair table (k_steps loads it once per launch)
-      using PosS = typename Pick<PERSIST, PosCoherent, PosGlobal>::type;
-      force_loop_any<TP, STRESS, true>(fast, R.potential, nt, A, IdxStreamed{lbase, (unsigned)i, lstride}, PosS{rc}, lane_t, nn, ri, prow, Lx, Ly,
-                                 Lz, iLx, iLy, iLz);
+      using PosS = typename Pick<PERSIST || COH, PosCoherent, PosGlobal>::type;
+      using IdxS = typename Pick<COH, IdxStreamedCg, IdxStreamed>::type;
+      force_loop_any<TP, STRESS, true>(fast, R.potential, nt, A, IdxS{lbase, (unsigned)i, lstride}, PosS{rc}, lane_t, nn,
+                                       ri, prow, Lx, Ly, Lz, iLx, iLy, iLz);
     }
     float fx = A.fx, fy = A.fy, fz = A.fz, uu = A.uu, ww = A.ww;
     double sxx = A.sxx, syy = A.syy, szz = A.szz, syz = A.syz, sxz = A.sxz, sxy = A.sxy;
@@ -995,7 +1055,7 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
       block_sum8(acc, s_warp, s_blk);
       if (replica_reduce(a, rep, R, tile - R.tile0, s_blk, s_scr, s_tot)) {
         if (FUSED) {
-          finish_step(a, rep, R, S, s_tot, true);
+          finish_step(a, rep, R, S, s_tot, true, bpar);
         } else if (threadIdx.x == 0) {
           S->pe = s_tot[P_PE];
           S->vir = s_tot[P_W] / 6.0;
@@ -2285,8 +2345,8 @@ struct Cs2Table {
 // Accept bits of a lane's run for up to four of the cell's particles (a
 // missing one repeats the last; its bits are unused): each candidate's
 // position is read once and tested against all four.
-template <bool WRAP, class CS2>
-__device__ __forceinline__ void run_tests4(const int* __restrict__ run, int nrun, const float4* __restrict__ rc,
+template <bool WRAP, bool COH, class CS2>
+__device__ __forceinline__ void run_tests4(const int* __restrict__ run, int nrun, const float4* rc,
                                            const float4 (&rp)[4], const int (&ip)[4], const CS2 (&cs)[4],
                                            float Lx, float Ly, float Lz, float iLx, float iLy, float iLz,
                                            unsigned (&bits)[4]) {
@@ -2296,7 +2356,7 @@ __device__ __forceinline__ void run_tests4(const int* __restrict__ run, int nrun
   for (int k = 0; k < kRunMax; ++k) {
     if (k < nrun) {
       const int j = run[k];
-      const float4 rj = __ldg(rc + j);
+      const float4 rj = COH ? ld_ca_f4(rc + j) : __ldg(rc + j);
       const int tj = __float_as_int(rj.w);
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
@@ -2337,32 +2397,35 @@ __device__ __forceinline__ int run_store(unsigned bits, const int* __restrict__ 
   return __shfl_sync(0xffffffffu, incl, 31);
 }
 
-__global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
+// The run build of one tile by the calling block (blockDim a multiple of 32:
+// one cell per warp at a time).  s_cs2: the cut-off table (kCs2Floats),
+// s_run: 32 * kRunStride ints per warp, s_max: one int.  COH: the positions
+// and cell arrays were written earlier in the same launch (k_batch), so they
+// are read with coherent loads.
+template <bool COH>
+__device__ __noinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
   constexpr unsigned FULL = 0xffffffffu;
-  __shared__ float s_cs2[kCs2Floats];
-  __shared__ int s_run[kRunWarps][32 * kRunStride];
-  __shared__ int s_max;
-  const int tile = blockIdx.x, rep = a.tile_rep[tile];
-  if (!rb_active(a, rep)) return;
+  const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
   const int nt = R.ntypes;
+  const int nwarps = blockDim.x >> 5;
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
-  if (threadIdx.x == 0) s_max = 0;
+  if (threadIdx.x == 0) *s_max = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int first = a.tile_first[tile];
   const int last = (tile + 1 < R.tile0 + R.ntiles) ? a.tile_first[tile + 1] : R.n;
-  const float4* __restrict__ rc = a.r[S->rbuf] + R.p0;
+  const float4* rc = a.r[COH ? __ldcg(&S->rbuf) : S->rbuf] + R.p0;
   const int maxn = R.max_nbrs;
   const unsigned stride8 = 8u * (unsigned)R.nbl_stride;
   unsigned* __restrict__ lbase = a.nbl + R.nbl0;
-  int* wrun = s_run[warp];
+  int* wrun = s_run + warp * 32 * kRunStride;
   const int* run = wrun + lane * kRunStride;
   const bool cells = R.nb_method == NB_CELLS;
   const int nx = R.nc[0], ny = R.nc[1], nz = R.nc[2];
-  const int* __restrict__ cbeg = a.cstart + R.cell0;  // absolute first slot (k_rb_fix)
-  const int* __restrict__ ccnt = a.cnt + R.cell0;
+  const int* cbeg = a.cstart + R.cell0;  // absolute first slot (k_rb_fix / block_sort)
+  const int* ccnt = a.cnt + R.cell0;
   // units of work: the cells from the first to the last particle's (keys
   // ascend along the slots), or one unit for all pairs
   int k0 = 0, k1 = 0;
@@ -2373,7 +2436,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
     k1 = cell_coord(rl.x, iLx, nx) + cell_coord(rl.y, iLy, ny) * nx + cell_coord(rl.z, iLz, nz) * nx * ny;
   }
   int wmax = 0;
-  for (int c = k0 + warp; c <= k1; c += kRunWarps) {
+  for (int c = k0 + warp; c <= k1; c += nwarps) {
     const int p0 = cells ? max(cbeg[c], first) : first;
     const int p1 = cells ? min(cbeg[c] + ccnt[c], last) : last;
     if (p0 >= p1) continue;  // no particle of this tile in the cell
@@ -2461,7 +2524,7 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
 #define RUNS(W, T, MK)                                                                                    \
   {                                                                                                       \
     const T cs[4] = {MK(crow[0]), MK(crow[1]), MK(crow[2]), MK(crow[3])};                                 \
-    run_tests4<W>(run, nrun, rc, rp, ip, cs, R.L[0], R.L[1], R.L[2], R.invL[0], R.invL[1], R.invL[2], bits); \
+    run_tests4<W, COH>(run, nrun, rc, rp, ip, cs, R.L[0], R.L[1], R.L[2], R.invL[0], R.invL[1], R.invL[2], bits); \
   }
 #define ONE(c) Cs2One{(c)[0]}
 #define TWO(c) Cs2Two{(c)[0], (c)[1]}
@@ -2496,19 +2559,377 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
     }
   }
   wmax = __reduce_max_sync(FULL, wmax);
-  if (lane == 0) atomicMax(&s_max, wmax);
+  if (lane == 0) atomicMax(s_max, wmax);
   __syncthreads();
   if (threadIdx.x == 0) {
-    const int s_max_v = s_max;
+    const int s_max_v = *s_max;
     atomicMax(&S->actual_max_nbrs, s_max_v);
-    if (s_max_v > R.max_nbrs) atomicExch(&S->overflow, 1);
+    if (s_max_v > R.max_nbrs) {
+      atomicExch(&S->overflow, 1);
+      if (COH) s_step_tally += 1ull << kTallyRebuildShift;  // k_batch: the launch stops at the step's end
+    }
     __threadfence();
     const unsigned cdone = atomicAdd(&a.rctr[rep], 1u);
     if (cdone == (unsigned)(R.ntiles - 1)) {
       a.rctr[rep] = 0u;
-      S->rebuild = 0;
       S->nrebuilds += 1;
+      // the replica's lists are complete: released to k_batch's force items
+      st_release_u32(reinterpret_cast<unsigned*>(&S->rebuild), 0u);
     }
+  }
+}
+
+__global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
+  __shared__ float s_cs2[kCs2Floats];
+  __shared__ int s_run[kRunWarps * 32 * kRunStride];
+  __shared__ int s_max;
+  if (!rb_active(a, a.tile_rep[blockIdx.x])) return;
+  build_runs_tile<false>(a, blockIdx.x, s_cs2, s_run, &s_max);
+}
+
+// ---------------------------------------------------------------------------
+// Batched persistent launch (k_batch): many replicas, any number of tiles
+// per block, list rebuilds inside the launch.
+// ---------------------------------------------------------------------------
+
+// Block-wide exclusive scan of one int per thread (blockDim a multiple of
+// 32, at most 1024); returns the thread's exclusive prefix, *total the sum.
+// s_w: 33 ints of shared memory.
+__device__ __forceinline__ int block_excl_scan(int x, int* s_w, int* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_w[wid] = incl;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int w = 0; w < nw; ++w) {
+      const int t = s_w[w];
+      s_w[w] = run;
+      run += t;
+    }
+    s_w[32] = run;
+  }
+  __syncthreads();
+  const int out = s_w[wid] + incl - x;
+  *total = s_w[32];
+  __syncthreads();
+  return out;
+}
+
+// The stable cell-key sort of one replica by the calling block, the same
+// permutation as the sort kernels (k_rb_clear .. k_rb_permute; RUMD's
+// thrust::sort_by_key on (cell key, current slot), Sample.h:174-188):
+// count with an arrival rank per cell, exclusive scan of the counts into
+// absolute cell starts, scatter, order each bucket by current slot, gather
+// r, v, images and ids into the other buffers, flip the parities, and
+// publish the sort (release) under `epoch`.  s_w: 33 ints of shared memory.
+__device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoch, int* s_w) {
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  const int tid = threadIdx.x, bd = blockDim.x;
+  if (R.nb_method == NB_CELLS) {
+    const int rb = __ldcg(&S->rbuf), ab = __ldcg(&S->abuf);
+    const int n = R.n, ncell = R.ncell;
+    const size_t p0 = (size_t)R.p0;
+    int* cnt = a.cnt + R.cell0;
+    int* cst = a.cstart + R.cell0;
+    for (int c = tid; c < ncell; c += bd) cnt[c] = 0;
+    __syncthreads();
+    // cell key (calculateCellIndices, NeighborList.cu:1142-1172) and arrival rank
+    for (int i = tid; i < n; i += bd) {
+      const float4 r = a.r[rb][p0 + i];
+      const int key = cell_coord(r.x, R.invL[0], R.nc[0]) + cell_coord(r.y, R.invL[1], R.nc[1]) * R.nc[0] +
+                      cell_coord(r.z, R.invL[2], R.nc[2]) * R.nc[0] * R.nc[1];
+      a.key[p0 + i] = key;
+      a.slot[p0 + i] = atomicAdd(&cnt[key], 1);
+    }
+    __syncthreads();
+    // absolute first slot of every cell
+    int carry = 0;
+    for (int base = 0; base < ncell; base += bd) {
+      const int c = base + tid;
+      const int x = c < ncell ? cnt[c] : 0;
+      int tot;
+      const int ex = block_excl_scan(x, s_w, &tot);
+      if (c < ncell) cst[c] = carry + ex;
+      carry += tot;
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += bd) a.order[p0 + cst[a.key[p0 + i]] + a.slot[p0 + i]] = (unsigned)i;
+    __syncthreads();
+    // each bucket by current slot: the result is the stable sort by key
+    for (int c = tid; c < ncell; c += bd) {
+      unsigned* o = a.order + p0 + cst[c];
+      const int m = cnt[c];
+      for (int q = 1; q < m; ++q) {
+        const unsigned x = o[q];
+        int k = q - 1;
+        while (k >= 0 && o[k] > x) {
+          o[k + 1] = o[k];
+          --k;
+        }
+        o[k + 1] = x;
+      }
+    }
+    __syncthreads();
+    // ParticleData::UpdateAfterSorting (ParticleData.cu:493-528)
+    for (int sl = tid; sl < n; sl += bd) {
+      const size_t gs = p0 + sl, go = p0 + a.order[p0 + sl];
+      a.r[rb ^ 1][gs] = a.r[rb][go];
+      a.v[ab ^ 1][gs] = a.v[ab][go];
+      a.im[ab ^ 1][gs] = a.im[ab][go];
+      a.uidx[ab ^ 1][gs] = a.uidx[ab][go];
+    }
+    __syncthreads();
+    if (tid == 0) {
+      S->rbuf = rb ^ 1;
+      S->abuf = ab ^ 1;
+    }
+  }
+  if (tid == 0) {
+    S->actual_max_nbrs = 0;  // the per-build maximum (k_rb_clear)
+    __threadfence();
+    st_release_u32(&S->sort_done, epoch);
+  }
+  __syncthreads();
+}
+
+// Bounded wait of thread 0 until *p == want (acquire); false when it gave up.
+__device__ __forceinline__ bool wait_eq_u32(const unsigned* p, unsigned want) {
+  for (unsigned it = 0; ld_acquire_u32(p) != want; ++it) {
+    if (it >= kWaitPolls) return false;
+    __nanosleep(64);
+  }
+  return true;
+}
+
+constexpr int kBatchMaxRep = 1024;   // replicas whose rebuild list a block holds in shared memory
+constexpr int kBatchMaxN = 65536;    // particles per replica (one block sorts a replica)
+constexpr int kBatchEpochSteps = 4096;  // epochs: launch generation * this + step + 1
+
+// Shared memory of k_batch after the tile's dynamic region: the step's
+// rebuild list (replica ids) and the prefix of their tile counts, and a bit
+// per replica that is on it.
+struct BatchShared {
+  int list[kBatchMaxRep];
+  int pref[kBatchMaxRep + 1];
+  unsigned bits[kBatchMaxRep / 32];
+  int scan[33];
+};
+
+// Every MD step of many replicas in one cooperative launch.  Per step the
+// blocks claim work items in ticket order (one atomic counter):
+//   1. the stable sort of each replica on the step's rebuild list (one block
+//      sorts one replica, block_sort);
+//   2. the fused force + Nose-Hoover tile of every tile of the other
+//      replicas (force_tile, as k_force);
+//   3. the list build of every tile of the listed replicas (build_runs_tile),
+//      each after its replica's sort (bounded wait on sort_done);
+//   4. their fused force + Nose-Hoover tiles, each after all of its
+//      replica's builds (bounded wait on the replica's rebuild flag, which
+//      the last build clears with release).
+// Every wait is on an item with an earlier ticket, taken by a running block
+// that does not wait on later items, so the claims always progress.  A
+// replica's arithmetic is that of the other paths (the same sort, list,
+// per-tile sums and reduction tree), whatever block runs which item.  The
+// replica finalizers put the replicas whose lists are due on the next step's
+// rebuild list (two lists alternated by step parity) and tally "steps left";
+// one grid barrier ends each step, after which every block takes the same
+// decision: stop when no replica has steps left, the budget is spent, a list
+// overflowed (the host repairs it) or a wait gave up.
+template <int TP>
+__global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_loop) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ unsigned s_rows, s_gen;
+  __shared__ int s_go, s_item, s_ok, s_max;
+  __shared__ unsigned long long s_now;
+  BatchShared* bs = reinterpret_cast<BatchShared*>(s_dyn + a.bshared_off);
+  PersistCtl* c = a.pctl;
+  if (threadIdx.x == 0) {
+    s_go = __ldcg(&c->err) == 0;
+    if (!s_go && blockIdx.x == 0) set_loop(h_loop, 0u);
+  }
+  __syncthreads();
+  // setup barrier; its last block zeroes the step words and the tickets and
+  // puts the replicas whose lists are due on the first step's rebuild list
+  if (s_go) {
+    if (threadIdx.x == 0) {
+      s_gen = ld_acquire_u32(&c->gen);
+      const unsigned long long nnow = atom_add_acq_rel_u64(&c->arrive, 1ull) + 1ull;
+      s_item = (nnow & kTallyArriveMask) == gridDim.x;
+    }
+    __syncthreads();
+    if (s_item) {
+      if (threadIdx.x == 0) {
+        c->word[0] = 0ull;
+        c->word[1] = 0ull;
+        c->ticket = 0u;
+        c->readers = 0u;
+        c->fcnt[0] = c->fcnt[1] = 0;
+        c->ftiles[0] = c->ftiles[1] = 0;
+        *a.any_rebuild = 0;
+      }
+      __syncthreads();
+      for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) {
+        const RepState* S = a.st + r;
+        if (a.rep[r].active && S->rebuild && !S->overflow && S->steps_left > 0) {
+          const int pos = atomicAdd(&c->fcnt[0], 1);
+          a.flist[pos] = r;
+          atomicAdd(&c->ftiles[0], a.rep[r].ntiles);
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        c->arrive = 0ull;
+        __threadfence();
+        st_release_u32(&c->gen, s_gen + 1u);
+      }
+    } else if (threadIdx.x == 0) {
+      s_go = barrier_wait(c, s_gen, h_loop);
+    }
+    __syncthreads();
+  }
+  const unsigned gen = s_gen;
+  int budget = __ldcg(&c->budget);
+  unsigned long long seen[2] = {0ull, 0ull};
+  unsigned base = 0;  // tickets of the steps before this one
+  for (int step = 0; s_go; ++step) {
+    const int par = step & 1;
+    const unsigned epoch = gen * kBatchEpochSteps + (unsigned)step + 1u;
+    // the step's rebuild list: every block reads the same one (its last
+    // reader clears it for reuse two steps on)
+    if (threadIdx.x == 0) {
+      s_step_tally = 0ull;
+      s_max = __ldcg(&c->fcnt[par]);
+    }
+    __syncthreads();
+    const int nf = min(s_max, kBatchMaxRep);
+    for (int k = threadIdx.x; k < kBatchMaxRep / 32; k += blockDim.x) bs->bits[k] = 0u;
+    __syncthreads();
+    int run = 0;
+    for (int k0 = 0; k0 < nf; k0 += blockDim.x) {
+      const int k = k0 + threadIdx.x;
+      const int r = k < nf ? __ldcg(a.flist + (size_t)par * a.rctr_half + k) : 0;
+      const int nt = k < nf ? a.rep[r].ntiles : 0;
+      int tot;
+      const int ex = block_excl_scan(nt, bs->scan, &tot);
+      if (k < nf) {
+        bs->list[k] = r;
+        bs->pref[k] = run + ex;
+        atomicOr(&bs->bits[r >> 5], 1u << (r & 31));
+      }
+      run += tot;
+    }
+    if (threadIdx.x == 0) {
+      bs->pref[nf] = run;
+      __threadfence();
+      if (atomicAdd(&c->readers, 1u) == gridDim.x - 1) {
+        c->readers = 0u;
+        c->fcnt[par] = 0;
+        c->ftiles[par] = 0;
+      }
+    }
+    __syncthreads();
+    const int t2 = run;                       // tiles of the listed replicas
+    const unsigned items = (unsigned)(nf + a.ntiles + 2 * t2);
+    // claim items until the step's are gone (each block overshoots once)
+    for (;;) {
+      if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - base);
+      __syncthreads();
+      const unsigned it = (unsigned)s_item;
+      if (it >= items) break;
+      if (it < (unsigned)nf) {
+        block_sort(a, bs->list[it], epoch, bs->scan);
+      } else if (it < (unsigned)(nf + a.ntiles)) {
+        const int tile = (int)it - nf;
+        const int r = a.tile_rep[tile];
+        if (!((bs->bits[r >> 5] >> (r & 31)) & 1u))
+          force_tile<TP, true, false, FM_STREAMED, false, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, nullptr,
+                                                                0, nullptr, nullptr, nullptr, par ^ 1);
+      } else {
+        const bool build = it < (unsigned)(nf + a.ntiles + t2);
+        const int k = (int)it - nf - a.ntiles - (build ? 0 : t2);
+        int lo = 0, hi = nf - 1;  // the listed replica holding flagged tile k
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (bs->pref[mid] <= k) lo = mid;
+          else hi = mid - 1;
+        }
+        const int r = bs->list[lo];
+        const int tile = a.rep[r].tile0 + (k - bs->pref[lo]);
+        RepState* S = a.st + r;
+        if (threadIdx.x == 0) {
+          s_ok = build ? wait_eq_u32(&S->sort_done, epoch)
+                       : wait_eq_u32(reinterpret_cast<const unsigned*>(&S->rebuild), 0u);
+          if (!s_ok) {
+            // recorded for the host and tallied with the barrier arrival, so
+            // that every block stops after this step
+            atomicExch(&c->err, 1);
+            s_step_tally += 1ull << kTallyRebuildShift;
+          }
+        }
+        __syncthreads();
+        if (s_ok) {
+          if (build) {
+            float* s_cs2 = reinterpret_cast<float*>(s_dyn);
+            int* s_run = reinterpret_cast<int*>(s_dyn + kCs2Floats * sizeof(float));
+            build_runs_tile<true>(a, tile, s_cs2, s_run, &s_max);
+          } else {
+            force_tile<TP, true, false, FM_STREAMED, false, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows,
+                                                                  nullptr, 0, nullptr, nullptr, nullptr, par ^ 1);
+          }
+        }
+      }
+      __syncthreads();
+    }
+    base += items + gridDim.x;
+    budget -= 1;
+    // step barrier: arrival + "steps left" and overflow tallies
+    if (threadIdx.x == 0) {
+      const unsigned long long mine = 1ull + s_step_tally;
+      const unsigned long long now = atom_add_acq_rel_u64(&c->word[par], mine) + mine;
+      const unsigned long long base_w = seen[par];
+      const bool last = ((now - base_w) & kTallyArriveMask) == gridDim.x;
+      unsigned long long tot = now;
+      int ok = 1;
+      if (!last) {
+        for (unsigned it = 0;; ++it) {
+          tot = ld_acquire_u64(&c->word[par]);
+          if (((tot - base_w) & kTallyArriveMask) == gridDim.x) break;
+          if (it >= kBarrierPolls) {
+            atomicExch(&c->err, 1);
+            set_loop(h_loop, 0u);
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      seen[par] = tot;
+      const unsigned long long d = tot - base_w;
+      const unsigned more = (unsigned)((d >> kTallyMoreShift) & kTallyField);
+      // list overflows and waits that gave up: the host repairs or reports
+      const unsigned stop = (unsigned)((d >> kTallyRebuildShift) & kTallyField);
+      // steps per launch: the epochs' and the tally fields' range, and the
+      // 32-bit ticket counter (at most nrep + 3 ntiles + grid tickets a step)
+      const unsigned per_step = (unsigned)a.nrep + 3u * (unsigned)a.ntiles + gridDim.x;
+      const int cap = min(min(kBatchEpochSteps - 2, (int)(kTallyField / (unsigned)(a.nrep + 1))),
+                          (int)min(0x7fffffffu, 0xffffffffu / per_step));
+      const int go = ok && stop == 0 && more > 0 && budget > 0 && step + 1 < cap;
+      if (last && !go) {
+        c->budget = budget;
+        set_loop(h_loop, (stop == 0 && more > 0 && budget > 0) ? 1u : 0u);
+      }
+      s_go = go;
+    }
+    __syncthreads();
   }
 }
 

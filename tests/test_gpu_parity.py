@@ -375,13 +375,18 @@ def test_conditional_and_plain_graphs_agree(capi, ka_params):
     assert res[0][1]["rebuilds"] == res[1][1]["rebuilds"]
 
 
-def test_replica_in_batch_equals_alone(capi, ka_params, oracle):
+@pytest.mark.parametrize("persistent", [1, 2])
+def test_replica_in_batch_equals_alone(capi, ka_params, oracle, persistent):
+    """A replica advanced in a batch -- by the step graphs with k_steps
+    (persistent = 1) or by the batched kernel k_batch with its in-launch
+    rebuilds (persistent = 2) -- ends bit for bit where it ends alone."""
     from rumd_b200 import initconf as I
     sizes = [600, 2048, 777, 5000]
     temps = [0.5, 1.0, 1.5, 2.0]
     confs = [I.ka_config(s, T=t, seed=s) for s, t in zip(sizes, temps)]
     steps = 300
     batch = new_engine(capi)
+    batch.set_variant(capi.VARIANT_PERSISTENT, persistent)
     ids = [batch.add(c["pos4"], c["box"], ka_params, 2, cutoff="SF", dt=0.005, T=t, vel4=c["vel4"])
            for c, t in zip(confs, temps)]
     batch.run(steps)
@@ -391,6 +396,7 @@ def test_replica_in_batch_equals_alone(capi, ka_params, oracle):
         alone.run(steps)
         assert np.array_equal(alone.get(a, "pos", s), batch.get(rid, "pos", s))
         assert alone.stats(a)["xi"] == batch.stats(rid)["xi"]
+        assert alone.stats(a)["rebuilds"] == batch.stats(rid)["rebuilds"]
         alone.close()
     batch.close()
 
