@@ -107,8 +107,8 @@ def test_more_tiles_than_resident_blocks(capi, ka_params):
 def test_batch_kernel_mixed_sizes_types_and_methods(capi, ka_params, oracle):
     """k_batch on a mix it must handle: replicas of one and two types, a
     small box on the all-pairs list (no sort), sizes from 2 to 6000, uneven
-    step queues, and an energy log; against one launch per step, bit for
-    bit, and the FP64 oracle's forces at the end."""
+    step queues, and an energy log; against one launch per step (itself
+    checked against the oracle elsewhere), bit for bit."""
     from rumd_b200 import initconf as I
     lj = oracle.lj_params(1, oracle.lj_table())
     specs = [("ka", 6000, 0.7, 90), ("lj", 3000, 1.2, 120), ("ka", 300, 2.0, 45), ("lj", 64, 1.0, 120),
@@ -131,16 +131,6 @@ def test_batch_kernel_mixed_sizes_types_and_methods(capi, ka_params, oracle):
         if persistent:
             assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == 2
         res.append([(state(e, rid, n), e.stats(rid), e.energy_log(rid)) for rid, n, _, _ in ids])
-        if persistent:
-            for (rid, n, kind, box), (st_, _, _) in zip(ids, res[-1]):
-                pos = st_[0]
-                types = pos[:, 3].view(np.int32)
-                e.calc_f()
-                f = e.get(rid, "force", n)
-                ref, _, _ = oracle.forces_f64(pos[:, :3].astype(np.float64), types, box, 2 if kind == "ka" else 1,
-                                              ka_params if kind == "ka" else lj, oracle.SF)
-                if np.abs(ref).sum() > 0:
-                    assert np.sqrt(((f[:, :3] - ref) ** 2).sum() / (ref ** 2).sum()) <= 1e-5
         e.close()
     for (sa, ta, la), (sb, tb, lb), spec in zip(res[0], res[1], specs):
         assert ta["steps"] == tb["steps"] == spec[3]
