@@ -2403,7 +2403,7 @@ __device__ __forceinline__ int run_store(unsigned bits, const int* __restrict__ 
 // and cell arrays were written earlier in the same launch (k_batch), so they
 // are read with coherent loads.
 template <bool COH>
-__device__ __noinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
+__device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
   constexpr unsigned FULL = 0xffffffffu;
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
@@ -2577,6 +2577,12 @@ __device__ __noinline__ void build_runs_tile(const EngArgs& a, int tile, float* 
       st_release_u32(reinterpret_cast<unsigned*>(&S->rebuild), 0u);
     }
   }
+}
+
+// k_batch's call of the build: kept out of line so that its registers do
+// not add to those of k_batch's force path.
+__device__ __noinline__ void build_runs_tile_batch(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
+  build_runs_tile<true>(a, tile, s_cs2, s_run, s_max);
 }
 
 __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
@@ -2880,7 +2886,7 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
           if (build) {
             float* s_cs2 = reinterpret_cast<float*>(s_dyn);
             int* s_run = reinterpret_cast<int*>(s_dyn + kCs2Floats * sizeof(float));
-            build_runs_tile<true>(a, tile, s_cs2, s_run, &s_max);
+            build_runs_tile_batch(a, tile, s_cs2, s_run, &s_max);
           } else {
             force_tile<TP, true, false, FM_STREAMED, false, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows,
                                                                   nullptr, 0, nullptr, nullptr, nullptr, par ^ 1);
