@@ -398,6 +398,7 @@ def batched(capi, device, pb, tp, steps, seed=0):
     e.run(500)
     t_b = time_run(capi, e, steps, device)
     rate_b = float(ns.sum()) * steps / t_b
+    kind = e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE)
     e.close()
     sample = list(range(0, R, 16))
     t_seq, ps_seq = 0.0, 0.0
@@ -411,7 +412,9 @@ def batched(capi, device, pb, tp, steps, seed=0):
         s.close()
     rate_s = ps_seq / t_seq
     return {"value": rate_b, "unit": "particle-steps/s", "replicas": R, "particles": int(ns.sum()),
-            "steps": steps, "sequential_plain_value": rate_s,
+            "steps": steps, "ms_per_step": t_b / steps * 1e3,
+            "persistent_kernel": {0: "none (one launch per step)", 1: "k_steps", 2: "k_batch"}.get(kind, kind),
+            "sequential_plain_value": rate_s,
             "sequential_sample": f"{len(sample)} of the {R} replicas run alone, one after another",
             "speedup_vs_sequential": rate_b / rate_s}
 

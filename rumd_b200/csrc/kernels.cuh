@@ -2753,9 +2753,14 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
   extern __shared__ __align__(128) unsigned char s_dyn[];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
   __shared__ __align__(8) uint64_t s_bar;
-  __shared__ unsigned s_rows, s_gen;
+  __shared__ unsigned s_rows;
   __shared__ int s_go, s_item, s_ok, s_max;
-  __shared__ unsigned long long s_now;
+  // the loop's bookkeeping, kept out of registers for the force path: the
+  // launch generation, the step budget, the tickets of the steps so far, the
+  // step barrier words' totals, the step's rebuild-list size and its tiles
+  __shared__ unsigned s_gen, s_base;
+  __shared__ int s_budget, s_nf, s_t2;
+  __shared__ unsigned long long s_seen[2];
   BatchShared* bs = reinterpret_cast<BatchShared*>(s_dyn + a.bshared_off);
   PersistCtl* c = a.pctl;
   if (threadIdx.x == 0) {
@@ -2800,59 +2805,61 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     } else if (threadIdx.x == 0) {
       s_go = barrier_wait(c, s_gen, h_loop);
     }
+    if (threadIdx.x == 0) {
+      s_budget = __ldcg(&c->budget);
+      s_base = 0u;
+      s_seen[0] = s_seen[1] = 0ull;
+    }
     __syncthreads();
   }
-  const unsigned gen = s_gen;
-  int budget = __ldcg(&c->budget);
-  unsigned long long seen[2] = {0ull, 0ull};
-  unsigned base = 0;  // tickets of the steps before this one
   for (int step = 0; s_go; ++step) {
     const int par = step & 1;
-    const unsigned epoch = gen * kBatchEpochSteps + (unsigned)step + 1u;
     // the step's rebuild list: every block reads the same one (its last
     // reader clears it for reuse two steps on)
     if (threadIdx.x == 0) {
       s_step_tally = 0ull;
-      s_max = __ldcg(&c->fcnt[par]);
+      s_nf = min(__ldcg(&c->fcnt[par]), kBatchMaxRep);
     }
     __syncthreads();
-    const int nf = min(s_max, kBatchMaxRep);
     for (int k = threadIdx.x; k < kBatchMaxRep / 32; k += blockDim.x) bs->bits[k] = 0u;
     __syncthreads();
-    int run = 0;
-    for (int k0 = 0; k0 < nf; k0 += blockDim.x) {
-      const int k = k0 + threadIdx.x;
-      const int r = k < nf ? __ldcg(a.flist + (size_t)par * a.rctr_half + k) : 0;
-      const int nt = k < nf ? a.rep[r].ntiles : 0;
-      int tot;
-      const int ex = block_excl_scan(nt, bs->scan, &tot);
-      if (k < nf) {
-        bs->list[k] = r;
-        bs->pref[k] = run + ex;
-        atomicOr(&bs->bits[r >> 5], 1u << (r & 31));
+    {
+      const int nf = s_nf;
+      int run = 0;
+      for (int k0 = 0; k0 < nf; k0 += blockDim.x) {
+        const int k = k0 + threadIdx.x;
+        const int r = k < nf ? __ldcg(a.flist + (size_t)par * a.rctr_half + k) : 0;
+        const int nt = k < nf ? a.rep[r].ntiles : 0;
+        int tot;
+        const int ex = block_excl_scan(nt, bs->scan, &tot);
+        if (k < nf) {
+          bs->list[k] = r;
+          bs->pref[k] = run + ex;
+          atomicOr(&bs->bits[r >> 5], 1u << (r & 31));
+        }
+        run += tot;
       }
-      run += tot;
-    }
-    if (threadIdx.x == 0) {
-      bs->pref[nf] = run;
-      __threadfence();
-      if (atomicAdd(&c->readers, 1u) == gridDim.x - 1) {
-        c->readers = 0u;
-        c->fcnt[par] = 0;
-        c->ftiles[par] = 0;
+      if (threadIdx.x == 0) {
+        bs->pref[nf] = run;
+        s_t2 = run;  // tiles of the listed replicas
+        __threadfence();
+        if (atomicAdd(&c->readers, 1u) == gridDim.x - 1) {
+          c->readers = 0u;
+          c->fcnt[par] = 0;
+          c->ftiles[par] = 0;
+        }
       }
     }
     __syncthreads();
-    const int t2 = run;                       // tiles of the listed replicas
-    const unsigned items = (unsigned)(nf + a.ntiles + 2 * t2);
     // claim items until the step's are gone (each block overshoots once)
     for (;;) {
-      if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - base);
+      if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - s_base);
       __syncthreads();
       const unsigned it = (unsigned)s_item;
-      if (it >= items) break;
+      const int nf = s_nf, t2 = s_t2;
+      if (it >= (unsigned)(nf + a.ntiles + 2 * t2)) break;
       if (it < (unsigned)nf) {
-        block_sort(a, bs->list[it], epoch, bs->scan);
+        block_sort(a, bs->list[it], s_gen * kBatchEpochSteps + (unsigned)step + 1u, bs->scan);
       } else if (it < (unsigned)(nf + a.ntiles)) {
         const int tile = (int)it - nf;
         const int r = a.tile_rep[tile];
@@ -2872,7 +2879,7 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
         const int tile = a.rep[r].tile0 + (k - bs->pref[lo]);
         RepState* S = a.st + r;
         if (threadIdx.x == 0) {
-          s_ok = build ? wait_eq_u32(&S->sort_done, epoch)
+          s_ok = build ? wait_eq_u32(&S->sort_done, s_gen * kBatchEpochSteps + (unsigned)step + 1u)
                        : wait_eq_u32(reinterpret_cast<const unsigned*>(&S->rebuild), 0u);
           if (!s_ok) {
             // recorded for the host and tallied with the barrier arrival, so
@@ -2895,13 +2902,13 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       }
       __syncthreads();
     }
-    base += items + gridDim.x;
-    budget -= 1;
     // step barrier: arrival + "steps left" and overflow tallies
     if (threadIdx.x == 0) {
+      s_base += (unsigned)(s_nf + a.ntiles + 2 * s_t2) + gridDim.x;
+      const int budget = --s_budget;
       const unsigned long long mine = 1ull + s_step_tally;
       const unsigned long long now = atom_add_acq_rel_u64(&c->word[par], mine) + mine;
-      const unsigned long long base_w = seen[par];
+      const unsigned long long base_w = s_seen[par];
       const bool last = ((now - base_w) & kTallyArriveMask) == gridDim.x;
       unsigned long long tot = now;
       int ok = 1;
@@ -2918,7 +2925,7 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
           __nanosleep(32);
         }
       }
-      seen[par] = tot;
+      s_seen[par] = tot;
       const unsigned long long d = tot - base_w;
       const unsigned more = (unsigned)((d >> kTallyMoreShift) & kTallyField);
       // list overflows and waits that gave up: the host repairs or reports
