@@ -2646,13 +2646,31 @@ __device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoc
     int* cst = a.cstart + R.cell0;
     for (int c = tid; c < ncell; c += bd) cnt[c] = 0;
     __syncthreads();
-    // cell key (calculateCellIndices, NeighborList.cu:1142-1172) and arrival rank
-    for (int i = tid; i < n; i += bd) {
-      const float4 r = a.r[rb][p0 + i];
-      const int key = cell_coord(r.x, R.invL[0], R.nc[0]) + cell_coord(r.y, R.invL[1], R.nc[1]) * R.nc[0] +
-                      cell_coord(r.z, R.invL[2], R.nc[2]) * R.nc[0] * R.nc[1];
-      a.key[p0 + i] = key;
-      a.slot[p0 + i] = atomicAdd(&cnt[key], 1);
+    // cell key (calculateCellIndices, NeighborList.cu:1142-1172) and arrival
+    // rank; a thread keeps kSortIlp particles' loads and atomics in flight
+    constexpr int kSortIlp = 8;
+    for (int i0 = tid; i0 < n; i0 += bd * kSortIlp) {
+      float4 r[kSortIlp];
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        const int i = i0 + u * bd;
+        r[u] = i < n ? a.r[rb][p0 + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      int key[kSortIlp], sl[kSortIlp];
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        key[u] = cell_coord(r[u].x, R.invL[0], R.nc[0]) + cell_coord(r[u].y, R.invL[1], R.nc[1]) * R.nc[0] +
+                 cell_coord(r[u].z, R.invL[2], R.nc[2]) * R.nc[0] * R.nc[1];
+        sl[u] = i0 + u * bd < n ? atomicAdd(&cnt[key[u]], 1) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        const int i = i0 + u * bd;
+        if (i < n) {
+          a.key[p0 + i] = key[u];
+          a.slot[p0 + i] = sl[u];
+        }
+      }
     }
     __syncthreads();
     // absolute first slot of every cell
@@ -2666,7 +2684,22 @@ __device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoc
       carry += tot;
     }
     __syncthreads();
-    for (int i = tid; i < n; i += bd) a.order[p0 + cst[a.key[p0 + i]] + a.slot[p0 + i]] = (unsigned)i;
+    for (int i0 = tid; i0 < n; i0 += bd * kSortIlp) {
+      int key[kSortIlp], sl[kSortIlp];
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        const int i = i0 + u * bd;
+        key[u] = i < n ? a.key[p0 + i] : 0;
+        sl[u] = i < n ? a.slot[p0 + i] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) key[u] = cst[key[u]];
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        const int i = i0 + u * bd;
+        if (i < n) a.order[p0 + key[u] + sl[u]] = (unsigned)i;
+      }
+    }
     __syncthreads();
     // each bucket by current slot: the result is the stable sort by key
     for (int c = tid; c < ncell; c += bd) {
@@ -2684,12 +2717,24 @@ __device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoc
     }
     __syncthreads();
     // ParticleData::UpdateAfterSorting (ParticleData.cu:493-528)
-    for (int sl = tid; sl < n; sl += bd) {
-      const size_t gs = p0 + sl, go = p0 + a.order[p0 + sl];
-      a.r[rb ^ 1][gs] = a.r[rb][go];
-      a.v[ab ^ 1][gs] = a.v[ab][go];
-      a.im[ab ^ 1][gs] = a.im[ab][go];
-      a.uidx[ab ^ 1][gs] = a.uidx[ab][go];
+    for (int s0 = tid; s0 < n; s0 += bd * kSortIlp) {
+      unsigned o[kSortIlp];
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        const int sl = s0 + u * bd;
+        o[u] = sl < n ? a.order[p0 + sl] : 0u;
+      }
+#pragma unroll
+      for (int u = 0; u < kSortIlp; ++u) {
+        const int sl = s0 + u * bd;
+        if (sl < n) {
+          const size_t gs = p0 + sl, go = p0 + o[u];
+          a.r[rb ^ 1][gs] = a.r[rb][go];
+          a.v[ab ^ 1][gs] = a.v[ab][go];
+          a.im[ab ^ 1][gs] = a.im[ab][go];
+          a.uidx[ab ^ 1][gs] = a.uidx[ab][go];
+        }
+      }
     }
     __syncthreads();
     if (tid == 0) {
@@ -2715,6 +2760,10 @@ __device__ __forceinline__ bool wait_eq_u32(const unsigned* p, unsigned want) {
 }
 
 constexpr int kBatchMaxRep = 1024;   // replicas whose rebuild list a block holds in shared memory
+// Tiles of the other replicas claimed between the sorts and the builds: a
+// third of the tiles, but no more than the tiles left once the listed
+// replicas' are taken out.
+__device__ __forceinline__ int batch_first_tiles(int ntiles, int t2) { return min(ntiles / 3, max(0, ntiles - t2)); }
 constexpr int kBatchMaxN = 65536;    // particles per replica (one block sorts a replica)
 constexpr int kBatchEpochSteps = 4096;  // epochs: launch generation * this + step + 1
 
@@ -2851,24 +2900,30 @@ __global__ void __maxnreg__(72) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       }
     }
     __syncthreads();
-    // claim items until the step's are gone (each block overshoots once)
+    // claim items until the step's are gone (each block overshoots once).
+    // Ticket order: [sorts] [the first q tiles, other replicas] [builds]
+    // [the remaining tiles] [the listed replicas' force tiles]: the first
+    // tiles give the sorts time, the remaining ones the builds.
     for (;;) {
       if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - s_base);
       __syncthreads();
       const unsigned it = (unsigned)s_item;
       const int nf = s_nf, t2 = s_t2;
+      const int q = batch_first_tiles(a.ntiles, t2);
       if (it >= (unsigned)(nf + a.ntiles + 2 * t2)) break;
+      const bool tile_item = it >= (unsigned)nf && (it < (unsigned)(nf + q) || (it >= (unsigned)(nf + q + t2) &&
+                                                                             it < (unsigned)(nf + a.ntiles + t2)));
       if (it < (unsigned)nf) {
         block_sort(a, bs->list[it], s_gen * kBatchEpochSteps + (unsigned)step + 1u, bs->scan);
-      } else if (it < (unsigned)(nf + a.ntiles)) {
-        const int tile = (int)it - nf;
+      } else if (tile_item) {
+        const int tile = it < (unsigned)(nf + q) ? (int)it - nf : (int)it - nf - t2;
         const int r = a.tile_rep[tile];
         if (!((bs->bits[r >> 5] >> (r & 31)) & 1u))
           force_tile<TP, true, false, FM_STREAMED, false, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, nullptr,
                                                                 0, nullptr, nullptr, nullptr, par ^ 1);
       } else {
-        const bool build = it < (unsigned)(nf + a.ntiles + t2);
-        const int k = (int)it - nf - a.ntiles - (build ? 0 : t2);
+        const bool build = it < (unsigned)(nf + q + t2);
+        const int k = build ? (int)it - nf - q : (int)it - nf - a.ntiles - t2;
         int lo = 0, hi = nf - 1;  // the listed replica holding flagged tile k
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
