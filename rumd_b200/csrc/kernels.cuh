@@ -261,8 +261,6 @@ __device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float
 // k_steps: what this block adds to its step-barrier arrival (its replica
 // still has steps, its tile asks for a rebuild); thread 0 only.
 __shared__ unsigned long long s_step_tally;
-// k_batch: a replica this block finalized and must sort for the next step (-1: none)
-__shared__ int s_sort_rep;
 constexpr int kTallyMoreShift = 24, kTallyRebuildShift = 44;
 constexpr unsigned long long kTallyArriveMask = (1ull << kTallyMoreShift) - 1ull;
 constexpr unsigned long long kTallyField = (1ull << 20) - 1ull;
@@ -311,7 +309,6 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
       const int pos = atomicAdd(&c->fcnt[bpar], 1);
       a.flist[(size_t)bpar * a.rctr_half + pos] = rep;
       atomicAdd(&c->ftiles[bpar], R.ntiles);
-      s_sort_rep = rep;  // k_batch sorts it right away, in this block
     }
   }
   // energies at run steps i with i % interval == 0, as Simulation.Run's
@@ -2704,18 +2701,51 @@ __device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoc
       }
     }
     __syncthreads();
-    // each bucket by current slot: the result is the stable sort by key
-    for (int c = tid; c < ncell; c += bd) {
-      unsigned* o = a.order + p0 + cst[c];
-      const int m = cnt[c];
-      for (int q = 1; q < m; ++q) {
-        const unsigned x = o[q];
-        int k = q - 1;
-        while (k >= 0 && o[k] > x) {
-          o[k + 1] = o[k];
-          --k;
+    // each bucket by current slot: the result is the stable sort by key.  A
+    // thread takes two cells at a time; buckets of up to kFixRegs slots are
+    // loaded together into registers, sorted by an odd-even transposition
+    // network and stored back (larger ones: insertion sort in place)
+    for (int c0 = tid; c0 < ncell; c0 += 2 * bd) {
+      int m[2], b[2];
+      unsigned x[2][kFixRegs];
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        const int c = c0 + u * bd;
+        m[u] = c < ncell ? cnt[c] : 0;
+        b[u] = c < ncell ? cst[c] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < 2; ++u)
+#pragma unroll
+        for (int k = 0; k < kFixRegs; ++k)
+          x[u][k] = (k < m[u] && m[u] <= kFixRegs) ? a.order[p0 + b[u] + k] : 0xffffffffu;
+#pragma unroll
+      for (int u = 0; u < 2; ++u) {
+        if (m[u] <= 1) continue;
+        if (m[u] <= kFixRegs) {
+#pragma unroll
+          for (int r = 0; r < kFixRegs; ++r)
+#pragma unroll
+            for (int k = r & 1; k + 1 < kFixRegs; k += 2) {
+              const unsigned lo = min(x[u][k], x[u][k + 1]), hi = max(x[u][k], x[u][k + 1]);
+              x[u][k] = lo;
+              x[u][k + 1] = hi;
+            }
+#pragma unroll
+          for (int k = 0; k < kFixRegs; ++k)
+            if (k < m[u]) a.order[p0 + b[u] + k] = x[u][k];
+        } else {
+          unsigned* o = a.order + p0 + b[u];
+          for (int q = 1; q < m[u]; ++q) {
+            const unsigned v = o[q];
+            int k = q - 1;
+            while (k >= 0 && o[k] > v) {
+              o[k + 1] = o[k];
+              --k;
+            }
+            o[k + 1] = v;
+          }
         }
-        o[k + 1] = x;
       }
     }
     __syncthreads();
@@ -2782,10 +2812,8 @@ struct BatchShared {
 
 // Every MD step of many replicas in one cooperative launch.  Per step the
 // blocks claim work items in ticket order (one atomic counter):
-//   1. in a launch's first step, the stable sort of each replica on the
-//      step's rebuild list (one block sorts one replica, block_sort); later
-//      the block that finalizes a replica whose list is due sorts it right
-//      after the step that asked for it;
+//   1. the stable sort of each replica on the step's rebuild list (one block
+//      sorts one replica, block_sort);
 //   2. the fused force + Nose-Hoover tile of every tile of the other
 //      replicas (force_tile, as k_force);
 //   3. the list build of every tile of the listed replicas (build_runs_tile),
@@ -2863,7 +2891,6 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       s_budget = __ldcg(&c->budget);
       s_base = 0u;
       s_seen[0] = s_seen[1] = 0ull;
-      s_sort_rep = -1;
     }
     __syncthreads();
   }
@@ -2908,17 +2935,14 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     __syncthreads();
     // claim items until the step's are gone (each block overshoots once).
     // Ticket order: [sorts] [the first q tiles, other replicas] [builds]
-    // [the remaining tiles] [the listed replicas' force tiles].  Sorts are
-    // items only in a launch's first step (q tiles then give them time);
-    // later, the finalizer that puts a replica on the next step's list sorts
-    // it at once (below), so the builds come first (q = 0).
+    // [the remaining tiles] [the listed replicas' force tiles]: the first
+    // tiles give the sorts time, the remaining ones the builds.
     for (;;) {
       if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - s_base);
       __syncthreads();
       const unsigned it = (unsigned)s_item;
-      const int t2 = s_t2;
-      const int nf = step == 0 ? s_nf : 0;  // sort items
-      const int q = step == 0 ? batch_first_tiles(a.ntiles, t2) : 0;
+      const int t2 = s_t2, nf = s_nf;
+      const int q = batch_first_tiles(a.ntiles, t2);
       if (it >= (unsigned)(nf + a.ntiles + 2 * t2)) break;
       const bool tile_item = it >= (unsigned)nf && (it < (unsigned)(nf + q) || (it >= (unsigned)(nf + q + t2) &&
                                                                              it < (unsigned)(nf + a.ntiles + t2)));
@@ -2933,7 +2957,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       } else {
         const bool build = it < (unsigned)(nf + q + t2);
         const int k = build ? (int)it - nf - q : (int)it - nf - a.ntiles - t2;
-        int lo = 0, hi = s_nf - 1;  // the listed replica holding flagged tile k
+        int lo = 0, hi = nf - 1;  // the listed replica holding flagged tile k
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
           if (bs->pref[mid] <= k) lo = mid;
@@ -2965,17 +2989,10 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
         }
       }
       __syncthreads();
-      // a replica this block finalized whose list is due: sort it now, for
-      // the next step (no tile of it runs again in this step)
-      if (s_sort_rep >= 0) {
-        block_sort(a, s_sort_rep, s_gen * kBatchEpochSteps + (unsigned)step + 2u, bs->scan);
-        if (threadIdx.x == 0) s_sort_rep = -1;
-        __syncthreads();
-      }
     }
     // step barrier: arrival + "steps left" and overflow tallies
     if (threadIdx.x == 0) {
-      s_base += (unsigned)((step == 0 ? s_nf : 0) + a.ntiles + 2 * s_t2) + gridDim.x;
+      s_base += (unsigned)(s_nf + a.ntiles + 2 * s_t2) + gridDim.x;
       const int budget = --s_budget;
       const unsigned long long mine = 1ull + s_step_tally;
       const unsigned long long now = atom_add_acq_rel_u64(&c->word[par], mine) + mine;
