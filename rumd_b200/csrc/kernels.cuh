@@ -2673,15 +2673,34 @@ __device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoc
       }
     }
     __syncthreads();
-    // absolute first slot of every cell
-    int carry = 0;
-    for (int base = 0; base < ncell; base += bd) {
-      const int c = base + tid;
-      const int x = c < ncell ? cnt[c] : 0;
-      int tot;
-      const int ex = block_excl_scan(x, s_w, &tot);
-      if (c < ncell) cst[c] = carry + ex;
-      carry += tot;
+    // absolute first slot of every cell: thread t owns the cells
+    // [t K, (t + 1) K), loads their counts together, and one block scan of
+    // the threads' totals gives every run's first slot
+    const int K = (ncell + bd - 1) / bd;
+    {
+      constexpr int kCh = 8;
+      const int c0 = tid * K, c1 = min(ncell, c0 + K);
+      int tot = 0;
+      for (int cb = c0; cb < c1; cb += kCh) {
+        int x[kCh];
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) x[u] = cb + u < c1 ? cnt[cb + u] : 0;
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) tot += x[u];
+      }
+      int all;
+      int run = block_excl_scan(tot, s_w, &all);
+      for (int cb = c0; cb < c1; cb += kCh) {
+        int x[kCh];
+#pragma unroll
+        for (int u = 0; u < kCh; ++u) x[u] = cb + u < c1 ? cnt[cb + u] : 0;
+#pragma unroll
+        for (int u = 0; u < kCh; ++u)
+          if (cb + u < c1) {
+            cst[cb + u] = run;
+            run += x[u];
+          }
+      }
     }
     __syncthreads();
     for (int i0 = tid; i0 < n; i0 += bd * kSortIlp) {
@@ -2702,48 +2721,53 @@ __device__ __noinline__ void block_sort(const EngArgs& a, int rep, unsigned epoc
     }
     __syncthreads();
     // each bucket by current slot: the result is the stable sort by key.  A
-    // thread takes two cells at a time; buckets of up to kFixRegs slots are
-    // loaded together into registers, sorted by an odd-even transposition
-    // network and stored back (larger ones: insertion sort in place)
-    for (int c0 = tid; c0 < ncell; c0 += 2 * bd) {
-      int m[2], b[2];
-      unsigned x[2][kFixRegs];
+    // thread takes its run of cells kFixCells at a time; buckets of up to
+    // kFixRegs slots are loaded together into registers, sorted by an
+    // odd-even transposition network and stored back (larger ones:
+    // insertion sort in place)
+    {
+      constexpr int kFixCells = 2;
+      const int c0 = tid * K, c1 = min(ncell, c0 + K);
+      for (int cb = c0; cb < c1; cb += kFixCells) {
+        int m[kFixCells], b[kFixCells];
+        unsigned x[kFixCells][kFixRegs];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        const int c = c0 + u * bd;
-        m[u] = c < ncell ? cnt[c] : 0;
-        b[u] = c < ncell ? cst[c] : 0;
-      }
+        for (int u = 0; u < kFixCells; ++u) {
+          const int c = cb + u;
+          m[u] = c < c1 ? cnt[c] : 0;
+          b[u] = c < c1 ? cst[c] : 0;
+        }
 #pragma unroll
-      for (int u = 0; u < 2; ++u)
-#pragma unroll
-        for (int k = 0; k < kFixRegs; ++k)
-          x[u][k] = (k < m[u] && m[u] <= kFixRegs) ? a.order[p0 + b[u] + k] : 0xffffffffu;
-#pragma unroll
-      for (int u = 0; u < 2; ++u) {
-        if (m[u] <= 1) continue;
-        if (m[u] <= kFixRegs) {
-#pragma unroll
-          for (int r = 0; r < kFixRegs; ++r)
-#pragma unroll
-            for (int k = r & 1; k + 1 < kFixRegs; k += 2) {
-              const unsigned lo = min(x[u][k], x[u][k + 1]), hi = max(x[u][k], x[u][k + 1]);
-              x[u][k] = lo;
-              x[u][k + 1] = hi;
-            }
+        for (int u = 0; u < kFixCells; ++u)
 #pragma unroll
           for (int k = 0; k < kFixRegs; ++k)
-            if (k < m[u]) a.order[p0 + b[u] + k] = x[u][k];
-        } else {
-          unsigned* o = a.order + p0 + b[u];
-          for (int q = 1; q < m[u]; ++q) {
-            const unsigned v = o[q];
-            int k = q - 1;
-            while (k >= 0 && o[k] > v) {
-              o[k + 1] = o[k];
-              --k;
+            x[u][k] = (k < m[u] && m[u] <= kFixRegs && m[u] > 1) ? a.order[p0 + b[u] + k] : 0xffffffffu;
+#pragma unroll
+        for (int u = 0; u < kFixCells; ++u) {
+          if (m[u] <= 1) continue;
+          if (m[u] <= kFixRegs) {
+#pragma unroll
+            for (int r = 0; r < kFixRegs; ++r)
+#pragma unroll
+              for (int k = r & 1; k + 1 < kFixRegs; k += 2) {
+                const unsigned lo = min(x[u][k], x[u][k + 1]), hi = max(x[u][k], x[u][k + 1]);
+                x[u][k] = lo;
+                x[u][k + 1] = hi;
+              }
+#pragma unroll
+            for (int k = 0; k < kFixRegs; ++k)
+              if (k < m[u]) a.order[p0 + b[u] + k] = x[u][k];
+          } else {
+            unsigned* o = a.order + p0 + b[u];
+            for (int q = 1; q < m[u]; ++q) {
+              const unsigned v = o[q];
+              int k = q - 1;
+              while (k >= 0 && o[k] > v) {
+                o[k + 1] = o[k];
+                --k;
+              }
+              o[k + 1] = v;
             }
-            o[k + 1] = v;
           }
         }
       }
@@ -2793,10 +2817,13 @@ __device__ __forceinline__ bool wait_eq_u32(const unsigned* p, unsigned want) {
 }
 
 constexpr int kBatchMaxRep = 1024;   // replicas whose rebuild list a block holds in shared memory
-// Tiles of the other replicas claimed between the sorts and the builds: a
-// third of the tiles, but no more than the tiles left once the listed
-// replicas' are taken out.
-__device__ __forceinline__ int batch_first_tiles(int ntiles, int t2) { return min(ntiles / 3, max(0, ntiles - t2)); }
+// Tiles of the other replicas claimed between the sorts and the builds: two
+// thirds of the tiles (on the 256-replica batch: 566, 548, 535 us per step
+// for a third, a half, two thirds), but no more than the tiles left once the
+// listed replicas' are taken out.
+__device__ __forceinline__ int batch_first_tiles(int ntiles, int t2) {
+  return min(2 * ntiles / 3, max(0, ntiles - t2));
+}
 constexpr int kBatchMaxN = 65536;    // particles per replica (one block sorts a replica)
 constexpr int kBatchEpochSteps = 4096;  // epochs: launch generation * this + step + 1
 
