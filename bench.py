@@ -355,20 +355,33 @@ def batch_workload(seed=0):
     """The batching configuration: 256 KA replicas, N = floor(exp(U(ln 512,
     ln 8192))) (seeded), T log-spaced from 0.45 to 2.0."""
     from rumd_b200 import initconf as I
-    rng = np.random.default_rng(seed)
-    R = 256
-    ns = np.floor(np.exp(rng.uniform(np.log(512), np.log(8192), R))).astype(int)
-    Ts = np.exp(np.linspace(np.log(0.45), np.log(2.0), R))
-    confs = [I.ka_config(int(n), T=float(T), seed=seed + k) for k, (n, T) in enumerate(zip(ns, Ts))]
-    return ns, Ts, confs
+    return I.ka_batch_workload(seed)
 
 
-def batch_engine(capi, device, pb, tp, ns, Ts, confs):
+def batch_tuning():
+    """The autotuner's pick for the 256-replica batch from the library's
+    autotune cache (rumd_b200/autotune_cache.json, profiles/autotune_batch256.md),
+    or the plain defaults when the cache has no entry for it."""
+    from rumd_b200 import autotune
+    path = os.path.join(ROOT, "rumd_b200", "autotune_cache.json")
+    key = autotune.signature(autotune.batch_replicas())
+    cache = {}
+    if os.path.exists(path):
+        with open(path) as fh:
+            cache = json.load(fh)
+    if key in cache:
+        e = cache[key]
+        return {"pb": e["pb"], "tp": e["tp"], "skin": e["skin"], "persistent": e.get("persistent", 1),
+                "source": "autotuner (rumd_b200/autotune_cache.json)"}
+    return {"pb": 64, "tp": 2, "skin": SKIN, "persistent": 1, "source": "defaults (no autotune entry)"}
+
+
+def batch_engine(capi, device, pb, tp, ns, Ts, confs, skin=SKIN):
     R = len(ns)
     params = ka_params()
     e = new_engine(capi, device=device, max_particles=int(ns.sum() + 64 * R), max_replicas=R, pb=pb, tp=tp)
     for c, T in zip(confs, Ts):
-        e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=SKIN, dt=DT, T=float(T), tau=TAU, vel4=c["vel4"])
+        e.add(c["pos4"], c["box"], params, 2, cutoff="SF", skin=skin, dt=DT, T=float(T), tau=TAU, vel4=c["vel4"])
     return e
 
 
@@ -376,7 +389,9 @@ def profile_batched(capi, device, args):
     """The batch with eager launches (b2md_run_timed) for ncu's launch list."""
     import torch
     ns, Ts, confs = batch_workload()
-    e = batch_engine(capi, device, args.pb, args.tp, ns, Ts, confs)
+    tune = batch_tuning()
+    e = batch_engine(capi, device, tune["pb"], tune["tp"], ns, Ts, confs, skin=tune["skin"])
+    e.set_variant(capi.VARIANT_PERSISTENT, tune["persistent"])
     e.run(300)
     torch.cuda.synchronize(device)
     torch.cuda.profiler.start()
@@ -390,11 +405,14 @@ def profile_batched(capi, device, args):
 
 def batched(capi, device, pb, tp, steps, seed=0):
     """256 KA replicas, N log-uniform in [512, 8192], T log-spaced 0.45..2.0,
-    advanced together; against sequential plain runs of every 16th replica."""
+    advanced together with the autotuner's launch shape and skin; against
+    sequential plain runs of every 16th replica (the plain defaults)."""
     R = 256
     ns, Ts, confs = batch_workload(seed)
     params = ka_params()
-    e = batch_engine(capi, device, pb, tp, ns, Ts, confs)
+    tune = batch_tuning()
+    e = batch_engine(capi, device, tune["pb"], tune["tp"], ns, Ts, confs, skin=tune["skin"])
+    e.set_variant(capi.VARIANT_PERSISTENT, tune["persistent"])
     e.run(500)
     t_b = time_run(capi, e, steps, device)
     rate_b = float(ns.sum()) * steps / t_b
@@ -412,7 +430,7 @@ def batched(capi, device, pb, tp, steps, seed=0):
         s.close()
     rate_s = ps_seq / t_seq
     return {"value": rate_b, "unit": "particle-steps/s", "replicas": R, "particles": int(ns.sum()),
-            "steps": steps, "ms_per_step": t_b / steps * 1e3,
+            "steps": steps, "ms_per_step": t_b / steps * 1e3, "tuning": tune,
             "persistent_kernel": {0: "none (one launch per step)", 1: "k_steps", 2: "k_batch"}.get(kind, kind),
             "sequential_plain_value": rate_s,
             "sequential_sample": f"{len(sample)} of the {R} replicas run alone, one after another",

@@ -118,7 +118,7 @@ class Autotune:
         best, table = search(candidates(**self.grid), measure)
         entry = {"pb": best["pb"], "tp": best["tp"], "skin": best["skin"], "rate": best["rate"], "table": table}
         if variants:
-            vbest, vtable = search_variants(entry, measure)
+            vbest, vtable = search_variants(entry, measure, variants=VARIANTS)
             entry.update({k: vbest[k] for k in VARIANT_KEYS if k in vbest})
             entry.update(rate=max(entry["rate"], vbest["rate"]), variant_table=vtable)
         cache[key] = entry
@@ -180,13 +180,29 @@ def device_measure(capi, replicas, device=0, steps=300, warmup=100):
     return measure
 
 
+def batch_replicas(seed=0):
+    """The 256-replica Kob-Andersen batch (initconf.ka_batch_workload) as
+    autotuner replicas: FCC starts, each at its own temperature."""
+    from . import initconf
+    ns, Ts, confs = initconf.ka_batch_workload(seed)
+    params = initconf.lj_params(2, initconf.KA)
+    return [dict(pos4=c["pos4"], vel4=c["vel4"], box=c["box"], params=params, ntypes=2, T=float(T), n=int(n),
+                 density=1.2) for n, T, c in zip(ns, Ts, confs)]
+
+
+# kernel variants worth trying on a large batch (persistent kernel, list build)
+BATCH_VARIANTS = tuple(dict(force_mode=0, sm_tiles=0, persistent=ps, build_lanes=bl) for ps in (1, 0) for bl in (0, 32))
+
+
 def main(argv=None):
-    """python -m rumd_b200.autotune --n 65536 --T 0.45 [--pbs 32,64 --tps 2,4 --skins 0.3]"""
+    """python -m rumd_b200.autotune --n 65536 --T 0.45 [--pbs 32,64 --tps 2,4 --skins 0.3]
+    python -m rumd_b200.autotune --batch256 --skins 0.3,0.4,0.5   (the 256-replica batch)"""
     import argparse
     from . import capi
     p = argparse.ArgumentParser()
     p.add_argument("--n", type=int, default=65536)
     p.add_argument("--T", type=float, default=0.45)
+    p.add_argument("--batch256", action="store_true", help="tune on the 256-replica Kob-Andersen batch")
     p.add_argument("--pbs", default="32,64,128")
     p.add_argument("--tps", default="1,2,4,8")
     p.add_argument("--skins", default="0.3")
@@ -194,10 +210,13 @@ def main(argv=None):
     p.add_argument("--cache", default="autotune.json")
     p.add_argument("--no-variants", action="store_true", help="skip the kernel-variant stage")
     args = p.parse_args(argv)
-    reps = [equilibrated_ka(capi, args.n, args.T)]
+    reps = batch_replicas() if args.batch256 else [equilibrated_ka(capi, args.n, args.T)]
     at = Autotune(cache_path=args.cache, pbs=tuple(int(x) for x in args.pbs.split(",")),
                   tps=tuple(int(x) for x in args.tps.split(",")),
                   skins=tuple(float(x) for x in args.skins.split(",")))
+    if args.batch256:
+        global VARIANTS
+        VARIANTS = BATCH_VARIANTS
     best = at.tune(reps, device_measure(capi, reps, steps=args.steps, warmup=200), force=True,
                    variants=not args.no_variants)
     for r in best["table"]:

@@ -176,3 +176,14 @@ def ka_config(n, density=1.2, T=0.73, seed=0):
 
 def lj_config(n, density=0.8442, T=0.722, seed=0):
     return make_config(n, density, T, seed=seed)
+
+
+def ka_batch_workload(seed=0, replicas=256, n_min=512, n_max=8192, T_min=0.45, T_max=2.0):
+    """The batching configuration: Kob-Andersen replicas at density 1.2 with
+    N = floor(exp(U(ln n_min, ln n_max))) (seeded PCG64) and temperatures
+    log-spaced from T_min to T_max.  Returns (sizes, temperatures, configs)."""
+    rng = np.random.default_rng(seed)
+    ns = np.floor(np.exp(rng.uniform(np.log(n_min), np.log(n_max), replicas))).astype(int)
+    Ts = np.exp(np.linspace(np.log(T_min), np.log(T_max), replicas))
+    confs = [ka_config(int(n), T=float(T), seed=seed + k) for k, (n, T) in enumerate(zip(ns, Ts))]
+    return ns, Ts, confs
