@@ -129,6 +129,12 @@ B2MD_API int b2md_engine_set_launch(b2md_engine* e, int pb, int tp);
 B2MD_API int b2md_engine_get_launch(b2md_engine* e, int* pb, int* tp);
 /* Device bytes currently allocated by the engine. */
 B2MD_API int b2md_engine_memory(b2md_engine* e, long long* bytes);
+/* Device bytes held by the active replicas in the engine's pools (used) and
+ * allocated by the engine in all (reserved, as b2md_engine_memory).  With
+ * b2md_replica_footprint this is the admission budget of a server: RUMD has
+ * one system per process and sizes its buffers per Sample
+ * (Sample.cu:208-249, NeighborList.cu:275-295). */
+B2MD_API int b2md_engine_usage(b2md_engine* e, long long* used, long long* reserved);
 /* Chooses CUDA-graph conditional rebuild nodes (1, default) or unconditional
  * early-exit rebuild kernels (0) for b2md_run. */
 B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
@@ -170,12 +176,22 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *                              neighbours share its L1; 0 = one block per tile.
  *   B2MD_VARIANT_PERSISTENT    1 (default): b2md_run drives streamed-mode
  *                              engines whose tiles all fit on the GPU at once
- *                              with one cooperative kernel that runs steps
- *                              back to back, with a grid barrier between
- *                              them, until a list rebuild is due; 0: one
- *                              kernel launch per step.
- *   B2MD_VARIANT_PERSISTENT_ACTIVE  read-only: 1 when the last run used the
- *                              persistent kernel.
+ *                              with one cooperative kernel (k_steps) that
+ *                              runs steps back to back, with a grid barrier
+ *                              between them, until a list rebuild is due;
+ *                              engines with more tiles than resident blocks
+ *                              (batches) with the batched kernel (k_batch),
+ *                              which runs whole steps, list rebuilds
+ *                              included, with one grid barrier each;
+ *                              2: k_batch whenever it applies (at most 1024
+ *                              replicas of at most 65536 particles);
+ *                              0: one kernel launch per step.
+ *   B2MD_VARIANT_PERSISTENT_ACTIVE  read-only: the persistent kernel of the
+ *                              current step graph (1 k_steps, 2 k_batch,
+ *                              0 none).
+ *   B2MD_VARIANT_GRAPH_BUILDS  read-only: step graphs instantiated so far
+ *                              (admissions and removals do not rebuild a
+ *                              k_batch graph).
  * No reference counterpart beyond Sample::SetPB_TP (Sample.h:96). */
 enum {
   B2MD_VARIANT_FORCE_MODE = 0,
@@ -185,16 +201,29 @@ enum {
   B2MD_VARIANT_SM_TILES = 4,
   B2MD_VARIANT_WINDOW_LIST_ROWS = 5,
   B2MD_VARIANT_PERSISTENT = 6,
-  B2MD_VARIANT_PERSISTENT_ACTIVE = 7
+  B2MD_VARIANT_PERSISTENT_ACTIVE = 7,
+  B2MD_VARIANT_GRAPH_BUILDS = 8
 };
 B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
 B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);
 
 /* Admission of one system (Sample::ReadConf + SetPotential + SetIntegrator,
- * Simulation.py:29-31,157-214).  vel4/im3 may be NULL (zero). */
+ * Simulation.py:29-31,157-214).  vel4/im3 may be NULL (zero).
+ * Admission does not wait for running work: the particle data is copied into
+ * the engine's pinned staging and uploaded in stream order after what is
+ * already queued (a running b2md_run_queued_async chunk), and the tile
+ * layout is applied before the next launch.  When pos4 and vel4 are both in
+ * page-locked memory (cudaMallocHost / cudaHostRegister) they are copied from
+ * directly and the call returns once those copies are done. */
 B2MD_API int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* pos4,
                      const float* vel4, const int* im3, int* id_out);
+/* Removal (a finished job leaving).  Returns at once: its memory goes back to
+ * the pools for later admissions, whose uploads are queued behind any work
+ * still using it. */
 B2MD_API int b2md_replica_remove(b2md_engine* e, int id);
+/* Device bytes that b2md_replica_add(d) would hold in the pools (its share
+ * of b2md_engine_usage's used bytes), without admitting anything. */
+B2MD_API int b2md_replica_footprint(b2md_engine* e, const b2md_replica_desc* d, long long* bytes);
 /* Copies a field out in original order (ParticleData::Copy*FromDevice,
  * ParticleData.cu:383-470).  out: n*4 floats, or n*3 ints for images. */
 B2MD_API int b2md_replica_get(b2md_engine* e, int id, int field, void* out);
@@ -209,9 +238,21 @@ B2MD_API int b2md_replica_read(b2md_engine* e, int id, float* pos4, float* vel4,
 B2MD_API int b2md_replica_set(b2md_engine* e, int id, int field, const void* in);
 /* Pair parameter table / cut-off method / skin / pair function
  * (PairPotential::SetParams + CopyParamsToGPU, PairPotential.cu:82-125;
- * SetNbListSkin; Sample::SetPotential with another Pot_* class). */
+ * SetNbListSkin; Sample::SetPotential with another Pot_* class).  The
+ * replica's potential list becomes this one potential (Sample.cu:251-259). */
 B2MD_API int b2md_replica_set_potential(b2md_engine* e, int id, int ntypes, const float* params,
                                int cutoff_method, float skin, int potential);
+/* Sample::AddPotential (Sample.cu:261-278): a second pair potential (same
+ * number of types; its own parameter table, cut-off method and pair
+ * function).  Sample::CalcF evaluates both (Sample.cu:335-336): the forces,
+ * energies, virials and stresses of the second are added to the first's
+ * once both per-particle sums are complete (PairPotential.cu:370-388).  One
+ * neighbour list serves both, built with the larger cut-off per type pair
+ * and the first potential's skin.  At most two potentials per replica; an
+ * engine holding such a replica runs its steps with the per-step graphs
+ * (the persistent kernels evaluate one potential). */
+B2MD_API int b2md_replica_add_potential(b2md_engine* e, int id, int ntypes, const float* params,
+                                        int cutoff_method, int potential);
 /* Integrator settings (IntegratorNVT::SetTimeStep, SetTargetTemperature,
  * SetRelaxationTime, SetThermostatState, SetThermostatOn*,
  * SetTemperatureChangePerTimeStep; IntegratorNVT.cu:132-190). */
@@ -262,9 +303,40 @@ B2MD_API int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kerne
                             long long* launches);
 /* Batched/served form: each replica advances its own queued step count
  * (b2md_replica_queue_steps) in the same launches; returns when all queues
- * are empty or after max_steps launches-worth of steps (0 = until empty). */
+ * are empty or after max_steps launches-worth of steps (0 = until empty).
+ * Queueing steps is itself asynchronous (in stream order). */
 B2MD_API int b2md_replica_queue_steps(b2md_engine* e, int id, long long nsteps);
 B2MD_API int b2md_run_queued(b2md_engine* e, long long max_steps, long long* steps_run);
+
+/* The served form's chunks, for a host that admits and retires jobs while the
+ * GPU runs.  b2md_run_queued_async applies pending admissions/removals,
+ * launches up to max_steps steps of the queued work (0 = until empty) and
+ * returns at once with a ticket; a snapshot of every replica's state at the
+ * end of the chunk is copied to pinned host memory behind it.  At most two
+ * chunks are in flight: a third call first waits for the oldest.  A batched
+ * persistent graph (k_batch) is not rebuilt by admissions or removals.
+ * b2md_run_queued_poll sets *done without blocking.  b2md_run_queued_wait
+ * waits for the chunk (one of the two most recent), reports a device wait
+ * that gave up, enlarges overflowed lists (their replicas continue in the
+ * next chunk), and returns the steps the chunk ran and, for replica ids
+ * 0..cap-1, B2MD_CHUNK_FIELDS doubles each from the snapshot (replicas not
+ * active when the chunk was launched have ACTIVE 0 and STEPS_LEFT -1).
+ * The analogue of RUMD's Simulation.Run loop (Simulation.py:538-622) for many
+ * systems at once, without the per-block host round trips. */
+#define B2MD_CHUNK_ACTIVE 0
+#define B2MD_CHUNK_STEPS 1
+#define B2MD_CHUNK_STEPS_LEFT 2
+#define B2MD_CHUNK_PE 3
+#define B2MD_CHUNK_VIRIAL 4
+#define B2MD_CHUNK_KE 5
+#define B2MD_CHUNK_XI 6
+#define B2MD_CHUNK_REBUILDS 7
+#define B2MD_CHUNK_OVERFLOW 8
+#define B2MD_CHUNK_FIELDS 9
+B2MD_API int b2md_run_queued_async(b2md_engine* e, long long max_steps, long long* ticket);
+B2MD_API int b2md_run_queued_poll(b2md_engine* e, long long ticket, int* done);
+B2MD_API int b2md_run_queued_wait(b2md_engine* e, long long ticket, long long* steps_run, double* states,
+                                  int cap);
 
 /* Parity hooks.  Neighbour list of replica id in ORIGINAL particle ids:
  * counts[n], nbl[n][max_nbrs] row-major (entries in list order). */

@@ -20,19 +20,22 @@ CUTOFF = {"NS": 0, "SP": 1, "SF": 2}
 POTENTIAL = {"LJ_12_6": 0, "LJ_12_6_smooth_2_4": 1, "IPL_n": 2}
 # kernel variants (b2md_engine_set_variant)
 VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP, VARIANT_SM_TILES = 0, 1, 2, 3, 4
-VARIANT_WINDOW_LIST_ROWS, VARIANT_PERSISTENT, VARIANT_PERSISTENT_ACTIVE = 5, 6, 7
+VARIANT_WINDOW_LIST_ROWS, VARIANT_PERSISTENT, VARIANT_PERSISTENT_ACTIVE, VARIANT_GRAPH_BUILDS = 5, 6, 7, 8
 FORCE_STREAMED, FORCE_STAGED, FORCE_WINDOW = 0, 1, 2
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",
               "target_T", "max_nbrs", "actual_max_nbrs", "mean_nbrs", "window_tiles", "tiles"]
 NSTAT = len(STAT_NAMES)
 NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
+# per-replica fields of a chunk's snapshot (b2md_run_queued_wait)
+CHUNK_FIELDS = ["active", "steps", "steps_left", "pe", "virial", "ke", "xi", "rebuilds", "overflow"]
 
 EXPORTS = [
     "b2md_engine_create", "b2md_engine_destroy", "b2md_engine_set_launch", "b2md_engine_get_launch",
-    "b2md_engine_memory",
+    "b2md_engine_memory", "b2md_engine_usage", "b2md_replica_footprint", "b2md_run_queued_async",
+    "b2md_run_queued_poll", "b2md_run_queued_wait",
     "b2md_engine_set_graph_mode", "b2md_engine_set_variant", "b2md_engine_get_variant", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
-    "b2md_replica_read", "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_set_integrator",
+    "b2md_replica_read", "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_add_potential", "b2md_replica_set_integrator",
     "b2md_replica_set_xi", "b2md_replica_set_reset_interval", "b2md_replica_set_nb_method",
     "b2md_replica_stats", "b2md_replica_set_energy_log", "b2md_replica_energy_log", "b2md_replica_stress", "b2md_calc_f",
     "b2md_integrate", "b2md_zero_momentum", "b2md_run", "b2md_run_timed", "b2md_replica_queue_steps",
@@ -75,6 +78,11 @@ def lib():
             "b2md_engine_set_launch": [P, i, i],
             "b2md_engine_get_launch": [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
             "b2md_engine_memory": [P, ctypes.POINTER(ll)],
+            "b2md_engine_usage": [P, ctypes.POINTER(ll), ctypes.POINTER(ll)],
+            "b2md_replica_footprint": [P, ctypes.POINTER(ReplicaDesc), ctypes.POINTER(ll)],
+            "b2md_run_queued_async": [P, ll, ctypes.POINTER(ll)],
+            "b2md_run_queued_poll": [P, ll, ctypes.POINTER(i)],
+            "b2md_run_queued_wait": [P, ll, ctypes.POINTER(ll), P, i],
             "b2md_engine_set_graph_mode": [P, i],
             "b2md_engine_set_variant": [P, i, i],
             "b2md_engine_get_variant": [P, i, ctypes.POINTER(ctypes.c_int)],
@@ -84,6 +92,7 @@ def lib():
             "b2md_replica_read": [P, i, P, P, P],
             "b2md_replica_set": [P, i, i, P],
             "b2md_replica_set_potential": [P, i, i, P, i, f, i],
+            "b2md_replica_add_potential": [P, i, i, P, i, i],
             "b2md_replica_set_integrator": [P, i, f, d, d, d, u],
             "b2md_replica_set_xi": [P, i, d],
             "b2md_replica_set_reset_interval": [P, i, i],
@@ -166,6 +175,28 @@ def pack_vel4(vel, masses_per_particle):
     return out
 
 
+def _desc(n, box, params, ntypes, cutoff="SF", skin=0.3, dt=0.005, T=1.0, tau=0.2, thermostat=True, xi=0.0,
+          reset_interval=100, max_nbrs=0, dT_per_step=0.0, energy_interval=0, energy_capacity=0,
+          thermostat_mask=None, potential="LJ_12_6"):
+    """b2md_replica_desc of a system (params: float32, kept alive by the caller)."""
+    d = ReplicaDesc()
+    d.n, d.ntypes = n, ntypes
+    for k in range(3):
+        d.box[k] = float(box[k])
+    d.params = params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    d.cutoff_method = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
+    d.skin, d.dt = skin, dt
+    d.target_T, d.tau, d.dT_per_step, d.xi = T, tau, dT_per_step, xi
+    if thermostat_mask is None:
+        thermostat_mask = 0xFFFFFFFF if thermostat else 0
+    d.thermostat_mask = thermostat_mask
+    d.reset_interval = reset_interval
+    d.max_nbrs = max_nbrs
+    d.energy_interval, d.energy_capacity = energy_interval, energy_capacity
+    d.potential = POTENTIAL[potential] if isinstance(potential, str) else int(potential)
+    return d
+
+
 class Engine:
     """Owns one b2md_engine: any number of resident MD systems on one GPU."""
 
@@ -174,6 +205,7 @@ class Engine:
         check(lib().b2md_engine_create(device, max_particles, max_replicas, max_list_entries, pb, tp,
                                        ctypes.byref(h)))
         self._h = h
+        self._cap = max(int(max_replicas), 1)
         self.pb, self.tp = self.launch()
 
     def close(self):
@@ -219,31 +251,33 @@ class Engine:
         check(lib().b2md_engine_memory(self._h, ctypes.byref(b)))
         return b.value
 
-    def add(self, pos4, box, params, ntypes, cutoff="SF", skin=0.3, dt=0.005, T=1.0, tau=0.2,
-            vel4=None, im3=None, thermostat=True, xi=0.0, reset_interval=100, max_nbrs=0,
-            dT_per_step=0.0, energy_interval=0, energy_capacity=0, thermostat_mask=None, potential="LJ_12_6"):
-        pos4 = np.ascontiguousarray(pos4, np.float32)
-        n = len(pos4)
+    def usage(self):
+        """(bytes held by the active replicas, bytes allocated by the engine)."""
+        u, r = ctypes.c_longlong(), ctypes.c_longlong()
+        check(lib().b2md_engine_usage(self._h, ctypes.byref(u), ctypes.byref(r)))
+        return u.value, r.value
+
+    def footprint(self, n, box, params, ntypes, **kw):
+        """Device bytes a replica of n particles would hold (b2md_replica_footprint);
+        keywords as for add()."""
         params = np.ascontiguousarray(params, np.float32)
-        d = ReplicaDesc()
-        d.n, d.ntypes = n, ntypes
-        for k in range(3):
-            d.box[k] = float(box[k])
-        d.params = params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        d.cutoff_method = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
-        d.skin, d.dt = skin, dt
-        d.target_T, d.tau, d.dT_per_step, d.xi = T, tau, dT_per_step, xi
-        if thermostat_mask is None:
-            thermostat_mask = 0xFFFFFFFF if thermostat else 0
-        d.thermostat_mask = thermostat_mask
-        d.reset_interval = reset_interval
-        d.max_nbrs = max_nbrs
-        d.energy_interval, d.energy_capacity = energy_interval, energy_capacity
-        d.potential = POTENTIAL[potential] if isinstance(potential, str) else int(potential)
+        d = _desc(n, box, params, ntypes, **kw)
+        b = ctypes.c_longlong()
+        check(lib().b2md_replica_footprint(self._h, ctypes.byref(d), ctypes.byref(b)))
+        return b.value
+
+    def add(self, pos4, box, params, ntypes, vel4=None, im3=None, **kw):
+        """Admits one system; keywords: cutoff, skin, dt, T, tau, thermostat, xi,
+        reset_interval, max_nbrs, dT_per_step, energy_interval, energy_capacity,
+        thermostat_mask, potential."""
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        params = np.ascontiguousarray(params, np.float32)
+        d = _desc(len(pos4), box, params, ntypes, **kw)
         v = None if vel4 is None else np.ascontiguousarray(vel4, np.float32)
         im = None if im3 is None else np.ascontiguousarray(im3, np.int32)
         rid = ctypes.c_int()
         check(lib().b2md_replica_add(self._h, ctypes.byref(d), _ptr(pos4), _ptr(v), _ptr(im), ctypes.byref(rid)))
+        self._cap = max(self._cap, rid.value + 1)
         return rid.value
 
     def remove(self, rid):
@@ -275,6 +309,13 @@ class Engine:
         c = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
         pk = POTENTIAL[potential] if isinstance(potential, str) else int(potential)
         check(lib().b2md_replica_set_potential(self._h, rid, ntypes, _ptr(params), c, skin, pk))
+
+    def add_potential(self, rid, ntypes, params, cutoff, potential="LJ_12_6"):
+        """A second pair potential whose forces and energies add to the first's."""
+        params = np.ascontiguousarray(params, np.float32)
+        c = CUTOFF[cutoff] if isinstance(cutoff, str) else int(cutoff)
+        pk = POTENTIAL[potential] if isinstance(potential, str) else int(potential)
+        check(lib().b2md_replica_add_potential(self._h, rid, ntypes, _ptr(params), c, pk))
 
     def set_integrator(self, rid, dt, T, tau, dT_per_step=0.0, thermostat_mask=0xFFFFFFFF):
         check(lib().b2md_replica_set_integrator(self._h, rid, dt, T, tau, dT_per_step, thermostat_mask))
@@ -336,6 +377,28 @@ class Engine:
         n = ctypes.c_longlong()
         check(lib().b2md_run_queued(self._h, int(max_steps), ctypes.byref(n)))
         return n.value
+
+    def run_queued_async(self, max_steps=0):
+        """Launches a chunk of the queued work and returns its ticket at once."""
+        t = ctypes.c_longlong()
+        check(lib().b2md_run_queued_async(self._h, int(max_steps), ctypes.byref(t)))
+        return t.value
+
+    def poll(self, ticket):
+        """True once the chunk has finished on the GPU (does not block)."""
+        d = ctypes.c_int()
+        check(lib().b2md_run_queued_poll(self._h, int(ticket), ctypes.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket, cap=None):
+        """Waits for a chunk: (steps it ran, [cap, len(CHUNK_FIELDS)] snapshot of
+        every replica id's state at its end; rows of replicas not active at its
+        launch have active 0 and steps_left -1)."""
+        cap = self._cap if cap is None else cap
+        out = np.zeros((cap, len(CHUNK_FIELDS)))
+        n = ctypes.c_longlong()
+        check(lib().b2md_run_queued_wait(self._h, int(ticket), ctypes.byref(n), _ptr(out), cap))
+        return n.value, out
 
     def nbl(self, rid, n, max_nbrs):
         counts = np.zeros(n, np.uint32)

@@ -110,12 +110,42 @@ struct HostRep {
   float rcmax = 0.f, skin = 0.f;
   std::vector<float> params;   // RUMD layout
   int nb_method_req = -1;      // -1 default
+  long long bytes = 0;         // device bytes held in the engine's pools (b2md_engine_usage)
+  // a second pair potential (b2md_replica_add_potential): RUMD layout table,
+  // pair function, cut-off method, its packed table's place
+  std::vector<float> params1;
+  int potential1 = -1, cutoff1 = 0;
+  long long par1 = -1;
+  int npar1 = 0;
 };
 
 template <class T>
 struct DevBuf {
   T* p = nullptr;
   long long n = 0;
+};
+
+// A region of the pinned staging ring whose host-to-device copies may still
+// be queued behind earlier work on the stream; reusable once `ev` completed.
+struct StageBlk {
+  size_t lo, hi;
+  cudaEvent_t ev;
+};
+
+// One chunk of queued steps launched by b2md_run_queued_async, with pinned
+// snapshots of the control block and the replica states copied right after
+// it in stream order.
+struct ChunkRec {
+  long long ticket = 0;        // 0: never used
+  bool waited = true;
+  bool persistent = false;     // budgeted persistent graph (else per-step graphs)
+  long long budget = 0, ran = 0;
+  cudaEvent_t done = nullptr;
+  int* h_in = nullptr;         // pinned: the step budget copied to the device
+  PersistCtl* h_ctl = nullptr; // pinned: control block after the chunk
+  RepState* h_st = nullptr;    // pinned: replica states after the chunk
+  int st_cap = 0;
+  std::vector<char> active;    // replicas active when the chunk was launched
 };
 
 }  // namespace
@@ -146,6 +176,19 @@ struct b2md_engine {
   int* h_budget = nullptr;     // pinned: the step budget written before each persistent launch
   void* h_stage = nullptr;     // pinned staging for particle uploads and read-backs (grown on demand)
   size_t h_stage_bytes = 0;
+  // pinned ring for host-to-device copies that may wait behind running work
+  // (admissions, layout uploads): a call fills a region and returns at once
+  char* ring = nullptr;
+  size_t ring_cap = 0, ring_head = 0;
+  std::vector<StageBlk> ring_pending;                  // regions with copies possibly in flight
+  std::vector<std::pair<size_t, size_t>> ring_open;    // regions of the current call (no event yet)
+  bool layout_dirty = false;     // admissions/removals since the last tile layout upload
+  std::vector<int> momentum_due; // replicas whose momentum is computed after the next upload
+  int graph_types = 0;           // pair-table rows in the current persistent graph's shared memory
+  bool wl_on = false;            // window-list pool allocated (force mode 2 used)
+  int graph_builds = 0;          // step-graph instantiations so far (B2MD_VARIANT_GRAPH_BUILDS)
+  ChunkRec chunk[2];             // b2md_run_queued_async chunks (by ticket parity)
+  long long chunk_seq = 0;
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
   float4* r[2] = {nullptr, nullptr};
   float4* v[2] = {nullptr, nullptr};
@@ -230,6 +273,76 @@ bool is_pinned(const void* p) {
   return at.type == cudaMemoryTypeHost;
 }
 
+// ---- pinned staging ring ----
+// Host-to-device copies from pageable memory may make the driver wait for the
+// stream, so copies that should not wait for running work (admissions, tile
+// layouts) go through this ring: the call copies its data into a region,
+// queues the copies and records an event behind them; a later call reuses the
+// region once that event has completed.  Only when the ring is full does a
+// call wait, for the oldest copies in its way.
+void ring_reset(b2md_engine* e) {
+  for (auto& b : e->ring_pending) cudaEventDestroy(b.ev);
+  e->ring_pending.clear();
+  e->ring_open.clear();
+  e->ring_head = 0;
+}
+
+// Records an event behind the copies queued from this call's regions.
+void stage_commit(b2md_engine* e) {
+  for (const auto& o : e->ring_open) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, e->stream));
+    e->ring_pending.push_back({o.first, o.second, ev});
+  }
+  e->ring_open.clear();
+}
+
+char* stage_alloc(b2md_engine* e, size_t bytes) {
+  const size_t n = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
+  if (2 * n > e->ring_cap) {
+    // grow: nothing may still read the old ring
+    CK(cudaStreamSynchronize(e->stream));
+    ring_reset(e);
+    if (e->ring) CK(cudaFreeHost(e->ring));
+    e->ring = nullptr;
+    e->ring_cap = 0;
+    const size_t cap = std::max<size_t>(4 * n, (size_t)16 << 20);
+    CK(cudaMallocHost(&e->ring, cap));
+    e->ring_cap = cap;
+  }
+  size_t lo = e->ring_head;
+  if (lo + n > e->ring_cap) lo = 0;
+  const size_t hi = lo + n;
+  for (const auto& o : e->ring_open)
+    if (o.first < hi && lo < o.second) {  // this call's own earlier region: commit it first
+      stage_commit(e);
+      break;
+    }
+  for (size_t k = 0; k < e->ring_pending.size();) {
+    StageBlk& b = e->ring_pending[k];
+    bool done;
+    if (b.lo < hi && lo < b.hi) {
+      CK(cudaEventSynchronize(b.ev));
+      done = true;
+    } else {
+      const cudaError_t q = cudaEventQuery(b.ev);
+      if (q != cudaSuccess && q != cudaErrorNotReady) throw CudaErr{q, "cudaEventQuery(stage)", __LINE__};
+      done = q == cudaSuccess;
+    }
+    if (done) {
+      cudaEventDestroy(b.ev);
+      b = e->ring_pending.back();
+      e->ring_pending.pop_back();
+    } else {
+      ++k;
+    }
+  }
+  e->ring_head = hi;
+  e->ring_open.push_back({lo, hi});
+  return e->ring + lo;
+}
+
 void invalidate_graphs(b2md_engine* e) {
   for (int k = 0; k < 3; ++k) {
     if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
@@ -263,13 +376,22 @@ void grow_particles(b2md_engine* e, long long need) {
   invalidate_graphs(e);
 }
 
+// The list pool; the 16-bit window list beside it only once force mode 2
+// has been chosen (enable_window_list).
 void grow_list(b2md_engine* e, long long need) {
   if (need <= e->ecap) return;
   long long nc = std::max(need, e->ecap + e->ecap / 2);
   dev_grow(e, e->nbl, e->ecap, nc, false);
-  dev_grow(e, e->wl, e->ecap, nc, false);
+  if (e->wl_on) dev_grow(e, e->wl, e->ecap, nc, false);
   e->ealloc.grow(nc);
   e->ecap = nc;
+  invalidate_graphs(e);
+}
+
+void enable_window_list(b2md_engine* e) {
+  if (e->wl_on) return;
+  dev_grow(e, e->wl, 0, e->ecap, false);
+  e->wl_on = true;
   invalidate_graphs(e);
 }
 
@@ -310,6 +432,14 @@ void grow_reps(b2md_engine* e, int need) {
   dev_grow(e, e->flist, 2LL * e->rcap, 2LL * nc, true);  // two halves (k_batch: by step parity)
   e->rcap = nc;
   invalidate_graphs(e);
+}
+
+// Largest type count over the active replicas.
+int max_types_active(const b2md_engine* e) {
+  int m = 1;
+  for (const auto& h : e->reps)
+    if (h.active) m = std::max(m, h.d.ntypes);
+  return m;
 }
 
 EngArgs make_args(b2md_engine* e) {
@@ -385,19 +515,9 @@ void drop_windows(b2md_engine* e) {
   if (e->wmeta && e->tcap > 0) CK(cudaMemsetAsync(e->wmeta, 0xff, (size_t)e->tcap * sizeof(int2), e->stream));
 }
 
-// Re-lays out tiles and reduction groups over the active replicas and uploads
-// the replica table.
-void relayout(b2md_engine* e) {
-  int T = 0, G = 0;
-  for (auto& h : e->reps) {
-    if (!h.active) { h.d.tile0 = T; h.d.ntiles = 0; h.d.group0 = G; h.d.ngroups = 0; h.d.active = 0; continue; }
-    h.d.tile0 = T;
-    h.d.ntiles = (h.n + e->pb - 1) / e->pb;
-    h.d.group0 = G;
-    h.d.ngroups = (h.d.ntiles + kGroup - 1) / kGroup;
-    T += h.d.ntiles;
-    G += h.d.ngroups;
-  }
+// Tile and reduction-group tables of at least T tiles and G groups.
+bool grow_tiles(b2md_engine* e, int T, int G) {
+  bool grew = false;
   if (T > e->tcap) {
     int nc = std::max(T, e->tcap * 2);
     dev_grow(e, e->tile_rep, e->tcap, nc, true);
@@ -408,34 +528,93 @@ void relayout(b2md_engine* e) {
     dev_grow(e, e->wseg, (long long)e->tcap * kWinSeg, (long long)nc * kWinSeg, false);
     dev_grow(e, e->wmeta, e->tcap, nc, false);
     e->tcap = nc;
+    grew = true;
   }
   if (G > e->gcap) {
     int nc = std::max(G, e->gcap * 2);
     dev_grow(e, e->gpart, 2LL * e->gcap * kNPart, 2LL * nc * kNPart, false);  // two halves
     dev_grow(e, e->gctr, 2LL * e->gcap, 2LL * nc, true);  // two halves
     e->gcap = nc;
+    grew = true;
   }
-  std::vector<int> trep(T), tfirst(T);
-  for (size_t r = 0; r < e->reps.size(); ++r) {
+  if (grew) invalidate_graphs(e);
+  return grew;
+}
+
+int persist_kind_for(b2md_engine* e);
+int max_types_active(const b2md_engine* e);
+
+// Re-lays out tiles and reduction groups over the active replicas and queues
+// the upload of the tile tables, the replica table and the layout words that
+// k_batch reads, through the staging ring: nothing waits for running work.
+// A batched persistent graph stays valid (it reads the layout from the
+// device) unless the pools moved or a replica brings more particle types
+// than its shared-memory pair table holds; the other graphs capture the
+// layout and are rebuilt.
+void apply_layout(b2md_engine* e) {
+  int T = 0, G = 0;
+  for (auto& h : e->reps) {
+    if (!h.active) { h.d.tile0 = T; h.d.ntiles = 0; h.d.group0 = G; h.d.ngroups = 0; h.d.active = 0; continue; }
+    h.d.tile0 = T;
+    h.d.ntiles = (h.n + e->pb - 1) / e->pb;
+    h.d.group0 = G;
+    h.d.ngroups = (h.d.ntiles + kGroup - 1) / kGroup;
+    T += h.d.ntiles;
+    G += h.d.ngroups;
+  }
+  grow_tiles(e, T, G);
+  const int R = (int)e->reps.size();
+  const size_t tb = ((size_t)T * sizeof(int) + 15) & ~(size_t)15;
+  const size_t rb = (size_t)R * sizeof(RepDev);
+  char* stage = stage_alloc(e, 2 * tb + rb + 16);
+  int* trep = reinterpret_cast<int*>(stage);
+  int* tfirst = reinterpret_cast<int*>(stage + tb);
+  RepDev* table = reinterpret_cast<RepDev*>(stage + 2 * tb);
+  int* lay = reinterpret_cast<int*>(stage + 2 * tb + rb);
+  for (int r = 0; r < R; ++r) {
     const HostRep& h = e->reps[r];
+    table[r] = h.d;
     for (int t = 0; t < h.d.ntiles; ++t) {
-      trep[h.d.tile0 + t] = (int)r;
+      trep[h.d.tile0 + t] = r;
       tfirst[h.d.tile0 + t] = t * e->pb;
     }
   }
+  lay[0] = T;
+  lay[1] = R;
   if (T > 0) {
-    CK(cudaMemcpyAsync(e->tile_rep, trep.data(), T * sizeof(int), cudaMemcpyHostToDevice, e->stream));
-    CK(cudaMemcpyAsync(e->tile_first, tfirst.data(), T * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->tile_rep, trep, T * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+    CK(cudaMemcpyAsync(e->tile_first, tfirst, T * sizeof(int), cudaMemcpyHostToDevice, e->stream));
   }
-  std::vector<RepDev> table(e->reps.size());
-  for (size_t r = 0; r < e->reps.size(); ++r) table[r] = e->reps[r].d;
-  if (!table.empty())
-    CK(cudaMemcpyAsync(e->rep, table.data(), table.size() * sizeof(RepDev), cudaMemcpyHostToDevice, e->stream));
-  CK(cudaStreamSynchronize(e->stream));
+  if (R > 0) CK(cudaMemcpyAsync(e->rep, table, rb, cudaMemcpyHostToDevice, e->stream));
+  static_assert(offsetof(PersistCtl, lay_nrep) == offsetof(PersistCtl, lay_ntiles) + sizeof(int), "layout words");
+  CK(cudaMemcpyAsync(&e->pctl->lay_ntiles, lay, 2 * sizeof(int), cudaMemcpyHostToDevice, e->stream));
+  stage_commit(e);
   e->ntiles = T;
   e->ngroups = G;
+  e->layout_dirty = false;
   drop_windows(e);  // tiles changed: no window until the next list build
-  invalidate_graphs(e);
+  const bool keep = e->graphs_valid && e->persist_kind == 2 && persist_kind_for(e) == 2 &&
+                    max_types_active(e) <= e->graph_types;
+  if (!keep) invalidate_graphs(e);
+}
+
+// Applies admissions and removals made since the last launch, then computes
+// the momentum of the replicas admitted since (before any kernel uses them).
+void launch_momentum_of(b2md_engine* e, int id);
+void ensure_layout(b2md_engine* e) {
+  if (e->layout_dirty) apply_layout(e);
+  if (!e->momentum_due.empty()) {
+    std::vector<int> due;
+    due.swap(e->momentum_due);
+    for (int id : due)
+      if (id < (int)e->reps.size() && e->reps[id].active) launch_momentum_of(e, id);
+  }
+}
+
+// Re-layout now (a launch shape change).
+void relayout(b2md_engine* e) {
+  e->layout_dirty = true;
+  ensure_layout(e);
 }
 
 void upload_rep(b2md_engine* e, int id) {
@@ -473,9 +652,8 @@ void write_field(b2md_engine* e, int id, size_t off, const T& val) {
 }
 #define WRITE_STATE(e, id, field, val) write_field(e, id, offsetof(RepState, field), (decltype(RepState::field))(val))
 
-// Packs a RUMD parameter table into the engine's per-pair rows and derives
-// the cell grid (NeighborList.cu:717-732).
-void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, float skin, int potential) {
+// A RUMD parameter table's pair function, cut-off method and parameters.
+void check_potential(int ntypes, const float* params, int cutoff, int potential) {
   if (ntypes < 1 || ntypes > kMaxTypes) api_fail(B2MD_ERR_ARG, "ntypes must be 1..8");
   if (cutoff < 0 || cutoff > 2) api_fail(B2MD_ERR_ARG, "cutoff method must be NS, SP or SF");
   if (potential < POT_LJ_12_6 || potential > POT_IPL_N)
@@ -484,15 +662,38 @@ void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, floa
     for (int k = 0; k < ntypes * ntypes; ++k)
       if (params[k * kNumParam] > 0.f && !(params[k * kNumParam + 1] > 0.f))
         api_fail(B2MD_ERR_ARG, "pair parameter 1 (1/sigma^2) must be positive");
+}
+
+// Cell grid (NeighborList.cu:717-732), method and minimum-image limits from
+// the largest cut-off of the replica's potentials.
+void derive_grid(HostRep& h);
+
+// Sample::SetPotential (Sample.cu:251-259): the replica's potential list
+// becomes this one potential (a second one added earlier is dropped).
+void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, float skin, int potential) {
+  check_potential(ntypes, params, cutoff, potential);
   if (!(skin >= 0.f)) api_fail(B2MD_ERR_ARG, "skin must be >= 0");
+  float rc = 0.f;
+  for (int k = 0; k < ntypes * ntypes; ++k) rc = std::max(rc, params[k * kNumParam]);
+  if (!(rc > 0.f)) api_fail(B2MD_ERR_ARG, "all cut-offs are zero");
   h.d.potential = potential;
   h.params.assign(params, params + ntypes * ntypes * kNumParam);
   h.d.ntypes = ntypes;
   h.d.cutoff = cutoff;
   h.skin = skin;
+  h.params1.clear();
+  h.potential1 = -1;
+  h.d.npot = 1;
+  h.d.potential1 = 0;
+  derive_grid(h);
+}
+
+void derive_grid(HostRep& h) {
+  const int ntypes = h.d.ntypes;
+  const float skin = h.skin;
   h.rcmax = 0.f;
-  for (int k = 0; k < ntypes * ntypes; ++k) h.rcmax = std::max(h.rcmax, params[k * kNumParam]);
-  if (!(h.rcmax > 0.f)) api_fail(B2MD_ERR_ARG, "all cut-offs are zero");
+  for (int k = 0; k < ntypes * ntypes; ++k) h.rcmax = std::max(h.rcmax, h.params[k * kNumParam]);
+  for (size_t k = 0; k < h.params1.size() / kNumParam; ++k) h.rcmax = std::max(h.rcmax, h.params1[k * kNumParam]);
   h.d.skin2_4 = (float)(0.25 * skin * skin);
   for (int d = 0; d < 3; ++d) h.d.ilim[d] = 0.5f * h.d.L[d] - (h.rcmax + 2.f * skin) - 0.01f;
   int ncheck[3];
@@ -507,28 +708,36 @@ void set_potential(HostRep& h, int ntypes, const float* params, int cutoff, floa
   else h.d.nb_method = grid_complete ? NB_CELLS : NB_N2;
 }
 
-std::vector<float> pack_params(const HostRep& h) {
+// The engine's per-pair rows of one potential (RUMD table `params`, pair
+// function `pot`, cut-off method `cutoff`).  q[6], the list build's
+// (rc + skin)^2, is the larger over the replica's potentials in the first
+// table (the list serves both).
+std::vector<float> pack_table(const HostRep& h, const std::vector<float>& params, int pot, int cutoff) {
   int T = h.d.ntypes;
   std::vector<float> out(T * T * kParStride, 0.f);
   for (int k = 0; k < T * T; ++k) {
-    const float* p = &h.params[k * kNumParam];
+    const float* p = &params[k * kNumParam];
     float* q = &out[k * kParStride];
     float rc = p[0];
     const float sc = p[kNumParam - 2], uc = p[kNumParam - 1];  // s(rc)*rc, u(rc)
     // fij's cut-off terms (PairPotential.h:1208-1221) as s -= c_s/r, u += c_s r + c_u0
-    const bool sf = h.d.cutoff == CUT_SF, sp = h.d.cutoff == CUT_SP;
+    const bool sf = cutoff == CUT_SF, sp = cutoff == CUT_SP;
     const float c_s = sf ? sc : 0.f;
     const float c_u0 = sf ? -(sc * rc + uc) : (sp ? -uc : 0.f);
     float cs = rc + h.skin;  // calculateNBL_*: (params + skin)^2 in float
     q[0] = rc * rc;
     q[6] = cs * cs;
-    if (h.d.potential == POT_LJ_12_6) {
+    if (&params == &h.params && !h.params1.empty()) {
+      const float cs1 = h.params1[k * kNumParam] + h.skin;
+      q[6] = std::max(q[6], cs1 * cs1);
+    }
+    if (pot == POT_LJ_12_6) {
       q[1] = p[1];
       q[2] = p[2];
       q[3] = c_s;
       q[4] = c_u0;
       q[5] = c_s;
-    } else if (h.d.potential == POT_LJ_12_6_SMOOTH_2_4) {
+    } else if (pot == POT_LJ_12_6_SMOOTH_2_4) {
       // u = 4eps [(s/r)^12 - (s/r)^6 + c2 (r/s)^2 + c4 (r/s)^4]: the r^2 and
       // r^4 terms folded into b, c (force) and e, g (energy) per unit of d^2
       const float is2 = p[1], a = p[2], c2 = p[3], c4 = p[4];
@@ -577,21 +786,42 @@ void place_cells(b2md_engine* e, HostRep& h) {
   h.d.ncell = ncell;
 }
 
-void place_params(b2md_engine* e, HostRep& h) {
-  std::vector<float> packed = pack_params(h);
-  int np = (int)packed.size();
-  if (h.par0 < 0 || h.npar != np) {
-    if (h.par0 >= 0) e->qalloc.release(h.par0, h.npar);
-    long long off = e->qalloc.alloc(np, 8);
-    if (off < 0) {
+// One packed table into the parameter pool at *off (placed, or moved when
+// its size changed), uploaded through the staging ring.
+void place_table(b2md_engine* e, const std::vector<float>& packed, long long* off, int* len) {
+  const int np = (int)packed.size();
+  if (*off < 0 || *len != np) {
+    if (*off >= 0) e->qalloc.release(*off, *len);
+    long long o = e->qalloc.alloc(np, 8);
+    if (o < 0) {
       grow_params(e, e->qcap + np + 8);
-      off = e->qalloc.alloc(np, 8);
+      o = e->qalloc.alloc(np, 8);
     }
-    h.par0 = off;
-    h.npar = np;
-    h.d.par0 = (int)off;
+    *off = o;
+    *len = np;
   }
-  CK(cudaMemcpyAsync(e->par + h.par0, packed.data(), np * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+  float* stage = reinterpret_cast<float*>(stage_alloc(e, np * sizeof(float)));
+  std::memcpy(stage, packed.data(), np * sizeof(float));
+  CK(cudaMemcpyAsync(e->par + *off, stage, np * sizeof(float), cudaMemcpyHostToDevice, e->stream));
+  stage_commit(e);
+}
+
+// The replica's packed tables: its potential's, and a second potential's.
+void place_params(b2md_engine* e, HostRep& h) {
+  place_table(e, pack_table(h, h.params, h.d.potential, h.d.cutoff), &h.par0, &h.npar);
+  h.d.par0 = (int)h.par0;
+  if (h.potential1 >= 0) {
+    place_table(e, pack_table(h, h.params1, h.potential1, h.cutoff1), &h.par1, &h.npar1);
+    h.d.par1 = (int)h.par1;
+    h.d.npot = 2;
+    h.d.potential1 = h.potential1;
+  } else {
+    if (h.par1 >= 0) e->qalloc.release(h.par1, h.npar1);
+    h.par1 = -1;
+    h.npar1 = 0;
+    h.d.par1 = 0;
+    h.d.npot = 1;
+  }
 }
 
 void place_list(b2md_engine* e, HostRep& h, int max_nbrs) {
@@ -837,6 +1067,14 @@ bool batch_eligible(const b2md_engine* e) {
   return true;
 }
 
+// The persistent kernels evaluate one potential per replica; a replica with
+// a second one runs on the per-step graphs (k_force adds its sums).
+bool single_potential(const b2md_engine* e) {
+  for (const auto& h : e->reps)
+    if (h.active && h.d.npot > 1) return false;
+  return true;
+}
+
 // Dynamic shared memory of k_batch: the larger of the force tile's region and
 // the list build's, then the per-block rebuild-list tables.
 size_t batch_smem(const b2md_engine* e, EngArgs& a) {
@@ -930,6 +1168,7 @@ void build_persist_graph(b2md_engine* e) {
 // and launches again).
 void build_batch_graph(b2md_engine* e) {
   EngArgs a = make_args(e);
+  e->graph_types = a.max_types;
   const size_t smem = batch_smem(e, a);
   force_fn(e, true, false, a);  // checks the shared-memory need
   BatchFn fb = batch_fn(e->tp);
@@ -983,6 +1222,7 @@ void build_batch_graph(b2md_engine* e) {
 // with persistent = 2), 0 none (one launch per step).
 int persist_kind_for(b2md_engine* e) {
   if (!persist_mode(e) || e->ntiles == 0 || e->reps.size() >= (1u << 20)) return 0;  // the barrier tally fields
+  if (!single_potential(e)) return 0;
   if (e->persist == 1) {
     EngArgs a = make_args(e);
     int per_sm = 0;
@@ -1012,6 +1252,7 @@ void ensure_graphs(b2md_engine* e) {
     build_graph(e, 1, kChunk);
   }
   e->graphs_valid = true;
+  ++e->graph_builds;
 }
 
 // A step-barrier wait of k_steps that gave up (reported, then cleared).
@@ -1049,6 +1290,7 @@ bool repair_overflow(b2md_engine* e) {
 }
 
 void calc_f(b2md_engine* e, bool stress) {
+  ensure_layout(e);
   for (int attempt = 0; attempt < 8; ++attempt) {
     EngArgs a = make_args(e);
     launch_rebuild(e, e->stream, a);
@@ -1069,6 +1311,7 @@ long long max_steps_left(b2md_engine* e) {
 
 // Runs up to `limit` steps of the queued work with the step graphs.
 long long run_steps(b2md_engine* e, long long limit) {
+  ensure_layout(e);
   long long done = 0;
   for (int guard = 0; guard < 64; ++guard) {
     long long todo = std::min(max_steps_left(e), limit - done);
@@ -1118,6 +1361,81 @@ int guarded(F&& fn) {
   }
 }
 
+// Waits for a chunk of b2md_run_queued_async and checks what it left: a
+// step-barrier wait that gave up is reported; overflowed lists are enlarged
+// and flagged for a rebuild (their replicas continue in the next chunk).
+void finish_chunk(b2md_engine* e, ChunkRec& c) {
+  CK(cudaEventSynchronize(c.done));
+  c.waited = true;
+  if (c.h_ctl->err) {
+    CK(cudaStreamSynchronize(e->stream));
+    check_persist(e);  // clears the flag and reports
+  }
+  c.ran = c.persistent ? c.budget - c.h_ctl->budget : c.budget;
+  bool fix = false;
+  for (size_t r = 0; r < c.active.size(); ++r)
+    if (c.active[r] && (c.h_st[r].overflow || c.h_st[r].err)) fix = true;
+  if (fix) repair_overflow(e);
+}
+
+ChunkRec* find_chunk(b2md_engine* e, long long ticket) {
+  for (auto& c : e->chunk)
+    if (c.ticket == ticket && ticket > 0) return &c;
+  api_fail(B2MD_ERR_ARG, "no chunk with this ticket (only the two most recent are kept)");
+}
+
+// A replica's host record from its description: validated, potential
+// packed and cell grid derived, nothing placed yet.
+HostRep describe(const b2md_replica_desc* d) {
+  if (d->n < 2) api_fail(B2MD_ERR_ARG, "need at least 2 particles");
+  for (int k = 0; k < 3; ++k)
+    if (!(d->box[k] > 0.f)) api_fail(B2MD_ERR_ARG, "box lengths must be positive");
+  if (!d->params) api_fail(B2MD_ERR_ARG, "params is null");
+  if (!(d->dt > 0.f)) api_fail(B2MD_ERR_ARG, "dt must be positive");
+  HostRep h;
+  h.n = d->n;
+  h.np = (d->n + 31) / 32 * 32;
+  h.d.n = d->n;
+  for (int k = 0; k < 3; ++k) {
+    h.d.L[k] = d->box[k];
+    h.d.invL[k] = 1.f / d->box[k];
+  }
+  set_potential(h, d->ntypes, d->params, d->cutoff_method, d->skin, d->potential);
+  h.d.dt = d->dt;
+  h.d.omega2 = (float)(4. * M_PI * M_PI / (d->tau * d->tau));
+  h.d.thermo_mask = d->thermostat_mask;
+  h.d.reset_interval = d->reset_interval;
+  h.d.dof = 3.0 * d->n - 3.0;
+  h.d.energy_interval = d->energy_interval;
+  h.d.active = 1;
+  return h;
+}
+
+int list_capacity(const HostRep& h, const b2md_replica_desc* d) {
+  return d->max_nbrs > 0 ? d->max_nbrs : estimate_max_nbrs(h);
+}
+
+// Device bytes per particle slot: r, v, images and ids double-buffered,
+// forces, virials, stresses, last-build positions, list length, sort order,
+// cell keys and slots.
+constexpr long long kSlotBytes = 2 * (3 * sizeof(float4) + sizeof(unsigned)) + 4 * sizeof(float4) + 4 * sizeof(int);
+
+// Device bytes replica h holds in the engine's pools (its slots, its list
+// -- and window list once force mode 2 is in use --, cells, pair table,
+// energy log, tile and group tables and its replica-table entries).
+long long replica_bytes(const b2md_engine* e, const HostRep& h) {
+  const long long nt = (h.n + e->pb - 1) / e->pb, ng = (nt + kGroup - 1) / kGroup;
+  long long b = (long long)h.np * kSlotBytes;
+  b += (long long)list_rows(h.d.max_nbrs) * h.np * (long long)(sizeof(unsigned) + (e->wl_on ? sizeof(unsigned short) : 0));
+  b += (long long)h.ncell * 2 * sizeof(int);
+  b += (long long)h.d.npot * h.d.ntypes * h.d.ntypes * kParStride * sizeof(float);
+  b += (long long)h.ecap * 5 * sizeof(double);
+  b += nt * (long long)(4 * sizeof(int) + 2 * kNPart * sizeof(double) + kWinSeg * sizeof(int4) + sizeof(int2));
+  b += ng * (long long)(2 * kNPart * sizeof(double) + 2 * sizeof(unsigned));
+  b += (long long)(sizeof(RepDev) + sizeof(RepState) + 4 * sizeof(int));
+  return b;
+}
+
 // RUMD's launch shapes mapped onto the engine's: tiles are whole warps (pb
 // rounded up to a multiple of 32, at most 512) and tp is a power of two up
 // to 8 (the largest one <= the request), halved until pb * tp <= 512.  RUMD's
@@ -1137,9 +1455,19 @@ bool map_launch(int pb, int tp, int* pb_out, int* tp_out) {
 }
 
 void launch_momentum(b2md_engine* e) {
+  ensure_layout(e);
   if (e->ntiles == 0) return;
   EngArgs a = make_args(e);
-  k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
+  k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp, 0);
+  check_launch();
+}
+
+// The momentum of one replica's velocities (after its admission).
+void launch_momentum_of(b2md_engine* e, int id) {
+  const HostRep& h = e->reps[id];
+  if (h.d.ntiles == 0) return;
+  EngArgs a = make_args(e);
+  k_momentum<<<h.d.ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp, h.d.tile0);
   check_launch();
 }
 
@@ -1179,10 +1507,17 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
     e->zalloc.init(0);
     grow_particles(e, std::max<long long>(max_particles, 32));
     grow_list(e, std::max<long long>(max_list_entries, 1024));
-    grow_cells(e, 1024);
-    grow_params(e, 1024);
+    // cells, pair tables and tile tables for the expected particles and
+    // replicas, so that admissions up to them do not grow (and move) a pool
+    const long long R = std::max(max_replicas, 1);
+    grow_cells(e, std::max<long long>(1024, max_particles / 2 + 128 * R));
+    grow_params(e, std::max<long long>(1024, 64 * R));
     grow_elog(e, 16);
-    grow_reps(e, std::max(max_replicas, 1));
+    grow_reps(e, (int)R);
+    if (max_particles > 0) {
+      const long long T = std::min<long long>(max_particles / pb + R, 1 << 30);
+      grow_tiles(e, (int)T, (int)(T / kGroup + R));
+    }
     // pinned staging for the expected particles, so that admissions and
     // read-backs do not allocate it later
     if (max_particles > 0) host_stage(e, (size_t)max_particles * kStagePerParticle);
@@ -1222,6 +1557,14 @@ int b2md_engine_destroy(b2md_engine* e) {
     if (p) cudaFree(p);
   if (e->h_budget) cudaFreeHost(e->h_budget);
   if (e->h_stage) cudaFreeHost(e->h_stage);
+  ring_reset(e);
+  if (e->ring) cudaFreeHost(e->ring);
+  for (auto& c : e->chunk) {
+    if (c.done) cudaEventDestroy(c.done);
+    if (c.h_in) cudaFreeHost(c.h_in);
+    if (c.h_ctl) cudaFreeHost(c.h_ctl);
+    if (c.h_st) cudaFreeHost(c.h_st);
+  }
   if (e->stream) cudaStreamDestroy(e->stream);
   if (e->cap_stream) cudaStreamDestroy(e->cap_stream);
   delete e;
@@ -1236,6 +1579,9 @@ int b2md_engine_set_launch(b2md_engine* e, int pb, int tp) {
     CK(cudaStreamSynchronize(e->stream));
     e->pb = pb;
     e->tp = tp;
+    invalidate_graphs(e);
+    for (auto& h : e->reps)
+      if (h.active) h.bytes = replica_bytes(e, h);
     relayout(e);
   });
 }
@@ -1266,8 +1612,13 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
     case B2MD_VARIANT_FORCE_MODE:
       if (value < FM_STREAMED || value > FM_WINDOW) return fail(B2MD_ERR_ARG, "force mode must be 0, 1 or 2");
       if (value == FM_WINDOW && e->force_mode != FM_WINDOW) {
-        // windows of earlier builds may be stale: none until the next list build
-        int rc = guarded([&] { drop_windows(e); });
+        // windows of earlier builds may be stale: none until the next list
+        // build, which also makes the window list (allocated now)
+        int rc = guarded([&] {
+          CK(cudaSetDevice(e->device));
+          enable_window_list(e);
+          drop_windows(e);
+        });
         if (rc) return rc;
       }
       e->force_mode = value;
@@ -1307,6 +1658,8 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
       break;
     case B2MD_VARIANT_PERSISTENT_ACTIVE:
       return fail(B2MD_ERR_ARG, "persistent_active is read-only");
+    case B2MD_VARIANT_GRAPH_BUILDS:
+      return fail(B2MD_ERR_ARG, "graph_builds is read-only");
     default:
       return fail(B2MD_ERR_ARG, "unknown variant %d", which);
   }
@@ -1325,6 +1678,7 @@ int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
     case B2MD_VARIANT_BUILD_SMEM: *value = e->build_smem ? 1 : 0; break;
     case B2MD_VARIANT_PERSISTENT: *value = e->persist; break;
     case B2MD_VARIANT_PERSISTENT_ACTIVE: *value = (e->graphs_valid && e->persist_on) ? e->persist_kind : 0; break;
+    case B2MD_VARIANT_GRAPH_BUILDS: *value = e->graph_builds; break;
     default: return fail(B2MD_ERR_ARG, "unknown variant %d", which);
   }
   return B2MD_OK;
@@ -1333,14 +1687,18 @@ int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
 int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* pos4, const float* vel4,
                      const int* im3, int* id_out) {
   if (!e || !d || !pos4 || !id_out) return fail(B2MD_ERR_ARG, "null argument");
-  if (d->n < 2) return fail(B2MD_ERR_ARG, "need at least 2 particles");
-  for (int k = 0; k < 3; ++k)
-    if (!(d->box[k] > 0.f)) return fail(B2MD_ERR_ARG, "box lengths must be positive");
-  if (!d->params) return fail(B2MD_ERR_ARG, "params is null");
-  if (!(d->dt > 0.f)) return fail(B2MD_ERR_ARG, "dt must be positive");
   return guarded([&] {
     CK(cudaSetDevice(e->device));
-    CK(cudaStreamSynchronize(e->stream));
+    HostRep h = describe(d);
+    // types must be in range, inverse masses positive
+    for (int i = 0; i < d->n; ++i) {
+      int t;
+      std::memcpy(&t, &pos4[4 * i + 3], 4);
+      if (t < 0 || t >= d->ntypes) api_fail(B2MD_ERR_ARG, "particle type out of range");
+    }
+    if (vel4)
+      for (int i = 0; i < h.n; ++i)
+        if (!(vel4[4 * i + 3] > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass (vel4[.,3]) must be positive");
     int id = -1;
     for (size_t r = 0; r < e->reps.size(); ++r)
       if (!e->reps[r].active) { id = (int)r; break; }
@@ -1349,28 +1707,6 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
       grow_reps(e, id + 1);
       e->reps.emplace_back();
     }
-    HostRep h;
-    h.n = d->n;
-    h.np = (d->n + 31) / 32 * 32;
-    h.d.n = d->n;
-    for (int k = 0; k < 3; ++k) {
-      h.d.L[k] = d->box[k];
-      h.d.invL[k] = 1.f / d->box[k];
-    }
-    set_potential(h, d->ntypes, d->params, d->cutoff_method, d->skin, d->potential);
-    // types must be in range
-    for (int i = 0; i < d->n; ++i) {
-      int t;
-      std::memcpy(&t, &pos4[4 * i + 3], 4);
-      if (t < 0 || t >= d->ntypes) api_fail(B2MD_ERR_ARG, "particle type out of range");
-    }
-    h.d.dt = d->dt;
-    h.d.omega2 = (float)(4. * M_PI * M_PI / (d->tau * d->tau));
-    h.d.thermo_mask = d->thermostat_mask;
-    h.d.reset_interval = d->reset_interval;
-    h.d.dof = 3.0 * d->n - 3.0;
-    h.d.energy_interval = d->energy_interval;
-    h.d.active = 1;
     // particle segment
     long long p0 = e->palloc.alloc(h.np, 32);
     if (p0 < 0) {
@@ -1382,7 +1718,7 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
     h.d.p0 = (int)p0;
     place_cells(e, h);
     place_params(e, h);
-    place_list(e, h, d->max_nbrs > 0 ? d->max_nbrs : estimate_max_nbrs(h));
+    place_list(e, h, list_capacity(h, d));
     if (d->energy_interval > 0 && d->energy_capacity > 0) {
       long long z = e->zalloc.alloc(d->energy_capacity, 1);
       if (z < 0) {
@@ -1398,35 +1734,38 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
       h.d.energy_cap = 0;
     }
     h.active = true;
-    // upload particle data (slot order = original order until the first
-    // sort): one pinned staging area holds r, v and the images as the device
-    // stores them, so each is one DMA copy; last_r and the ids are made on
-    // the device
-    if (vel4)
-      for (int i = 0; i < h.n; ++i)
-        if (!(vel4[4 * i + 3] > 0.f)) api_fail(B2MD_ERR_ARG, "inverse mass (vel4[.,3]) must be positive");
+    h.bytes = replica_bytes(e, h);
+    // particle data (slot order = original order until the first sort).
+    // Arrays the caller already pinned are copied from directly, and the
+    // call then returns when the copies are done; otherwise r, v and the
+    // images are packed into the staging ring, as the device stores them,
+    // and the call returns at once -- the copies run after the work already
+    // queued (a running chunk), before the next launch.  last_r and the ids
+    // are made on the device.
     const size_t nb = (size_t)h.n * sizeof(float4);
-    char* stage = static_cast<char*>(host_stage(e, (size_t)h.n * kStagePerParticle));
+    const bool direct = is_pinned(pos4) && vel4 && is_pinned(vel4);
     const float4* sr = reinterpret_cast<const float4*>(pos4);
     const float4* sv = reinterpret_cast<const float4*>(vel4);
-    int4* si = reinterpret_cast<int4*>(stage + 2 * nb);
-    // arrays the caller already pinned are copied from directly
-    if (!is_pinned(pos4)) {
-      std::memcpy(stage, pos4, nb);
-      sr = reinterpret_cast<const float4*>(stage);
-    }
-    if (!vel4 || !is_pinned(vel4)) {
+    if (!direct) {
+      char* stage = stage_alloc(e, 2 * nb);
+      float4* r = reinterpret_cast<float4*>(stage);
       float4* v = reinterpret_cast<float4*>(stage + nb);
+      std::memcpy(r, pos4, nb);
       if (vel4) std::memcpy(v, vel4, nb);
       else
         for (int i = 0; i < h.n; ++i) v[i] = make_float4(0.f, 0.f, 0.f, 1.f);
+      sr = r;
       sv = v;
     }
-    for (int i = 0; i < h.n; ++i)
-      si[i] = im3 ? make_int4(im3[3 * i], im3[3 * i + 1], im3[3 * i + 2], 0) : make_int4(0, 0, 0, 0);
     CK(cudaMemcpyAsync(e->r[0] + p0, sr, nb, cudaMemcpyHostToDevice, e->stream));
     CK(cudaMemcpyAsync(e->v[0] + p0, sv, nb, cudaMemcpyHostToDevice, e->stream));
-    CK(cudaMemcpyAsync(e->im[0] + p0, si, nb, cudaMemcpyHostToDevice, e->stream));
+    if (im3) {
+      int4* si = reinterpret_cast<int4*>(stage_alloc(e, nb));
+      for (int i = 0; i < h.n; ++i) si[i] = make_int4(im3[3 * i], im3[3 * i + 1], im3[3 * i + 2], 0);
+      CK(cudaMemcpyAsync(e->im[0] + p0, si, nb, cudaMemcpyHostToDevice, e->stream));
+    } else {
+      CK(cudaMemsetAsync(e->im[0] + p0, 0, nb, e->stream));
+    }
     CK(cudaMemcpyAsync(e->last_r + p0, e->r[0] + p0, nb, cudaMemcpyDeviceToDevice, e->stream));
     k_iota<<<(h.n + 255) / 256, 256, 0, e->stream>>>(e->uidx[0] + p0, h.n);
     check_launch();
@@ -1434,17 +1773,19 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
     CK(cudaMemsetAsync(e->w + p0, 0, h.np * sizeof(float4), e->stream));
     CK(cudaMemsetAsync(e->sts + p0, 0, h.np * sizeof(float4), e->stream));
     CK(cudaMemsetAsync(e->nn + p0, 0, h.np * sizeof(unsigned), e->stream));
-    RepState s;
-    std::memset(&s, 0, sizeof(s));
-    s.xi = d->xi;
-    s.T = d->target_T;
-    s.dT = d->dT_per_step;
-    s.rebuild = 1;
-    CK(cudaMemcpyAsync(e->st + id, &s, sizeof(RepState), cudaMemcpyHostToDevice, e->stream));
+    RepState* s = reinterpret_cast<RepState*>(stage_alloc(e, sizeof(RepState)));
+    std::memset(s, 0, sizeof(RepState));
+    s->xi = d->xi;
+    s->T = d->target_T;
+    s->dT = d->dT_per_step;
+    s->rebuild = 1;
+    CK(cudaMemcpyAsync(e->st + id, s, sizeof(RepState), cudaMemcpyHostToDevice, e->stream));
+    stage_commit(e);
     e->reps[id] = h;
-    relayout(e);
-    launch_momentum(e);
-    CK(cudaStreamSynchronize(e->stream));
+    // tiles, the replica table and the momentum follow before the next launch
+    e->layout_dirty = true;
+    e->momentum_due.push_back(id);
+    if (direct) CK(cudaStreamSynchronize(e->stream));
     *id_out = id;
   });
 }
@@ -1452,16 +1793,40 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
 int b2md_replica_remove(b2md_engine* e, int id) {
   return guarded([&] {
     HostRep& h = get_rep(e, id);
-    CK(cudaSetDevice(e->device));
-    CK(cudaStreamSynchronize(e->stream));
+    // The ranges go back to the pools at once: whatever is queued on the
+    // stream (a running chunk) still finishes with them before any later
+    // admission's copies, which are queued behind it, overwrite them.
     e->palloc.release(h.p0, h.np);
     e->ealloc.release(h.nbl0, h.nbl_len);
     e->calloc.release(h.cell0, h.ncell);
     e->qalloc.release(h.par0, h.npar);
+    if (h.par1 >= 0) e->qalloc.release(h.par1, h.npar1);
     if (h.elog0 >= 0) e->zalloc.release(h.elog0, h.ecap);
     h = HostRep();
-    relayout(e);
+    e->layout_dirty = true;  // the tile layout without it is uploaded before the next launch
   });
+}
+
+int b2md_replica_footprint(b2md_engine* e, const b2md_replica_desc* d, long long* bytes) {
+  if (!e || !d || !bytes) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    HostRep h = describe(d);
+    const int ncell = h.d.nc[0] * h.d.nc[1] * h.d.nc[2];
+    h.ncell = ncell;
+    h.d.max_nbrs = list_capacity(h, d);
+    h.ecap = (d->energy_interval > 0 && d->energy_capacity > 0) ? d->energy_capacity : 0;
+    *bytes = replica_bytes(e, h);
+  });
+}
+
+int b2md_engine_usage(b2md_engine* e, long long* used, long long* reserved) {
+  if (!e || !used || !reserved) return fail(B2MD_ERR_ARG, "null argument");
+  long long u = 0;
+  for (const auto& h : e->reps)
+    if (h.active) u += h.bytes;
+  *used = u;
+  *reserved = e->bytes;
+  return B2MD_OK;
 }
 
 int b2md_replica_get(b2md_engine* e, int id, int field, void* out) {
@@ -1588,6 +1953,32 @@ int b2md_replica_set_potential(b2md_engine* e, int id, int ntypes, const float* 
     place_params(e, h);
     int want = estimate_max_nbrs(h);
     if (want > h.d.max_nbrs) place_list(e, h, want);
+    h.bytes = replica_bytes(e, h);
+    upload_rep(e, id);
+    WRITE_STATE(e, id, rebuild, 1);
+    invalidate_graphs(e);
+  });
+}
+
+int b2md_replica_add_potential(b2md_engine* e, int id, int ntypes, const float* params, int cutoff_method,
+                               int potential) {
+  if (!params) return fail(B2MD_ERR_ARG, "params is null");
+  return guarded([&] {
+    HostRep& h = get_rep(e, id);
+    CK(cudaSetDevice(e->device));
+    CK(cudaStreamSynchronize(e->stream));
+    if (ntypes != h.d.ntypes) api_fail(B2MD_ERR_ARG, "the added potential must have the replica's number of types");
+    if (h.potential1 >= 0) api_fail(B2MD_ERR_ARG, "a replica holds at most two potentials");
+    check_potential(ntypes, params, cutoff_method, potential);
+    h.params1.assign(params, params + ntypes * ntypes * kNumParam);
+    h.potential1 = potential;
+    h.cutoff1 = cutoff_method;
+    derive_grid(h);  // the list reaches the larger cut-off
+    place_cells(e, h);
+    place_params(e, h);
+    int want = estimate_max_nbrs(h);
+    if (want > h.d.max_nbrs) place_list(e, h, want);
+    h.bytes = replica_bytes(e, h);
     upload_rep(e, id);
     WRITE_STATE(e, id, rebuild, 1);
     invalidate_graphs(e);
@@ -1637,8 +2028,7 @@ int b2md_replica_set_nb_method(b2md_engine* e, int id, int method) {
     CK(cudaSetDevice(e->device));
     CK(cudaStreamSynchronize(e->stream));
     h.nb_method_req = method;
-    std::vector<float> params = h.params;
-    set_potential(h, h.d.ntypes, params.data(), h.d.cutoff, h.skin, h.d.potential);
+    derive_grid(h);
     upload_rep(e, id);
     WRITE_STATE(e, id, rebuild, 1);
     invalidate_graphs(e);
@@ -1650,6 +2040,7 @@ int b2md_replica_stats(b2md_engine* e, int id, double* out) {
   return guarded([&] {
     HostRep& h = get_rep(e, id);
     CK(cudaSetDevice(e->device));
+    ensure_layout(e);
     RepState s = read_state(e, id);
     out[B2MD_STAT_PE] = s.pe;
     out[B2MD_STAT_VIRIAL] = s.vir;
@@ -1776,6 +2167,7 @@ int b2md_integrate(b2md_engine* e) {
   if (!e) return fail(B2MD_ERR_ARG, "null engine");
   return guarded([&] {
     CK(cudaSetDevice(e->device));
+    ensure_layout(e);
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
     k_integrate<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
@@ -1787,11 +2179,12 @@ int b2md_zero_momentum(b2md_engine* e) {
   if (!e) return fail(B2MD_ERR_ARG, "null engine");
   return guarded([&] {
     CK(cudaSetDevice(e->device));
+    ensure_layout(e);
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
-    k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
+    k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp, 0);
     k_apply_zero_momentum<<<e->ntiles, e->pb, 0, e->stream>>>(a);
-    k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp);
+    k_momentum<<<e->ntiles, e->pb * e->tp, 0, e->stream>>>(a, e->tp, 0);
     check_launch();
   });
 }
@@ -1801,6 +2194,7 @@ int b2md_run(b2md_engine* e, long long nsteps) {
   if (nsteps < 0) return fail(B2MD_ERR_ARG, "nsteps must be >= 0");
   return guarded([&] {
     CK(cudaSetDevice(e->device));
+    ensure_layout(e);
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
     int R = (int)e->reps.size();
@@ -1822,6 +2216,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     CK(cudaSetDevice(e->device));
     *step_kernel_ms = 0.0;
     *launches = 0;
+    ensure_layout(e);
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
     int R = (int)e->reps.size();
@@ -1975,8 +2370,9 @@ int b2md_replica_queue_steps(b2md_engine* e, int id, long long nsteps) {
   return guarded([&] {
     get_rep(e, id);
     CK(cudaSetDevice(e->device));
-    RepState s = read_state(e, id);
-    WRITE_STATE(e, id, steps_left, s.steps_left + nsteps);
+    // in stream order: after the work already queued, before the next launch
+    k_queue_steps<<<1, 1, 0, e->stream>>>(e->st + id, nsteps);
+    check_launch();
   });
 }
 
@@ -1984,9 +2380,108 @@ int b2md_run_queued(b2md_engine* e, long long max_steps, long long* steps_run) {
   if (!e) return fail(B2MD_ERR_ARG, "null engine");
   return guarded([&] {
     CK(cudaSetDevice(e->device));
+    ensure_layout(e);
     long long lim = max_steps > 0 ? max_steps : (1LL << 62);
     long long n = e->ntiles ? run_steps(e, lim) : 0;
     if (steps_run) *steps_run = n;
+  });
+}
+
+int b2md_run_queued_async(b2md_engine* e, long long max_steps, long long* ticket) {
+  if (!e || !ticket) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    ChunkRec& c = e->chunk[(e->chunk_seq + 1) & 1];
+    if (c.ticket && !c.waited) finish_chunk(e, c);  // a third chunk waits for the oldest
+    if (!c.done) {
+      CK(cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+      CK(cudaMallocHost(&c.h_in, sizeof(int)));
+      CK(cudaMallocHost(&c.h_ctl, sizeof(PersistCtl)));
+    }
+    ensure_layout(e);
+    const int R = (int)e->reps.size();
+    if (R > c.st_cap) {
+      if (c.h_st) CK(cudaFreeHost(c.h_st));  // its last copy completed (the chunk was waited)
+      c.h_st = nullptr;
+      c.st_cap = 0;
+      CK(cudaMallocHost(&c.h_st, (size_t)std::max(R, e->rcap) * sizeof(RepState)));
+      c.st_cap = std::max(R, e->rcap);
+    }
+    c.active.assign(R, 0);
+    for (int r = 0; r < R; ++r) c.active[r] = e->reps[r].active ? 1 : 0;
+    c.persistent = false;
+    c.budget = 0;
+    c.ran = 0;
+    if (e->ntiles > 0) {
+      ensure_graphs(e);
+      const long long lim = max_steps > 0 ? std::min<long long>(max_steps, 1 << 30) : (1 << 30);
+      if (e->persist_on) {
+        // the persistent graph runs until the budget is spent, no replica
+        // has steps left or a list overflows; it leaves the unspent budget
+        c.persistent = true;
+        c.budget = lim;
+        *c.h_in = (int)lim;
+        CK(cudaMemcpyAsync(&e->pctl->budget, c.h_in, sizeof(int), cudaMemcpyHostToDevice, e->stream));
+        CK(cudaGraphLaunch(e->gexec[2], e->stream));
+      } else {
+        // per-step graphs: the queue lengths decide how many (read first)
+        const long long todo = std::min(max_steps_left(e), lim);
+        for (long long k = 0; k < todo / kChunk; ++k) CK(cudaGraphLaunch(e->gexec[1], e->stream));
+        for (long long k = 0; k < todo % kChunk; ++k) CK(cudaGraphLaunch(e->gexec[0], e->stream));
+        c.budget = todo;
+      }
+    }
+    CK(cudaMemcpyAsync(c.h_ctl, e->pctl, sizeof(PersistCtl), cudaMemcpyDeviceToHost, e->stream));
+    if (R > 0) CK(cudaMemcpyAsync(c.h_st, e->st, (size_t)R * sizeof(RepState), cudaMemcpyDeviceToHost, e->stream));
+    CK(cudaEventRecord(c.done, e->stream));
+    c.ticket = ++e->chunk_seq;
+    c.waited = false;
+    *ticket = c.ticket;
+  });
+}
+
+int b2md_run_queued_poll(b2md_engine* e, long long ticket, int* done) {
+  if (!e || !done) return fail(B2MD_ERR_ARG, "null argument");
+  return guarded([&] {
+    ChunkRec* c = find_chunk(e, ticket);
+    if (c->waited) {
+      *done = 1;
+      return;
+    }
+    CK(cudaSetDevice(e->device));
+    const cudaError_t q = cudaEventQuery(c->done);
+    if (q != cudaSuccess && q != cudaErrorNotReady) throw CudaErr{q, "cudaEventQuery(chunk)", __LINE__};
+    *done = q == cudaSuccess;
+  });
+}
+
+int b2md_run_queued_wait(b2md_engine* e, long long ticket, long long* steps_run, double* states, int cap) {
+  if (!e) return fail(B2MD_ERR_ARG, "null argument");
+  if (cap < 0 || (cap > 0 && !states)) return fail(B2MD_ERR_ARG, "states must hold cap rows");
+  return guarded([&] {
+    CK(cudaSetDevice(e->device));
+    ChunkRec* c = find_chunk(e, ticket);
+    if (!c->waited) finish_chunk(e, *c);
+    if (steps_run) *steps_run = c->ran;
+    const int R = (int)c->active.size();
+    for (int r = 0; r < cap; ++r) {
+      double* o = states + (size_t)r * B2MD_CHUNK_FIELDS;
+      for (int k = 0; k < B2MD_CHUNK_FIELDS; ++k) o[k] = 0.0;
+      if (r >= R || !c->active[r]) {
+        o[B2MD_CHUNK_STEPS_LEFT] = -1.0;
+        continue;
+      }
+      const RepState& s = c->h_st[r];
+      o[B2MD_CHUNK_ACTIVE] = 1.0;
+      o[B2MD_CHUNK_STEPS] = (double)s.steps;
+      o[B2MD_CHUNK_STEPS_LEFT] = (double)s.steps_left;
+      o[B2MD_CHUNK_PE] = s.pe;
+      o[B2MD_CHUNK_VIRIAL] = s.vir;
+      o[B2MD_CHUNK_KE] = s.ke_t;
+      o[B2MD_CHUNK_XI] = s.xi;
+      o[B2MD_CHUNK_REBUILDS] = s.nrebuilds;
+      o[B2MD_CHUNK_OVERFLOW] = s.overflow;
+    }
   });
 }
 

@@ -83,6 +83,10 @@ struct RepDev {
   double dof;
   int active;
   int potential;  // POT_*
+  // Sample::AddPotential: a second pair function evaluated over the same list
+  // (built with the larger cut-off of the two), its sums added to the
+  // first's; npot = 1 or 2
+  int npot, par1, potential1;
 };
 
 struct RepState {
@@ -111,6 +115,11 @@ struct PersistCtl {
   unsigned readers; // k_batch: blocks that have read the step's rebuild list
   int fcnt[2];      // k_batch: replicas on the rebuild list of steps of each parity
   int ftiles[2];    // k_batch: their tiles
+  // the tile layout in effect (written by the host with every re-layout, in
+  // stream order): graphs of k_batch read these instead of capturing them,
+  // so admissions and removals need no new graph
+  int lay_ntiles;
+  int lay_nrep;
 };
 
 struct EngArgs {

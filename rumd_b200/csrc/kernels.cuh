@@ -979,6 +979,41 @@ __device__ __forceinline__ bool force_tile(const EngArgs& a, int tile, unsigned 
         }
       }
     }
+    if constexpr (!PERSIST && !COH) {
+      if (R.npot > 1) {
+        // Sample::CalcF's potential loop (Sample.cu:335-336): the second
+        // pair function's per-particle sums, over the same list (read from
+        // global memory in every force mode), are added to the first's once
+        // both are complete -- the store-then-accumulate of
+        // PairPotential.cu:370-388
+        PairAcc B;
+        const float* prow1 = a.par + R.par1 + ti * nt * kParStride;
+        force_loop_any<TP, STRESS, false>(fast, R.potential1, nt, B, IdxStreamed{lbase, (unsigned)i, lstride},
+                                          PosGlobal{rc}, lane_t, nn, ri, prow1, Lx, Ly, Lz, iLx, iLy, iLz);
+        if (TP > 1) {
+#pragma unroll
+          for (int o = TP / 2; o > 0; o >>= 1) {
+            B.fx += __shfl_xor_sync(0xffffffffu, B.fx, o);
+            B.fy += __shfl_xor_sync(0xffffffffu, B.fy, o);
+            B.fz += __shfl_xor_sync(0xffffffffu, B.fz, o);
+            B.uu += __shfl_xor_sync(0xffffffffu, B.uu, o);
+            B.ww += __shfl_xor_sync(0xffffffffu, B.ww, o);
+            if (STRESS) {
+              B.sxx += __shfl_xor_sync(0xffffffffu, B.sxx, o);
+              B.syy += __shfl_xor_sync(0xffffffffu, B.syy, o);
+              B.szz += __shfl_xor_sync(0xffffffffu, B.szz, o);
+              B.syz += __shfl_xor_sync(0xffffffffu, B.syz, o);
+              B.sxz += __shfl_xor_sync(0xffffffffu, B.sxz, o);
+              B.sxy += __shfl_xor_sync(0xffffffffu, B.sxy, o);
+            }
+          }
+        }
+        fx += B.fx; fy += B.fy; fz += B.fz; uu += B.uu; ww += B.ww;
+        if (STRESS) {
+          sxx += B.sxx; syy += B.syy; szz += B.szz; syz += B.syz; sxz += B.sxz; sxy += B.sxy;
+        }
+      }
+    }
     if constexpr (PERSIST && FUSED) {
       // the block's first warp past its neighbour loop waits (bounded) for
       // the previous step's finalizer, which stores the step count last, with
@@ -1321,7 +1356,8 @@ __global__ void k_gate_loop(EngArgs a, cudaGraphConditionalHandle h_loop) {
   __shared__ int s_any;
   if (threadIdx.x == 0) s_any = 0;
   __syncthreads();
-  for (int r = threadIdx.x; r < a.nrep; r += blockDim.x)
+  const int nrep = __ldcg(&a.pctl->lay_nrep);  // the layout in effect (not the captured one)
+  for (int r = threadIdx.x; r < nrep; r += blockDim.x)
     if (a.rep[r].active && !a.st[r].overflow && a.st[r].steps_left > 0) s_any = 1;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1372,11 +1408,12 @@ __global__ void __launch_bounds__(kMaxBlock) k_integrate(EngArgs a, int tp) {
 
 // Total momentum and mass of the current velocities (calculateMomentum +
 // sumIdenticalArrays, IntegratorNVT.cu:176-183, 462-471), FP64.
-__global__ void __launch_bounds__(kMaxBlock) k_momentum(EngArgs a, int tp) {
+// Tiles tile0 .. tile0 + gridDim.x - 1 (all tiles, or one replica's).
+__global__ void __launch_bounds__(kMaxBlock) k_momentum(EngArgs a, int tp, int tile0) {
   __shared__ double s_warp[(kMaxBlock / 32) * kNPart];
   __shared__ double s_scr[kMaxBlock];
   __shared__ double s_blk[kNPart], s_tot[kNPart];
-  const int tile = blockIdx.x;
+  const int tile = tile0 + blockIdx.x;
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
   RepState* S = a.st + rep;
@@ -1427,6 +1464,10 @@ __global__ void k_set_steps(EngArgs a, long long nsteps, int reset_run_step) {
   a.st[rep].steps_left = nsteps;
   if (reset_run_step) a.st[rep].run_step = 0;
 }
+
+// Adds queued steps to one replica (in stream order, after the work queued
+// before it).
+__global__ void k_queue_steps(RepState* s, long long nsteps) { s->steps_left += nsteps; }
 
 // Gate: publishes "any replica flagged for rebuild" to the first conditional node.
 __global__ void k_gate(EngArgs a, cudaGraphConditionalHandle h) {
@@ -2869,10 +2910,13 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
   // step barrier words' totals, the step's rebuild-list size and its tiles
   __shared__ unsigned s_gen, s_base;
   __shared__ int s_budget, s_nf, s_t2;
+  __shared__ int s_ntiles, s_nrep;  // the layout in effect (not the captured one)
   __shared__ unsigned long long s_seen[2];
   BatchShared* bs = reinterpret_cast<BatchShared*>(s_dyn + a.bshared_off);
   PersistCtl* c = a.pctl;
   if (threadIdx.x == 0) {
+    s_ntiles = __ldcg(&c->lay_ntiles);
+    s_nrep = __ldcg(&c->lay_nrep);
     s_go = __ldcg(&c->err) == 0;
     if (!s_go && blockIdx.x == 0) set_loop(h_loop, 0u);
   }
@@ -2897,7 +2941,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
         *a.any_rebuild = 0;
       }
       __syncthreads();
-      for (int r = threadIdx.x; r < a.nrep; r += blockDim.x) {
+      for (int r = threadIdx.x; r < s_nrep; r += blockDim.x) {
         const RepState* S = a.st + r;
         if (a.rep[r].active && S->rebuild && !S->overflow && S->steps_left > 0) {
           const int pos = atomicAdd(&c->fcnt[0], 1);
@@ -2968,11 +3012,11 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - s_base);
       __syncthreads();
       const unsigned it = (unsigned)s_item;
-      const int t2 = s_t2, nf = s_nf;
-      const int q = batch_first_tiles(a.ntiles, t2);
-      if (it >= (unsigned)(nf + a.ntiles + 2 * t2)) break;
+      const int t2 = s_t2, nf = s_nf, ntiles = s_ntiles;
+      const int q = batch_first_tiles(ntiles, t2);
+      if (it >= (unsigned)(nf + ntiles + 2 * t2)) break;
       const bool tile_item = it >= (unsigned)nf && (it < (unsigned)(nf + q) || (it >= (unsigned)(nf + q + t2) &&
-                                                                             it < (unsigned)(nf + a.ntiles + t2)));
+                                                                             it < (unsigned)(nf + ntiles + t2)));
       if (it < (unsigned)nf) {
         block_sort(a, bs->list[it], s_gen * kBatchEpochSteps + (unsigned)step + 1u, bs->scan);
       } else if (tile_item) {
@@ -2983,7 +3027,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
                                                                 0, nullptr, nullptr, nullptr, par ^ 1);
       } else {
         const bool build = it < (unsigned)(nf + q + t2);
-        const int k = build ? (int)it - nf - q : (int)it - nf - a.ntiles - t2;
+        const int k = build ? (int)it - nf - q : (int)it - nf - ntiles - t2;
         int lo = 0, hi = nf - 1;  // the listed replica holding flagged tile k
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
@@ -3019,7 +3063,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     }
     // step barrier: arrival + "steps left" and overflow tallies
     if (threadIdx.x == 0) {
-      s_base += (unsigned)(s_nf + a.ntiles + 2 * s_t2) + gridDim.x;
+      s_base += (unsigned)(s_nf + s_ntiles + 2 * s_t2) + gridDim.x;
       const int budget = --s_budget;
       const unsigned long long mine = 1ull + s_step_tally;
       const unsigned long long now = atom_add_acq_rel_u64(&c->word[par], mine) + mine;
@@ -3047,8 +3091,8 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       const unsigned stop = (unsigned)((d >> kTallyRebuildShift) & kTallyField);
       // steps per launch: the epochs' and the tally fields' range, and the
       // 32-bit ticket counter (at most nrep + 3 ntiles + grid tickets a step)
-      const unsigned per_step = (unsigned)a.nrep + 3u * (unsigned)a.ntiles + gridDim.x;
-      const int cap = min(min(kBatchEpochSteps - 2, (int)(kTallyField / (unsigned)(a.nrep + 1))),
+      const unsigned per_step = (unsigned)s_nrep + 3u * (unsigned)s_ntiles + gridDim.x;
+      const int cap = min(min(kBatchEpochSteps - 2, (int)(kTallyField / (unsigned)(s_nrep + 1))),
                           (int)min(0x7fffffffu, 0xffffffffu / per_step));
       const int go = ok && stop == 0 && more > 0 && budget > 0 && step + 1 < cap;
       if (last && !go) {

@@ -147,6 +147,7 @@ PYBIND11_MODULE(_rumd, m) {
            py::arg("velocities") = py::none(), py::arg("images") = py::none())
       .def("SetPotential", &Sample::SetPotential, py::keep_alive<1, 2>())
       .def("AddPotential", &Sample::AddPotential, py::keep_alive<1, 2>())
+      .def("GetPotentials", &Sample::GetPotentials, py::return_value_policy::reference)
       .def("SetIntegrator", &Sample::SetIntegrator, py::keep_alive<1, 2>())
       .def("GetIntegrator", &Sample::GetIntegrator, py::return_value_policy::reference)
       .def("CalcF", &Sample::CalcF, py::arg("calc_stresses") = false)

@@ -462,19 +462,44 @@ void Sample::SetMass(unsigned t, float m) {
   if (HasReplica()) Check(b2md_replica_set(eng, rid, B2MD_FIELD_VEL, v.data()), "SetMass");
 }
 
+// Sample::SetPotential (Sample.cu:251-259): the potential list becomes this
+// one potential.
 void Sample::SetPotential(Potential* p) {
   auto* pp = dynamic_cast<PairPotential*>(p);
   if (!pp) throw RUMD_Error("Sample", "SetPotential", "only Lennard-Jones pair potentials are supported");
   if (pot && pot != pp) pot->SetSample(nullptr);
+  if (pot2 && pot2 != pp) pot2->SetSample(nullptr);
+  pot2 = nullptr;
   pot = pp;
   pot->SetSample(this);
   PotentialChanged();
 }
 
+// Sample::AddPotential (Sample.cu:261-278): one more potential in the list
+// that CalcF evaluates, the first storing forces, energies, virials and
+// stresses and the other adding to them (Sample.cu:335-336,
+// PairPotential.cu:370-388).  The engine holds two pair potentials per
+// sample, over one neighbour list built with the larger cut-off and the
+// first potential's skin.
 void Sample::AddPotential(Potential* p) {
-  if (pot && pot != p)
-    throw RUMD_Error("Sample", "AddPotential", "one pair potential per sample is supported; use SetPotential");
-  SetPotential(p);
+  auto* pp = dynamic_cast<PairPotential*>(p);
+  if (!pp) throw RUMD_Error("Sample", "AddPotential", "only Lennard-Jones pair potentials are supported");
+  if (!pot) {
+    SetPotential(p);
+    return;
+  }
+  if (pp == pot || pp == pot2) throw RUMD_Error("Sample", "AddPotential", "this potential is already in the list");
+  if (pot2) throw RUMD_Error("Sample", "AddPotential", "at most two pair potentials per sample are supported");
+  pot2 = pp;
+  pot2->SetSample(this);
+  PotentialChanged();
+}
+
+std::vector<PairPotential*> Sample::GetPotentials() const {
+  std::vector<PairPotential*> out;
+  if (pot) out.push_back(pot);
+  if (pot2) out.push_back(pot2);
+  return out;
 }
 
 void Sample::SetIntegrator(Integrator* i) {
@@ -518,6 +543,12 @@ void Sample::EnsureReplica() {
   d.max_nbrs = (int)pot->GetNeighborList().GetMaxNumNbrs();
   d.potential = pot->PotentialKind();
   Check(b2md_replica_add(eng, &d, pos.data(), vel.data(), im.data(), &rid), "SetNumberOfParticles");
+  if (pot2) {
+    std::vector<float> t2 = pot2->ParamTable(GetNumberOfTypes());
+    Check(b2md_replica_add_potential(eng, rid, (int)GetNumberOfTypes(), t2.data(), pot2->GetCutoffMethod(),
+                                     pot2->PotentialKind()),
+          "AddPotential");
+  }
   int m = pot->GetNeighborList().MethodCode();
   if (m != -1) Check(b2md_replica_set_nb_method(eng, rid, m), "SetNB_Method");
   if (elog_interval > 0) Check(b2md_replica_set_energy_log(eng, rid, elog_interval, elog_capacity), "SetEnergyLog");
@@ -544,6 +575,12 @@ void Sample::PotentialChanged() {
   Check(b2md_replica_set_potential(eng, rid, (int)GetNumberOfTypes(), table.data(), pot->GetCutoffMethod(),
                                    pot->GetNbListSkin(), pot->PotentialKind()),
         "SetPotential");
+  if (pot2) {
+    std::vector<float> t2 = pot2->ParamTable(GetNumberOfTypes());
+    Check(b2md_replica_add_potential(eng, rid, (int)GetNumberOfTypes(), t2.data(), pot2->GetCutoffMethod(),
+                                     pot2->PotentialKind()),
+          "AddPotential");
+  }
 }
 
 void Sample::IntegratorChanged() {

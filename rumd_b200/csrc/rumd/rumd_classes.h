@@ -247,6 +247,8 @@ class Sample {
   void SetIntegrator(Integrator* itg);
   Integrator* GetIntegrator() const { return itg; }
   PairPotential* GetPairPotential() const { return pot; }
+  // the potentials CalcF evaluates (one or two)
+  std::vector<PairPotential*> GetPotentials() const;
 
   void CalcF(bool calc_stresses = false);
   // Simulation.Run's time-step loop as fused device graphs (momentum reset
@@ -306,6 +308,7 @@ class Sample {
   std::vector<float> pos, vel, box, mass;  // host copies until the replica exists
   std::vector<int> type, im;
   PairPotential* pot = nullptr;
+  PairPotential* pot2 = nullptr;  // a second potential (AddPotential)
   Integrator* itg = nullptr;
   bool include_kinetic_stress = false;
   bool verbose = true;

@@ -76,10 +76,13 @@ class Simulation:
         self.sample.SetPotential(potential)
 
     def AddPotential(self, potential, clear=False):
+        """Simulation.AddPotential (Simulation.py:178-196): appends to the list that
+        CalcF evaluates (two pair potentials at most)."""
         if clear or not self.potentialList:
             self.SetPotential(potential)
         else:
             self.sample.AddPotential(potential)
+            self.potentialList.append(potential)
 
     def SetIntegrator(self, itg):
         self.sample.SetIntegrator(itg)

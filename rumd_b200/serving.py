@@ -2,28 +2,43 @@
 
 Jobs (independent MD systems of any size and step count) arrive over time.
 The server keeps every admitted job's state resident in HBM as a replica of
-one engine, admits queued jobs as soon as the memory budget allows, and
-advances all resident jobs together: each round is one `run_queued` call of
-`chunk_steps` steps in which every replica advances by up to that many of its
-own remaining steps.  Jobs that finish leave between rounds, which frees
-their slot and memory for the next queued jobs.  Because a replica's
-arithmetic does not depend on which other replicas share the launches, every
-job's result is the same alone and in the mix.
+one engine and advances all resident jobs together in chunks: each chunk is
+one `run_queued_async` launch in which every replica advances by up to the
+chunk's step count of its own remaining steps.  Two chunks are kept in
+flight, so the GPU never waits for the host:
+
+  * arrivals: a job's initial configuration is built on a worker thread as
+    soon as it arrives (the stand-in for a client uploading it), off the
+    serving loop;
+  * admission, FIFO: the head of the queue is admitted when its configuration
+    is ready and the engine's reported memory (`usage`) plus the job's
+    `footprint` fits the HBM budget.  `add` only queues the upload behind the
+    running chunks and returns; the job joins the next chunk launched;
+  * completion: each chunk leaves a snapshot of every replica's state in
+    pinned host memory; when the oldest chunk finishes the server reads it,
+    retires the jobs it shows finished (results from the snapshot) and
+    removes them, which returns their memory at once, and launches the next
+    chunk.
+
+Because a replica's arithmetic does not depend on which other replicas share
+the launches, every job's result is the same alone and in the mix.
 
 `MDServer` takes the engine as an argument, so the scheduling logic runs
 unchanged against a fake engine in the CPU tests.
 """
 import time
+from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
 
 from . import initconf
 
-# Device bytes per particle held by an engine replica: positions/velocities/
-# images/ids double-buffered, forces, virials, stresses, last-build positions,
-# list length, sort scratch.
-BYTES_PER_PARTICLE = 2 * (16 + 16 + 16 + 4) + 16 * 4 + 4 * 4
+DENSITY = {"KA": 1.2, "LJ": 0.8442}
+# snapshot columns (capi.CHUNK_FIELDS)
+SNAP = {k: i for i, k in enumerate(["active", "steps", "steps_left", "pe", "virial", "ke", "xi", "rebuilds",
+                                     "overflow"])}
 
 
 @dataclass
@@ -44,15 +59,6 @@ class Job:
         return self.done - self.arrival
 
 
-def job_bytes(job, skin=0.3):
-    """HBM needed by a job: particle arrays + neighbour list + cell arrays."""
-    density = 1.2 if job.kind == "KA" else 0.8442
-    rc = 2.5
-    max_nbrs = int(np.ceil(1.5 * 4.0 / 3.0 * np.pi * (rc + skin) ** 3 * density)) + 1
-    cells = (job.n / density) / ((rc + skin) / 2) ** 3
-    return int(job.n * (BYTES_PER_PARTICLE + 4 * max_nbrs) + 8 * cells + 4096)
-
-
 def poisson_stream(njobs, rate=50.0, seed=0, n_range=(256, 32768), steps_range=(1000, 100000),
                    T_range=(0.5, 2.0)):
     """Seeded job stream: Poisson arrivals at `rate` jobs/s, KA or LJ 50/50,
@@ -67,78 +73,176 @@ def poisson_stream(njobs, rate=50.0, seed=0, n_range=(256, 32768), steps_range=(
                 seed=seed * 100003 + k) for k in range(njobs)]
 
 
+def job_params(job):
+    if job.kind == "KA":
+        return initconf.lj_params(2, initconf.KA), 2
+    return initconf.lj_params(1, initconf.LJ), 1
+
+
 def job_config(job):
     """Initial configuration and parameter table of a job."""
+    params, ntypes = job_params(job)
     if job.kind == "KA":
-        c = initconf.ka_config(job.n, T=job.T, seed=job.seed)
-        return c, initconf.lj_params(2, initconf.KA), 2
-    c = initconf.lj_config(job.n, T=job.T, seed=job.seed)
-    return c, initconf.lj_params(1, initconf.LJ), 1
+        return initconf.ka_config(job.n, T=job.T, seed=job.seed), params, ntypes
+    return initconf.lj_config(job.n, T=job.T, seed=job.seed), params, ntypes
+
+
+def job_box(job):
+    """The job's cubic box (the configuration's density)."""
+    L = (job.n / DENSITY[job.kind]) ** (1.0 / 3.0)
+    return np.array([L, L, L], np.float32)
+
+
+class _Ready:
+    """A finished result in the shape of a Future (configurations built inline)."""
+
+    def __init__(self, value):
+        self.value = value
+
+    def done(self):
+        return True
+
+    def result(self):
+        return self.value
+
+
+@dataclass
+class _Resident:
+    job: Job
+    left: int                  # steps left, from the latest snapshot that includes the job
+    first_ticket: int = 0      # the first chunk launched after the admission (0: none yet)
 
 
 class MDServer:
-    def __init__(self, engine, hbm_budget=150e9, chunk_steps=200, dt=0.005, skin=0.3, tau=0.2,
-                 clock=time.perf_counter, sleep=time.sleep):
+    """chunk_steps: steps per chunk, or "auto": about `chunk_seconds` of GPU
+    time at `rate_hint` particle-steps/s over the resident particles (between
+    min_chunk_steps and max_chunk_steps).  workers: threads that build
+    arriving jobs' configurations (0: inline).  max_resident: replicas at
+    once (the batched kernel's limit)."""
+
+    def __init__(self, engine, hbm_budget=150e9, chunk_steps="auto", dt=0.005, skin=0.3, tau=0.2,
+                 clock=time.perf_counter, sleep=time.sleep, workers=2, max_resident=1024, chunk_seconds=0.05,
+                 rate_hint=1.5e9, min_chunk_steps=16, max_chunk_steps=2000, poll_seconds=2e-4, in_flight=2):
         self.engine = engine
         self.budget = float(hbm_budget)
-        self.chunk = int(chunk_steps)
+        self.chunk = chunk_steps
         self.dt, self.skin, self.tau = dt, skin, tau
         self.clock, self.sleep = clock, sleep
-        self.used = 0
+        self.workers = int(workers)
+        self.max_resident = int(max_resident)
+        self.chunk_seconds, self.rate_hint = chunk_seconds, rate_hint
+        self.min_chunk, self.max_chunk = int(min_chunk_steps), int(max_chunk_steps)
+        self.poll_seconds = poll_seconds
+        self.in_flight = int(in_flight)
         self.max_used = 0
-        self.running = {}     # replica id -> (job, remaining steps)
-        self.queue_depth = []
+        self.running = {}      # replica id -> _Resident
+        self.timeline = []     # after each chunk: (t, jobs waiting, jobs resident, backlog particle-steps)
+        self.chunks = 0
 
-    def admit(self, job, now):
-        c, params, ntypes = job_config(job)
+    # ---- memory ----
+    @property
+    def used(self):
+        return self.engine.usage()[0]
+
+    def job_footprint(self, job):
+        """Device bytes the engine reports for the job (box from its density)."""
+        params, ntypes = job_params(job)
+        return self.engine.footprint(job.n, job_box(job), params, ntypes, cutoff="SF", skin=self.skin)
+
+    # ---- jobs ----
+    def admit(self, job, conf, now):
+        c, params, ntypes = conf
         rid = self.engine.add(c["pos4"], c["box"], params, ntypes, cutoff="SF", skin=self.skin, dt=self.dt,
                               T=job.T, tau=self.tau, vel4=c["vel4"])
         self.engine.queue(rid, job.steps)
-        self.used += job_bytes(job, self.skin)
-        self.max_used = max(self.max_used, self.used)
         job.admitted = now
-        self.running[rid] = [job, job.steps]
+        self.running[rid] = _Resident(job, job.steps)
+        self.max_used = max(self.max_used, self.used)
 
-    def retire(self, rid, now):
-        job, _ = self.running.pop(rid)
-        st = self.engine.stats(rid)
-        job.result = {"pe": st["pe"], "ke": st["ke"], "xi": st["xi"], "steps": st["steps"],
-                      "rebuilds": st["rebuilds"]}
+    def retire(self, rid, row, now):
+        job = self.running.pop(rid).job
+        job.result = {"pe": float(row[SNAP["pe"]]), "ke": float(row[SNAP["ke"]]), "xi": float(row[SNAP["xi"]]),
+                      "steps": int(row[SNAP["steps"]]), "rebuilds": int(row[SNAP["rebuilds"]])}
         job.done = now
         self.engine.remove(rid)
-        self.used -= job_bytes(job, self.skin)
+
+    def chunk_length(self):
+        if self.chunk != "auto":
+            return int(self.chunk)
+        parts = sum(r.job.n for r in self.running.values() if r.left > 0)
+        k = int(self.chunk_seconds * self.rate_hint / max(parts, 1))
+        return max(self.min_chunk, min(self.max_chunk, k))
+
+    def _after_chunk(self, ticket, snap, now, waiting):
+        for rid, r in list(self.running.items()):
+            if r.first_ticket == 0 or ticket < r.first_ticket:
+                continue  # admitted after this chunk was launched
+            row = snap[rid]
+            r.left = int(row[SNAP["steps_left"]])
+            if r.left <= 0:
+                self.retire(rid, row, now)
+        backlog = sum(r.left * r.job.n for r in self.running.values()) + sum(j.n * j.steps for j in waiting)
+        self.timeline.append((now, len(waiting), len(self.running), float(backlog)))
+
+    @property
+    def queue_depth(self):
+        """Jobs waiting for admission, after each chunk."""
+        return [w for _, w, _, _ in self.timeline]
 
     def serve(self, jobs, realtime=True):
         """Runs the whole stream; returns the jobs with admitted/done times set."""
         pending = sorted(jobs, key=lambda j: j.arrival)
         for j in pending:
-            if job_bytes(j, self.skin) > self.budget:
+            if self.job_footprint(j) > self.budget:
                 raise ValueError(f"job {j.id} needs more memory than the whole budget")
+        pool = ThreadPoolExecutor(self.workers) if self.workers > 0 else None
+        confs = {}
+        waiting = deque()
+        inflight = deque()
         t0 = self.clock()
         k = 0
-        waiting = []
-        while k < len(pending) or waiting or self.running:
-            now = self.clock() - t0 if realtime else float("inf")
-            while k < len(pending) and pending[k].arrival <= now:
-                waiting.append(pending[k])
-                k += 1
-            # FIFO admission while the budget allows
-            while waiting and self.used + job_bytes(waiting[0], self.skin) <= self.budget:
-                self.admit(waiting.pop(0), self.clock() - t0)
-            self.queue_depth.append(len(waiting))
-            if not self.running:
-                if k < len(pending):
-                    self.sleep(max(0.0, pending[k].arrival - (self.clock() - t0)))
-                continue
-            ran = self.engine.run_queued(self.chunk)
-            now = self.clock() - t0
-            for rid in list(self.running):
-                self.running[rid][1] -= ran
-                if self.running[rid][1] <= 0:
-                    if self.engine.stats(rid)["steps_left"] <= 0:
-                        self.retire(rid, now)
+        try:
+            while k < len(pending) or waiting or self.running or inflight:
+                now = self.clock() - t0 if realtime else float("inf")
+                while k < len(pending) and pending[k].arrival <= now:
+                    j = pending[k]
+                    k += 1
+                    waiting.append(j)
+                    confs[j.id] = pool.submit(job_config, j) if pool else _Ready(job_config(j))
+                # FIFO admission: the head waits for its configuration and for room
+                while waiting and len(self.running) < self.max_resident and confs[waiting[0].id].done():
+                    j = waiting[0]
+                    conf = confs[j.id].result()
+                    c, params, ntypes = conf
+                    need = self.engine.footprint(len(c["pos4"]), c["box"], params, ntypes, cutoff="SF",
+                                                 skin=self.skin)
+                    if self.used + need > self.budget:
+                        break
+                    waiting.popleft()
+                    del confs[j.id]
+                    self.admit(j, conf, self.clock() - t0)
+                # keep the GPU fed: chunks in flight while any resident job has steps left
+                while len(inflight) < self.in_flight and any(r.left > 0 for r in self.running.values()):
+                    t = self.engine.run_queued_async(self.chunk_length())
+                    self.chunks += 1
+                    inflight.append(t)
+                    for r in self.running.values():
+                        if r.first_ticket == 0:
+                            r.first_ticket = t
+                if inflight:
+                    if self.engine.poll(inflight[0]):
+                        t = inflight.popleft()
+                        _, snap = self.engine.wait(t)
+                        self._after_chunk(t, snap, self.clock() - t0, waiting)
                     else:
-                        self.running[rid][1] = int(self.engine.stats(rid)["steps_left"])
+                        self.sleep(self.poll_seconds)
+                elif waiting:
+                    self.sleep(self.poll_seconds)  # the head's configuration is still being built
+                elif k < len(pending):
+                    self.sleep(max(0.0, pending[k].arrival - (self.clock() - t0)))
+        finally:
+            if pool:
+                pool.shutdown(wait=True)
         return jobs
 
 
@@ -163,6 +267,32 @@ def latency_summary(jobs):
     return {"jobs": len(jobs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
             "mean_s": float(lat.mean()), "particle_steps": ps, "makespan_s": span,
             "throughput": ps / span if span > 0 else 0.0}
+
+
+def timeline_summary(server, jobs, step_s=1.0):
+    """Load over time: per `step_s` window, the largest number of jobs waiting
+    for admission and resident, and the backlog (particle-steps still to run)
+    at the window's end; with the offered load and whether the server kept up."""
+    tl = server.timeline
+    if not tl:
+        return {}
+    end = tl[-1][0]
+    rows = []
+    i = 0
+    for w in range(int(np.ceil(end / step_s)) + 1):
+        hi = (w + 1) * step_s
+        sel = []
+        while i < len(tl) and tl[i][0] < hi:
+            sel.append(tl[i])
+            i += 1
+        if sel:
+            rows.append([round(hi, 3), max(s[1] for s in sel), max(s[2] for s in sel), sel[-1][3]])
+    arrivals = [j.arrival for j in jobs]
+    span = max(arrivals) - min(arrivals)
+    work = float(sum(j.n * j.steps for j in jobs))
+    return {"window_s": step_s, "columns": ["t_s", "max_waiting", "max_resident", "backlog_particle_steps"],
+            "rows": rows, "arrival_span_s": span, "offered_particle_steps_per_s": work / span if span > 0 else None,
+            "max_waiting": max(s[1] for s in tl), "max_resident": max(s[2] for s in tl), "chunks": server.chunks}
 
 
 def serve_one_at_a_time(engine_factory, jobs, dt=0.005, skin=0.3, tau=0.2, clock=time.perf_counter,

@@ -154,3 +154,106 @@ def test_rumd_classes_on_reference_configuration(rumd, oracle, tmp_path, cls):
                                   pot.GetCutoffMethod(), potential)
     assert rms_rel(f, ref) <= 1e-5
     assert abs(s.GetPotentialEnergy() - u.sum()) <= 1e-5 * abs(u.sum())
+
+
+# A second potential with its own, shorter cut-off (2.0 sigma): the list is
+# built with the larger one, and each pair function applies its own.
+SMOOTH2 = {(0, 0): (1.0, 0.3, 2.0), (0, 1): (0.8, 0.45, 2.0), (1, 1): (0.88, 0.15, 2.0)}
+
+
+@pytest.mark.parametrize("tp", [1, 4])
+@pytest.mark.parametrize("force_mode", [0, 1, 2])
+def test_second_potential_adds_to_the_first(capi, oracle, melt, force_mode, tp):
+    """Sample::CalcF's potential loop (Sample.cu:335-336): LJ 12-6 (SF,
+    rc 2.5 sigma) plus a smoothed LJ (SP, rc 2.0 sigma) on one sample against
+    the sum of the FP64 oracle's two pair sums, in every force mode: forces
+    rms relative 1e-5, energy and virial 1e-5 relative, the six pair-stress
+    components rms relative 1e-5."""
+    N = len(melt["pos4"])
+    lj = oracle.lj_params(2, oracle.ka_table())
+    sm = oracle.smooth_params(2, SMOOTH2)
+    e = capi.Engine(device=0, pb=64, tp=tp)
+    e.set_variant(capi.VARIANT_FORCE_MODE, force_mode)
+    rid = e.add(melt["pos4"], melt["box"], lj, 2, cutoff="SF")
+    e.add_potential(rid, 2, sm, "SP", "LJ_12_6_smooth_2_4")
+    with pytest.raises(ValueError):
+        e.add_potential(rid, 2, sm, "SP", "LJ_12_6_smooth_2_4")  # two at most
+    e.calc_f(stress=True)
+    f = e.get(rid, "force", N).astype(np.float64)
+    st = e.stats(rid)
+    sts = e.get(rid, "stress", N).astype(np.float64)
+    w = e.get(rid, "virial", N).astype(np.float64)
+    g6 = np.stack([sts[:, 0], sts[:, 1], sts[:, 2], sts[:, 3], w[:, 1], w[:, 2]], 1)
+    e.close()
+    pos = melt["pos4"][:, :3].astype(np.float64)
+    types = melt["pos4"][:, 3].view(np.int32)
+    f1, u1, w1 = oracle.forces_f64(pos, types, melt["box"], 2, lj, capi.CUTOFF["SF"], "LJ_12_6")
+    f2, u2, w2 = oracle.forces_f64(pos, types, melt["box"], 2, sm, capi.CUTOFF["SP"], "LJ_12_6_smooth_2_4")
+    assert rms_rel(f2, f1) > 0.01  # the second potential matters
+    assert rms_rel(f[:, :3], f1 + f2) <= 1e-5
+    assert np.abs(f[:, 3] - (u1 + u2)).max() < 1e-4
+    u = u1.sum() + u2.sum()
+    assert abs(st["pe"] - u) <= 1e-5 * abs(u)
+    assert abs(st["virial"] - (w1 + w2).sum() / 6) <= 1e-5 * abs((w1 + w2).sum() / 6) + 1e-3
+    o6 = (oracle.stress_f64(pos, types, melt["box"], 2, lj, capi.CUTOFF["SF"], "LJ_12_6")
+          + oracle.stress_f64(pos, types, melt["box"], 2, sm, capi.CUTOFF["SP"], "LJ_12_6_smooth_2_4"))
+    assert rms_rel(g6, o6) <= 1e-5
+
+
+def test_two_half_potentials_run_as_one(capi, oracle, melt):
+    """LJ 12-6 with epsilon/2, added twice, is LJ 12-6 with epsilon bit for
+    bit: halving epsilon halves every coefficient and every pair term exactly
+    (a power of two), both passes sum the same list in the same order, and the
+    second's sums are added to the first's.  So a 300-step NVT run with the
+    two potentials (per-step graphs) must give the one-potential run's
+    positions, energies and thermostat state exactly."""
+    N = len(melt["pos4"])
+    full = oracle.lj_params(2, oracle.ka_table())
+    half = oracle.lj_params(2, {k: (s, eps / 2, rc) for k, (s, eps, rc) in KA.items()})
+    assert np.array_equal(half[1::12] * 2, full[1::12])  # A12
+    out = []
+    for two in (False, True):
+        e = capi.Engine(device=0, pb=64, tp=4)
+        rid = e.add(melt["pos4"], melt["box"], half if two else full, 2, cutoff="SF", T=0.8, vel4=melt["vel4"])
+        if two:
+            e.add_potential(rid, 2, half, "SF")
+        e.run(300)
+        st = e.stats(rid)
+        kind = e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE)
+        out.append((e.get(rid, "pos", N), st, kind))
+        e.close()
+    (p1, s1, k1), (p2, s2, k2) = out
+    assert k2 == 0  # the replica with two potentials ran on the per-step graphs
+    assert s1["rebuilds"] == s2["rebuilds"] > 1
+    assert s1["pe"] == s2["pe"] and s1["ke"] == s2["ke"] and s1["xi"] == s2["xi"]
+    assert np.array_equal(p1, p2)
+
+
+def test_rumd_classes_add_potential(rumd, oracle, tmp_path):
+    """Sample::AddPotential through the RUMD classes: both potentials act, a
+    third is refused, SetPotential goes back to one."""
+    s, g = golden_sample(rumd, tmp_path)
+    lj = rumd.Pot_LJ_12_6(cutoff_method=rumd.ShiftedForce)
+    sm = rumd.Pot_LJ_12_6_smooth_2_4(cutoff_method=rumd.ShiftedPotential)
+    for (i, j), (sig, eps, rc) in KA.items():
+        lj.SetParams(i, j, sig, eps, rc)
+    for (i, j), (sig, eps, rc) in SMOOTH2.items():
+        sm.SetParams(i, j, sig, eps, rc)
+    s.SetPotential(lj)
+    s.AddPotential(sm)
+    assert len(s.GetPotentials()) == 2
+    s.CalcF()
+    pos = np.asarray(s.GetPositions(), np.float64)
+    types = np.asarray(s.GetTypes(), np.int32)
+    box = np.asarray(s.GetBoxLengths())
+    f1, u1, _ = oracle.forces_f64(pos, types, box, 2, oracle.lj_params(2, KA), 2, "LJ_12_6")
+    f2, u2, _ = oracle.forces_f64(pos, types, box, 2, oracle.smooth_params(2, SMOOTH2), 1, "LJ_12_6_smooth_2_4")
+    assert rms_rel(np.asarray(s.GetForces(), np.float64), f1 + f2) <= 1e-5
+    assert abs(s.GetPotentialEnergy() - (u1.sum() + u2.sum())) <= 1e-5 * abs(u1.sum() + u2.sum())
+    third = rumd.Pot_LJ_12_6(cutoff_method=rumd.ShiftedForce)
+    with pytest.raises(Exception):
+        s.AddPotential(third)
+    s.SetPotential(lj)
+    assert len(s.GetPotentials()) == 1
+    s.CalcF()
+    assert rms_rel(np.asarray(s.GetForces(), np.float64), f1) <= 1e-5

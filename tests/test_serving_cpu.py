@@ -20,18 +20,31 @@ class FakeClock:
 
 
 class FakeEngine:
-    """Advances queued steps like b2md_run_queued.  Cost model of one round on
-    the virtual clock: a fixed launch cost per step (what a small system alone
-    is bound by) plus the particle-steps of all replicas at `rate`."""
+    """The engine calls the server makes, on a virtual clock.  A chunk runs
+    when it is launched: every replica advances by up to its step count, and
+    the clock advances by a fixed launch cost per step (what a small system
+    alone is bound by) plus the particle-steps of all replicas at `rate`.
+    Memory: 600 bytes per particle."""
+
+    BYTES_PER_PARTICLE = 600
 
     def __init__(self, clock, rate=1e9):
         self.clock, self.rate = clock, rate
-        self.reps, self.next = {}, 0
+        self.reps, self.free = {}, []
         self.max_live = 0
+        self.tickets = 0
+        self.snaps = {}
+
+    def footprint(self, n, box, params, ntypes, **kw):
+        return n * self.BYTES_PER_PARTICLE
+
+    def usage(self):
+        return sum(r["n"] for r in self.reps.values()) * self.BYTES_PER_PARTICLE, 0
 
     def add(self, pos4, box, params, ntypes, **kw):
-        rid = self.next
-        self.next += 1
+        rid = min(self.free) if self.free else len(self.reps)
+        if rid in self.free:
+            self.free.remove(rid)
         self.reps[rid] = {"n": len(pos4), "left": 0, "steps": 0}
         self.max_live = max(self.max_live, len(self.reps))
         return rid
@@ -50,12 +63,35 @@ class FakeEngine:
         self.clock.t += todo * 10e-6 + work / self.rate
         return todo
 
+    def run_queued_async(self, k):
+        ran = self.run_queued(k)
+        self.tickets += 1
+        cap = max(self.reps) + 1 if self.reps else 0
+        snap = np.zeros((cap, 9))
+        snap[:, 2] = -1
+        for rid, r in self.reps.items():
+            snap[rid, [0, 1, 2, 3, 5, 6, 7]] = [1, r["steps"], r["left"], -5.0, 1.0, 0.0, 1]
+        self.snaps[self.tickets] = (ran, snap)
+        return self.tickets
+
+    def poll(self, ticket):
+        return True
+
+    def wait(self, ticket):
+        ran, snap = self.snaps.pop(ticket)
+        cap = max(list(self.reps) + [len(snap) - 1]) + 1
+        out = np.zeros((cap, 9))
+        out[:, 2] = -1
+        out[:len(snap)] = snap
+        return ran, out
+
     def stats(self, rid):
         r = self.reps[rid]
         return {"pe": -5.0, "ke": 1.0, "xi": 0.0, "steps": r["steps"], "rebuilds": 1, "steps_left": r["left"]}
 
     def remove(self, rid):
         del self.reps[rid]
+        self.free.append(rid)
 
 
 def small_stream(n=40, rate=50.0):
@@ -79,7 +115,7 @@ def test_all_jobs_complete_with_exact_step_counts():
     from rumd_b200 import serving
     clk = FakeClock()
     eng = FakeEngine(clk)
-    srv = serving.MDServer(eng, hbm_budget=150e9, chunk_steps=100, clock=clk, sleep=clk.sleep)
+    srv = serving.MDServer(eng, hbm_budget=150e9, chunk_steps=100, clock=clk, sleep=clk.sleep, workers=0)
     jobs = srv.serve(small_stream())
     assert all(j.done >= j.admitted >= j.arrival for j in jobs)
     assert all(j.result["steps"] == j.steps for j in jobs)
@@ -91,10 +127,10 @@ def test_all_jobs_complete_with_exact_step_counts():
 def test_budget_limits_concurrency_and_keeps_fifo():
     from rumd_b200 import serving
     jobs = small_stream(30, rate=1e6)  # everything arrives at once
-    budget = 3 * max(serving.job_bytes(j) for j in jobs)
+    budget = 3 * max(j.n for j in jobs) * FakeEngine.BYTES_PER_PARTICLE
     clk = FakeClock()
     eng = FakeEngine(clk)
-    srv = serving.MDServer(eng, hbm_budget=budget, chunk_steps=50, clock=clk, sleep=clk.sleep)
+    srv = serving.MDServer(eng, hbm_budget=budget, chunk_steps=50, clock=clk, sleep=clk.sleep, workers=0)
     srv.serve(jobs)
     assert srv.max_used <= budget
     assert 3 <= eng.max_live < len(jobs)
@@ -107,7 +143,7 @@ def test_job_larger_than_budget_is_rejected():
     from rumd_b200 import serving
     jobs = small_stream(3)
     clk = FakeClock()
-    srv = serving.MDServer(FakeEngine(clk), hbm_budget=1000, clock=clk, sleep=clk.sleep)
+    srv = serving.MDServer(FakeEngine(clk), hbm_budget=1000, clock=clk, sleep=clk.sleep, workers=0)
     with pytest.raises(ValueError):
         srv.serve(jobs)
 
@@ -117,7 +153,7 @@ def test_continuous_batching_beats_one_at_a_time_on_latency():
     overlaps jobs, so the mix finishes sooner than the sequential loop."""
     from rumd_b200 import serving
     clk = FakeClock()
-    srv = serving.MDServer(FakeEngine(clk, rate=2e8), chunk_steps=100, clock=clk, sleep=clk.sleep)
+    srv = serving.MDServer(FakeEngine(clk, rate=2e8), chunk_steps=100, clock=clk, sleep=clk.sleep, workers=0)
     mix = serving.latency_summary(srv.serve(small_stream()))
     clk2 = FakeClock()
     seq = serving.latency_summary(serving.serve_one_at_a_time(lambda: _closing(FakeEngine(clk2, rate=2e8)),
@@ -178,3 +214,61 @@ def test_two_rank_gloo_sharding():
         assert sorted(gathered[0] + gathered[1]) == list(range(64))
         assert not set(gathered[0]) & set(gathered[1])
         assert tmax == 2.0
+
+
+def test_snapshot_of_a_chunk_launched_before_admission_is_ignored():
+    """A replica id can be reused by a job admitted after a chunk was
+    launched; that chunk's snapshot shows the previous owner (done) and must
+    not retire the new job."""
+    from rumd_b200 import serving
+    clk = FakeClock()
+    eng = FakeEngine(clk)
+    srv = serving.MDServer(eng, clock=clk, sleep=clk.sleep, workers=0)
+    job = serving.Job(id=0, kind="KA", n=256, T=1.0, steps=100, arrival=0.0)
+    rid = eng.add(np.zeros((256, 4), np.float32), None, None, 2)
+    srv.running[rid] = serving._Resident(job, 100, first_ticket=5)
+    snap = np.zeros((1, 9))
+    snap[0, serving.SNAP["active"]] = 1
+    snap[0, serving.SNAP["steps"]] = 100
+    srv._after_chunk(4, snap, 1.0, [])
+    assert rid in srv.running and job.done < 0
+    srv._after_chunk(5, snap, 2.0, [])
+    assert rid not in srv.running and job.done == 2.0 and job.result["steps"] == 100
+
+
+def test_configurations_built_on_worker_threads_keep_fifo():
+    from rumd_b200 import serving
+    jobs = small_stream(20, rate=1e6)
+    clk = FakeClock()
+    eng = FakeEngine(clk)
+    budget = 4 * max(j.n for j in jobs) * FakeEngine.BYTES_PER_PARTICLE
+    srv = serving.MDServer(eng, hbm_budget=budget, chunk_steps=80, clock=clk, sleep=clk.sleep, workers=2)
+    srv.serve(jobs)
+    assert all(j.result["steps"] == j.steps for j in jobs)
+    order = sorted(jobs, key=lambda j: (j.admitted, j.id))
+    assert [j.id for j in order] == sorted(j.id for j in jobs)
+    assert srv.max_used <= budget and not eng.reps
+
+
+def test_auto_chunk_length_follows_the_resident_particles():
+    from rumd_b200 import serving
+    clk = FakeClock()
+    srv = serving.MDServer(FakeEngine(clk), clock=clk, sleep=clk.sleep, workers=0, chunk_seconds=0.05,
+                           rate_hint=1e9, min_chunk_steps=16, max_chunk_steps=2000)
+    for rid, n in enumerate([100000, 400000]):
+        srv.running[rid] = serving._Resident(serving.Job(rid, "LJ", n, 1.0, 10, 0.0), 10)
+    assert srv.chunk_length() == 100  # 0.05 s * 1e9 / 5e5 particles
+    srv.running.pop(1)
+    srv.running[0].left = 0
+    assert srv.chunk_length() == 2000  # nothing left to run: the cap
+
+
+def test_timeline_summary_reports_backlog_and_offered_load():
+    from rumd_b200 import serving
+    clk = FakeClock()
+    srv = serving.MDServer(FakeEngine(clk, rate=1e8), chunk_steps=100, clock=clk, sleep=clk.sleep, workers=0)
+    jobs = srv.serve(small_stream(30, rate=200.0))
+    s = serving.timeline_summary(srv, jobs, step_s=0.05)
+    assert s["rows"] and s["columns"][0] == "t_s"
+    assert s["offered_particle_steps_per_s"] > 0 and s["chunks"] == srv.chunks > 0
+    assert s["rows"][-1][3] == 0.0  # drained at the end
