@@ -461,7 +461,7 @@ def served(capi, device, pb, tp, njobs, seed=0):
                            workers=2, max_resident=1024)
     srv.serve(jobs)
     reserved = e.memory()
-    builds = e.get_variant(capi.VARIANT_GRAPH_BUILDS)
+    counters = e.counters()
     e.close()
     summ = serving.latency_summary(jobs)
     tl = serving.timeline_summary(srv, jobs)
@@ -485,7 +485,7 @@ def served(capi, device, pb, tp, njobs, seed=0):
     return {"value": thr, "unit": "particle-steps/s", "jobs": summ["jobs"],
             "p50_latency_s": summ["p50_s"], "p99_latency_s": summ["p99_s"], "makespan_s": summ["makespan_s"],
             "particle_steps": summ["particle_steps"], "hbm_max_used_bytes": srv.max_used,
-            "hbm_reserved_bytes": reserved, "graph_builds": builds, "chunks": srv.chunks, "tuning": tune,
+            "hbm_reserved_bytes": reserved, "engine_counters": counters, "tuning": tune,
             "sustainability": verdict, "load_over_time": tl,
             "one_at_a_time_value": one_rate,
             "one_at_a_time_sample": f"{len(sample)} of the {njobs} jobs run alone back to back (wall clock)",

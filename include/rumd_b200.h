@@ -135,6 +135,21 @@ B2MD_API int b2md_engine_memory(b2md_engine* e, long long* bytes);
  * one system per process and sizes its buffers per Sample
  * (Sample.cu:208-249, NeighborList.cu:275-295). */
 B2MD_API int b2md_engine_usage(b2md_engine* e, long long* used, long long* reserved);
+/* Counters of the engine's host-side events since its creation (the first
+ * n of B2MD_COUNTERS): step-graph instantiations; valid graphs dropped by a
+ * re-layout, by a pool growth (pools moved), by a list repair, by another
+ * setting change; neighbour lists enlarged after an overflow; tile layouts
+ * applied; b2md_run_queued_async chunks launched. */
+#define B2MD_COUNTER_GRAPH_BUILDS 0
+#define B2MD_COUNTER_INVAL_LAYOUT 1
+#define B2MD_COUNTER_INVAL_POOL 2
+#define B2MD_COUNTER_INVAL_REPAIR 3
+#define B2MD_COUNTER_INVAL_OTHER 4
+#define B2MD_COUNTER_LIST_REPAIRS 5
+#define B2MD_COUNTER_LAYOUTS 6
+#define B2MD_COUNTER_CHUNKS 7
+#define B2MD_COUNTERS 8
+B2MD_API int b2md_engine_counters(b2md_engine* e, long long* out, int n);
 /* Chooses CUDA-graph conditional rebuild nodes (1, default) or unconditional
  * early-exit rebuild kernels (0) for b2md_run. */
 B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);

@@ -27,12 +27,14 @@ STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_lef
               "target_T", "max_nbrs", "actual_max_nbrs", "mean_nbrs", "window_tiles", "tiles"]
 NSTAT = len(STAT_NAMES)
 NB_METHOD = {"default": -1, "sort": 0, "n2": 1}
+COUNTER_NAMES = ["graph_builds", "graphs_dropped_by_layout", "graphs_dropped_by_pool_growth",
+                 "graphs_dropped_by_list_repair", "graphs_dropped_by_settings", "list_repairs", "layouts", "chunks"]
 # per-replica fields of a chunk's snapshot (b2md_run_queued_wait)
 CHUNK_FIELDS = ["active", "steps", "steps_left", "pe", "virial", "ke", "xi", "rebuilds", "overflow"]
 
 EXPORTS = [
     "b2md_engine_create", "b2md_engine_destroy", "b2md_engine_set_launch", "b2md_engine_get_launch",
-    "b2md_engine_memory", "b2md_engine_usage", "b2md_replica_footprint", "b2md_run_queued_async",
+    "b2md_engine_memory", "b2md_engine_usage", "b2md_engine_counters", "b2md_replica_footprint", "b2md_run_queued_async",
     "b2md_run_queued_poll", "b2md_run_queued_wait",
     "b2md_engine_set_graph_mode", "b2md_engine_set_variant", "b2md_engine_get_variant", "b2md_replica_add", "b2md_replica_remove", "b2md_replica_get",
     "b2md_replica_read", "b2md_replica_set", "b2md_replica_set_potential", "b2md_replica_add_potential", "b2md_replica_set_integrator",
@@ -79,6 +81,7 @@ def lib():
             "b2md_engine_get_launch": [P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)],
             "b2md_engine_memory": [P, ctypes.POINTER(ll)],
             "b2md_engine_usage": [P, ctypes.POINTER(ll), ctypes.POINTER(ll)],
+            "b2md_engine_counters": [P, P, i],
             "b2md_replica_footprint": [P, ctypes.POINTER(ReplicaDesc), ctypes.POINTER(ll)],
             "b2md_run_queued_async": [P, ll, ctypes.POINTER(ll)],
             "b2md_run_queued_poll": [P, ll, ctypes.POINTER(i)],
@@ -256,6 +259,12 @@ class Engine:
         u, r = ctypes.c_longlong(), ctypes.c_longlong()
         check(lib().b2md_engine_usage(self._h, ctypes.byref(u), ctypes.byref(r)))
         return u.value, r.value
+
+    def counters(self):
+        """The engine's host-side event counters (b2md_engine_counters) by name."""
+        out = np.zeros(len(COUNTER_NAMES), np.int64)
+        check(lib().b2md_engine_counters(self._h, _ptr(out), len(COUNTER_NAMES)))
+        return dict(zip(COUNTER_NAMES, out.tolist()))
 
     def footprint(self, n, box, params, ntypes, **kw):
         """Device bytes a replica of n particles would hold (b2md_replica_footprint);

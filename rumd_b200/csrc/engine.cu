@@ -187,6 +187,9 @@ struct b2md_engine {
   int graph_types = 0;           // pair-table rows in the current persistent graph's shared memory
   bool wl_on = false;            // window-list pool allocated (force mode 2 used)
   int graph_builds = 0;          // step-graph instantiations so far (B2MD_VARIANT_GRAPH_BUILDS)
+  long long invalidations[4] = {0, 0, 0, 0};  // valid graphs dropped, by reason (INV_*)
+  long long list_repairs = 0;    // lists enlarged after an overflow
+  long long layout_uploads = 0;  // tile layouts applied
   ChunkRec chunk[2];             // b2md_run_queued_async chunks (by ticket parity)
   long long chunk_seq = 0;
   RangeAlloc palloc, ealloc, calloc, qalloc, zalloc;
@@ -343,7 +346,11 @@ char* stage_alloc(b2md_engine* e, size_t bytes) {
   return e->ring + lo;
 }
 
-void invalidate_graphs(b2md_engine* e) {
+// Why valid step graphs were dropped (b2md_engine_counters).
+enum { INV_OTHER = 0, INV_LAYOUT = 1, INV_POOL = 2, INV_REPAIR = 3, INV_REASONS = 4 };
+
+void invalidate_graphs(b2md_engine* e, int why = INV_OTHER) {
+  if (e->graphs_valid) ++e->invalidations[why];
   for (int k = 0; k < 3; ++k) {
     if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     if (e->graph[k]) cudaGraphDestroy(e->graph[k]);
@@ -373,7 +380,7 @@ void grow_particles(b2md_engine* e, long long need) {
   dev_grow(e, e->slot, e->pcap, nc, true);
   e->palloc.grow(nc);
   e->pcap = nc;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 // The list pool; the 16-bit window list beside it only once force mode 2
@@ -385,14 +392,14 @@ void grow_list(b2md_engine* e, long long need) {
   if (e->wl_on) dev_grow(e, e->wl, e->ecap, nc, false);
   e->ealloc.grow(nc);
   e->ecap = nc;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 void enable_window_list(b2md_engine* e) {
   if (e->wl_on) return;
   dev_grow(e, e->wl, 0, e->ecap, false);
   e->wl_on = true;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 void grow_cells(b2md_engine* e, long long need) {
@@ -402,7 +409,7 @@ void grow_cells(b2md_engine* e, long long need) {
   dev_grow(e, e->cstart, e->ccap, nc, true);
   e->calloc.grow(nc);
   e->ccap = nc;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 void grow_params(b2md_engine* e, long long need) {
@@ -411,7 +418,7 @@ void grow_params(b2md_engine* e, long long need) {
   dev_grow(e, e->par, e->qcap, nc, true);
   e->qalloc.grow(nc);
   e->qcap = nc;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 void grow_elog(b2md_engine* e, long long need) {
@@ -420,7 +427,7 @@ void grow_elog(b2md_engine* e, long long need) {
   dev_grow(e, e->elog, e->zcap * 5, nc * 5, true);
   e->zalloc.grow(nc);
   e->zcap = nc;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 void grow_reps(b2md_engine* e, int need) {
@@ -431,7 +438,7 @@ void grow_reps(b2md_engine* e, int need) {
   dev_grow(e, e->rctr, 2LL * e->rcap, 2LL * nc, true);  // two halves (k_steps: by step parity)
   dev_grow(e, e->flist, 2LL * e->rcap, 2LL * nc, true);  // two halves (k_batch: by step parity)
   e->rcap = nc;
-  invalidate_graphs(e);
+  invalidate_graphs(e, INV_POOL);
 }
 
 // Largest type count over the active replicas.
@@ -537,7 +544,7 @@ bool grow_tiles(b2md_engine* e, int T, int G) {
     e->gcap = nc;
     grew = true;
   }
-  if (grew) invalidate_graphs(e);
+  if (grew) invalidate_graphs(e, INV_POOL);
   return grew;
 }
 
@@ -595,7 +602,8 @@ void apply_layout(b2md_engine* e) {
   drop_windows(e);  // tiles changed: no window until the next list build
   const bool keep = e->graphs_valid && e->persist_kind == 2 && persist_kind_for(e) == 2 &&
                     max_types_active(e) <= e->graph_types;
-  if (!keep) invalidate_graphs(e);
+  if (!keep) invalidate_graphs(e, INV_LAYOUT);
+  ++e->layout_uploads;
 }
 
 // Applies admissions and removals made since the last launch, then computes
@@ -1284,8 +1292,9 @@ bool repair_overflow(b2md_engine* e) {
     WRITE_STATE(e, (int)r, overflow, 0);
     WRITE_STATE(e, (int)r, rebuild, 1);
     any = true;
+    ++e->list_repairs;
   }
-  if (any) invalidate_graphs(e);
+  if (any) invalidate_graphs(e, INV_REPAIR);
   return any;
 }
 
@@ -1817,6 +1826,15 @@ int b2md_replica_footprint(b2md_engine* e, const b2md_replica_desc* d, long long
     h.ecap = (d->energy_interval > 0 && d->energy_capacity > 0) ? d->energy_capacity : 0;
     *bytes = replica_bytes(e, h);
   });
+}
+
+int b2md_engine_counters(b2md_engine* e, long long* out, int n) {
+  if (!e || (n > 0 && !out)) return fail(B2MD_ERR_ARG, "null argument");
+  const long long v[B2MD_COUNTERS] = {e->graph_builds, e->invalidations[INV_LAYOUT], e->invalidations[INV_POOL],
+                                      e->invalidations[INV_REPAIR], e->invalidations[INV_OTHER], e->list_repairs,
+                                      e->layout_uploads, e->chunk_seq};
+  for (int k = 0; k < n && k < B2MD_COUNTERS; ++k) out[k] = v[k];
+  return B2MD_OK;
 }
 
 int b2md_engine_usage(b2md_engine* e, long long* used, long long* reserved) {

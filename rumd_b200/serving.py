@@ -136,7 +136,9 @@ class MDServer:
         self.in_flight = int(in_flight)
         self.max_used = 0
         self.running = {}      # replica id -> _Resident
-        self.timeline = []     # after each chunk: (t, jobs waiting, jobs resident, backlog particle-steps)
+        # after each chunk: (t, jobs waiting, jobs resident, backlog particle-steps,
+        # resident particles with steps left, steps the chunk ran)
+        self.timeline = []
         self.chunks = 0
 
     # ---- memory ----
@@ -173,7 +175,8 @@ class MDServer:
         k = int(self.chunk_seconds * self.rate_hint / max(parts, 1))
         return max(self.min_chunk, min(self.max_chunk, k))
 
-    def _after_chunk(self, ticket, snap, now, waiting):
+    def _after_chunk(self, ticket, snap, now, waiting, ran=0):
+        parts = sum(r.job.n for r in self.running.values() if r.left > 0)
         for rid, r in list(self.running.items()):
             if r.first_ticket == 0 or ticket < r.first_ticket:
                 continue  # admitted after this chunk was launched
@@ -182,12 +185,12 @@ class MDServer:
             if r.left <= 0:
                 self.retire(rid, row, now)
         backlog = sum(r.left * r.job.n for r in self.running.values()) + sum(j.n * j.steps for j in waiting)
-        self.timeline.append((now, len(waiting), len(self.running), float(backlog)))
+        self.timeline.append((now, len(waiting), len(self.running), float(backlog), parts, int(ran)))
 
     @property
     def queue_depth(self):
         """Jobs waiting for admission, after each chunk."""
-        return [w for _, w, _, _ in self.timeline]
+        return [row[1] for row in self.timeline]
 
     def serve(self, jobs, realtime=True):
         """Runs the whole stream; returns the jobs with admitted/done times set."""
@@ -232,8 +235,8 @@ class MDServer:
                 if inflight:
                     if self.engine.poll(inflight[0]):
                         t = inflight.popleft()
-                        _, snap = self.engine.wait(t)
-                        self._after_chunk(t, snap, self.clock() - t0, waiting)
+                        ran, snap = self.engine.wait(t)
+                        self._after_chunk(t, snap, self.clock() - t0, waiting, ran)
                     else:
                         self.sleep(self.poll_seconds)
                 elif waiting:
@@ -271,8 +274,10 @@ def latency_summary(jobs):
 
 def timeline_summary(server, jobs, step_s=1.0):
     """Load over time: per `step_s` window, the largest number of jobs waiting
-    for admission and resident, and the backlog (particle-steps still to run)
-    at the window's end; with the offered load and whether the server kept up."""
+    for admission and resident, the backlog (particle-steps still to run) at
+    the window's end, the resident particles with steps left and the mean
+    time of a step of the chunks that ended in the window; with the offered
+    load."""
     tl = server.timeline
     if not tl:
         return {}
@@ -286,11 +291,16 @@ def timeline_summary(server, jobs, step_s=1.0):
             sel.append(tl[i])
             i += 1
         if sel:
-            rows.append([round(hi, 3), max(s[1] for s in sel), max(s[2] for s in sel), sel[-1][3]])
+            steps = sum(s[5] for s in sel)
+            t_lo = tl[i - len(sel) - 1][0] if i - len(sel) - 1 >= 0 else 0.0
+            step_us = (sel[-1][0] - t_lo) / steps * 1e6 if steps else None
+            rows.append([round(hi, 3), max(s[1] for s in sel), max(s[2] for s in sel), sel[-1][3],
+                         max(s[4] for s in sel), None if step_us is None else round(step_us, 1)])
     arrivals = [j.arrival for j in jobs]
     span = max(arrivals) - min(arrivals)
     work = float(sum(j.n * j.steps for j in jobs))
-    return {"window_s": step_s, "columns": ["t_s", "max_waiting", "max_resident", "backlog_particle_steps"],
+    return {"window_s": step_s, "columns": ["t_s", "max_waiting", "max_resident", "backlog_particle_steps",
+                                            "max_resident_particles", "us_per_step"],
             "rows": rows, "arrival_span_s": span, "offered_particle_steps_per_s": work / span if span > 0 else None,
             "max_waiting": max(s[1] for s in tl), "max_resident": max(s[2] for s in tl), "chunks": server.chunks}
 
