@@ -207,6 +207,11 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *   B2MD_VARIANT_GRAPH_BUILDS  read-only: step graphs instantiated so far
  *                              (admissions and removals do not rebuild a
  *                              k_batch graph).
+ *   B2MD_VARIANT_SPLIT_SORT_TILES  k_batch: replicas of at least this many
+ *                              tiles (default 16) sort their particles as
+ *                              phase items spread over many blocks; smaller
+ *                              ones are sorted by one block each.  Same
+ *                              permutation either way.
  * No reference counterpart beyond Sample::SetPB_TP (Sample.h:96). */
 enum {
   B2MD_VARIANT_FORCE_MODE = 0,
@@ -217,7 +222,8 @@ enum {
   B2MD_VARIANT_WINDOW_LIST_ROWS = 5,
   B2MD_VARIANT_PERSISTENT = 6,
   B2MD_VARIANT_PERSISTENT_ACTIVE = 7,
-  B2MD_VARIANT_GRAPH_BUILDS = 8
+  B2MD_VARIANT_GRAPH_BUILDS = 8,
+  B2MD_VARIANT_SPLIT_SORT_TILES = 9
 };
 B2MD_API int b2md_engine_set_variant(b2md_engine* e, int which, int value);
 B2MD_API int b2md_engine_get_variant(b2md_engine* e, int which, int* value);

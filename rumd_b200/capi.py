@@ -21,6 +21,7 @@ POTENTIAL = {"LJ_12_6": 0, "LJ_12_6_smooth_2_4": 1, "IPL_n": 2}
 # kernel variants (b2md_engine_set_variant)
 VARIANT_FORCE_MODE, VARIANT_BUILD_LANES, VARIANT_BUILD_SMEM, VARIANT_WINDOW_CAP, VARIANT_SM_TILES = 0, 1, 2, 3, 4
 VARIANT_WINDOW_LIST_ROWS, VARIANT_PERSISTENT, VARIANT_PERSISTENT_ACTIVE, VARIANT_GRAPH_BUILDS = 5, 6, 7, 8
+VARIANT_SPLIT_SORT_TILES = 9
 FORCE_STREAMED, FORCE_STAGED, FORCE_WINDOW = 0, 1, 2
 FIELD = {"pos": 0, "vel": 1, "force": 2, "virial": 3, "images": 4, "stress": 5}
 STAT_NAMES = ["pe", "virial", "ke", "xi", "ke2", "steps", "rebuilds", "steps_left", "overflow",

@@ -172,6 +172,7 @@ struct b2md_engine {
   bool persist_on = false;     // the current graphs are persistent ones (kind below)
   int persist_kind = 0;        // 1 k_steps, 2 k_batch
   int* flist = nullptr;        // k_batch rebuild lists (2 x rcap)
+  int split_tiles = 16;        // k_batch: replicas of at least this many tiles sort in phases over many blocks
   PersistCtl* pctl = nullptr;  // k_steps control block
   int* h_budget = nullptr;     // pinned: the step budget written before each persistent launch
   void* h_stage = nullptr;     // pinned staging for particle uploads and read-backs (grown on demand)
@@ -484,6 +485,7 @@ EngArgs make_args(b2md_engine* e) {
   a.wl_rows = e->force_mode == FM_WINDOW ? std::min(list_rows(a.idx_rows), e->wl_rows_cap & ~7) : 0;
   a.flist = e->flist;
   a.bshared_off = 0;
+  a.split_tiles = e->split_tiles;
   return a;
 }
 
@@ -1669,6 +1671,10 @@ int b2md_engine_set_variant(b2md_engine* e, int which, int value) {
       return fail(B2MD_ERR_ARG, "persistent_active is read-only");
     case B2MD_VARIANT_GRAPH_BUILDS:
       return fail(B2MD_ERR_ARG, "graph_builds is read-only");
+    case B2MD_VARIANT_SPLIT_SORT_TILES:
+      if (value < 1) return fail(B2MD_ERR_ARG, "split_sort_tiles must be >= 1 (got %d)", value);
+      e->split_tiles = value;
+      break;
     default:
       return fail(B2MD_ERR_ARG, "unknown variant %d", which);
   }
@@ -1688,6 +1694,7 @@ int b2md_engine_get_variant(b2md_engine* e, int which, int* value) {
     case B2MD_VARIANT_PERSISTENT: *value = e->persist; break;
     case B2MD_VARIANT_PERSISTENT_ACTIVE: *value = (e->graphs_valid && e->persist_on) ? e->persist_kind : 0; break;
     case B2MD_VARIANT_GRAPH_BUILDS: *value = e->graph_builds; break;
+    case B2MD_VARIANT_SPLIT_SORT_TILES: *value = e->split_tiles; break;
     default: return fail(B2MD_ERR_ARG, "unknown variant %d", which);
   }
   return B2MD_OK;

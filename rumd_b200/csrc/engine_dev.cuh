@@ -102,6 +102,7 @@ struct RepState {
   int actual_max_nbrs, nlog;
   int err;               // a bounded device wait gave up (reported to the host)
   unsigned sort_done;    // k_batch: epoch of the replica's last in-launch sort
+  unsigned sort_items;   // k_batch: phase items of the replica's split sort completed (reset by the last)
 };
 
 // Control block of the persistent step kernel (k_steps), one per engine.
@@ -172,6 +173,7 @@ struct EngArgs {
   unsigned* smctr;     // per-region claim counters [nreg] + tiles claimed [nreg]
   int* flist;          // k_batch: rebuild lists, two halves by step parity (replica ids)
   int bshared_off;     // k_batch: offset of its per-block tables in dynamic shared memory
+  int split_tiles;     // k_batch: replicas of at least this many tiles sort as phase items over many blocks
 };
 
 }  // namespace b2md

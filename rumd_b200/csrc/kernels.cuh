@@ -2857,6 +2857,147 @@ __device__ __forceinline__ bool wait_eq_u32(const unsigned* p, unsigned want) {
   return true;
 }
 
+// Bounded wait of thread 0 until *p >= want (acquire); false when it gave up.
+__device__ __forceinline__ bool wait_ge_u32(const unsigned* p, unsigned want) {
+  for (unsigned it = 0; ld_acquire_u32(p) < want; ++it) {
+    if (it >= kWaitPolls) return false;
+    __nanosleep(64);
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// The split sort of k_batch: the stable cell-key sort of a large replica as
+// phase items that any blocks take, one item per tile (or per the tile's
+// share of the cells), so that a 32k-particle replica sorts in a few
+// microseconds per phase instead of one block running all of it.  The
+// phases are those of block_sort and of the sort kernels:
+//   0 clear the cell counts of a chunk of cells        (C items)
+//   1 cell key and arrival rank of a tile's particles  (C items)
+//   2 absolute cell starts (one block scan)            (1 item)
+//   3 scatter a tile's particles to their buckets      (C items)
+//   4 order a chunk of cells' buckets by current slot
+//     and gather r, v, images and ids of their slots   (C items)
+// where C is the replica's tile count.  Each finished item adds one to the
+// replica's sort_items (acquire-release); an item of phase p waits (bounded)
+// until the items of the earlier phases are all counted: split_sort_need.
+// The last item of phase 4 flips the buffer parities, resets the count and
+// publishes the sort under the step's epoch, as block_sort does.  The
+// permutation is the same stable sort.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned split_sort_need(int phase, unsigned C) {
+  return phase == 0 ? 0u : phase == 1 ? C : phase == 2 ? 2u * C : phase == 3 ? 2u * C + 1u : 3u * C + 1u;
+}
+__device__ __forceinline__ unsigned split_sort_items(unsigned C) { return 4u * C + 1u; }
+
+__device__ __forceinline__ int cell_key_of(const RepDev& R, const float4& r) {
+  // calculateCellIndices (NeighborList.cu:1142-1172)
+  return cell_coord(r.x, R.invL[0], R.nc[0]) + cell_coord(r.y, R.invL[1], R.nc[1]) * R.nc[0] +
+         cell_coord(r.z, R.invL[2], R.nc[2]) * R.nc[0] * R.nc[1];
+}
+
+// Orders bucket o[0, m) ascending (slot indices): small buckets in registers
+// by an odd-even transposition network, larger ones by insertion in place.
+__device__ __forceinline__ void order_bucket(unsigned* o, int m) {
+  if (m <= 1) return;
+  if (m <= kFixRegs) {
+    unsigned x[kFixRegs];
+#pragma unroll
+    for (int k = 0; k < kFixRegs; ++k) x[k] = k < m ? o[k] : 0xffffffffu;
+#pragma unroll
+    for (int r = 0; r < kFixRegs; ++r)
+#pragma unroll
+      for (int k = r & 1; k + 1 < kFixRegs; k += 2) {
+        const unsigned lo = min(x[k], x[k + 1]), hi = max(x[k], x[k + 1]);
+        x[k] = lo;
+        x[k + 1] = hi;
+      }
+#pragma unroll
+    for (int k = 0; k < kFixRegs; ++k)
+      if (k < m) o[k] = x[k];
+    return;
+  }
+  for (int q = 1; q < m; ++q) {
+    const unsigned v = o[q];
+    int k = q - 1;
+    while (k >= 0 && o[k] > v) {
+      o[k + 1] = o[k];
+      --k;
+    }
+    o[k + 1] = v;
+  }
+}
+
+// One item of phase `phase` (chunk: the tile / cell chunk index within the
+// replica).  rb, ab: the replica's buffer parities before the sort.
+__device__ __noinline__ void split_sort_item(const EngArgs& a, int rep, int phase, int chunk, int rb, int ab,
+                                             int* s_w) {
+  const RepDev& R = a.rep[rep];
+  const size_t p0 = (size_t)R.p0;
+  int* cnt = a.cnt + R.cell0;
+  int* cst = a.cstart + R.cell0;
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int ch = cell_chunk(R);
+  const int c0 = min(R.ncell, chunk * ch), c1 = min(R.ncell, c0 + ch);
+  const int tile = R.tile0 + chunk;
+  const int i0 = a.tile_first[tile];
+  const int i1 = chunk + 1 < R.ntiles ? a.tile_first[tile + 1] : R.n;
+  if (phase == 0) {
+    for (int c = c0 + tid; c < c1; c += bd) cnt[c] = 0;
+  } else if (phase == 1) {
+    for (int i = i0 + tid; i < i1; i += bd) {
+      const int key = cell_key_of(R, a.r[rb][p0 + i]);
+      a.key[p0 + i] = key;
+      a.slot[p0 + i] = atomicAdd(&cnt[key], 1);
+    }
+  } else if (phase == 2) {
+    // absolute first slot of every cell: thread t owns a run of cells, one
+    // block scan of the runs' totals
+    const int ncell = R.ncell;
+    const int K = (ncell + bd - 1) / bd;
+    constexpr int kCh = 8;
+    const int e0 = tid * K, e1 = min(ncell, e0 + K);
+    int tot = 0;
+    for (int cb = e0; cb < e1; cb += kCh) {
+      int x[kCh];
+#pragma unroll
+      for (int u = 0; u < kCh; ++u) x[u] = cb + u < e1 ? cnt[cb + u] : 0;
+#pragma unroll
+      for (int u = 0; u < kCh; ++u) tot += x[u];
+    }
+    int all;
+    int run = block_excl_scan(tot, s_w, &all);
+    for (int cb = e0; cb < e1; cb += kCh) {
+      int x[kCh];
+#pragma unroll
+      for (int u = 0; u < kCh; ++u) x[u] = cb + u < e1 ? cnt[cb + u] : 0;
+#pragma unroll
+      for (int u = 0; u < kCh; ++u)
+        if (cb + u < e1) {
+          cst[cb + u] = run;
+          run += x[u];
+        }
+    }
+  } else if (phase == 3) {
+    for (int i = i0 + tid; i < i1; i += bd) a.order[p0 + cst[a.key[p0 + i]] + a.slot[p0 + i]] = (unsigned)i;
+  } else {
+    // buckets of the chunk's cells by current slot (= the stable sort), then
+    // the gather of their slots (ParticleData::UpdateAfterSorting,
+    // ParticleData.cu:493-528)
+    for (int c = c0 + tid; c < c1; c += bd) order_bucket(a.order + p0 + cst[c], cnt[c]);
+    __syncthreads();
+    const int s0 = c0 < R.ncell ? cst[c0] : R.n;
+    const int s1 = c1 < R.ncell ? cst[c1] : R.n;
+    for (int sl = s0 + tid; sl < s1; sl += bd) {
+      const size_t gs = p0 + sl, go = p0 + a.order[gs];
+      a.r[rb ^ 1][gs] = a.r[rb][go];
+      a.v[ab ^ 1][gs] = a.v[ab][go];
+      a.im[ab ^ 1][gs] = a.im[ab][go];
+      a.uidx[ab ^ 1][gs] = a.uidx[ab][go];
+    }
+  }
+}
+
 constexpr int kBatchMaxRep = 1024;   // replicas whose rebuild list a block holds in shared memory
 // Tiles of the other replicas claimed between the sorts and the builds: two
 // thirds of the tiles (on the 256-replica batch: 566, 548, 535 us per step
@@ -2874,6 +3015,9 @@ constexpr int kBatchEpochSteps = 4096;  // epochs: launch generation * this + st
 struct BatchShared {
   int list[kBatchMaxRep];
   int pref[kBatchMaxRep + 1];
+  int spref[kBatchMaxRep + 1];  // prefix of the split-sort chunks (tiles of the replicas sorted in phases)
+  int slist[kBatchMaxRep];      // replicas sorted by one block each
+  int blist[kBatchMaxRep];      // replicas sorted in phases
   unsigned bits[kBatchMaxRep / 32];
   int scan[33];
 };
@@ -2910,6 +3054,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
   // step barrier words' totals, the step's rebuild-list size and its tiles
   __shared__ unsigned s_gen, s_base;
   __shared__ int s_budget, s_nf, s_t2;
+  __shared__ int s_ns, s_nb, s_cs;  // the step's one-block sorts, split sorts and their chunks
   __shared__ int s_ntiles, s_nrep;  // the layout in effect (not the captured one)
   __shared__ unsigned long long s_seen[2];
   BatchShared* bs = reinterpret_cast<BatchShared*>(s_dyn + a.bshared_off);
@@ -2978,22 +3123,35 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     __syncthreads();
     {
       const int nf = s_nf;
-      int run = 0;
+      int run = 0, srun = 0, brun = 0;
       for (int k0 = 0; k0 < nf; k0 += blockDim.x) {
         const int k = k0 + threadIdx.x;
         const int r = k < nf ? __ldcg(a.flist + (size_t)par * a.rctr_half + k) : 0;
         const int nt = k < nf ? a.rep[r].ntiles : 0;
-        int tot;
+        // replicas of at least split_tiles tiles (cell method) sort in phases
+        const int big = (k < nf && nt >= a.split_tiles && a.rep[r].nb_method == NB_CELLS) ? 1 : 0;
+        int tot, stot, btot;
         const int ex = block_excl_scan(nt, bs->scan, &tot);
+        const int sex = block_excl_scan(big ? nt : 0, bs->scan, &stot);
+        const int bex = block_excl_scan(big, bs->scan, &btot);
         if (k < nf) {
           bs->list[k] = r;
           bs->pref[k] = run + ex;
+          bs->spref[k] = srun + sex;
+          if (big) bs->blist[brun + bex] = r;
+          else bs->slist[k - (brun + bex)] = r;
           atomicOr(&bs->bits[r >> 5], 1u << (r & 31));
         }
         run += tot;
+        srun += stot;
+        brun += btot;
       }
       if (threadIdx.x == 0) {
         bs->pref[nf] = run;
+        bs->spref[nf] = srun;
+        s_cs = srun;
+        s_nb = brun;
+        s_ns = nf - brun;
         s_t2 = run;  // tiles of the listed replicas
         __threadfence();
         if (atomicAdd(&c->readers, 1u) == gridDim.x - 1) {
@@ -3005,29 +3163,82 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     }
     __syncthreads();
     // claim items until the step's are gone (each block overshoots once).
-    // Ticket order: [sorts] [the first q tiles, other replicas] [builds]
-    // [the remaining tiles] [the listed replicas' force tiles]: the first
-    // tiles give the sorts time, the remaining ones the builds.
+    // Ticket order: [one-block sorts] [split sorts: phase 0 .. 4 items of
+    // every replica sorted in phases] [the first q tiles, other replicas]
+    // [builds] [the remaining tiles] [the listed replicas' force tiles]: the
+    // first tiles give the sorts time, the remaining ones the builds.  Every
+    // wait is on items with earlier tickets.
     for (;;) {
       if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - s_base);
       __syncthreads();
       const unsigned it = (unsigned)s_item;
       const int t2 = s_t2, nf = s_nf, ntiles = s_ntiles;
+      const int ns = s_ns, nb = s_nb, cs = s_cs;
+      const int so = ns + 4 * cs + nb;  // sort items
       const int q = batch_first_tiles(ntiles, t2);
-      if (it >= (unsigned)(nf + ntiles + 2 * t2)) break;
-      const bool tile_item = it >= (unsigned)nf && (it < (unsigned)(nf + q) || (it >= (unsigned)(nf + q + t2) &&
-                                                                             it < (unsigned)(nf + ntiles + t2)));
-      if (it < (unsigned)nf) {
-        block_sort(a, bs->list[it], s_gen * kBatchEpochSteps + (unsigned)step + 1u, bs->scan);
+      const unsigned epoch = s_gen * kBatchEpochSteps + (unsigned)step + 1u;
+      if (it >= (unsigned)(so + ntiles + 2 * t2)) break;
+      const bool tile_item = it >= (unsigned)so && (it < (unsigned)(so + q) || (it >= (unsigned)(so + q + t2) &&
+                                                                             it < (unsigned)(so + ntiles + t2)));
+      if (it < (unsigned)ns) {
+        block_sort(a, bs->slist[it], epoch, bs->scan);
+      } else if (it < (unsigned)so) {
+        // a split-sort item: its phase, replica and chunk
+        int j = (int)it - ns, phase;
+        if (j < cs) phase = 0;
+        else if ((j -= cs) < cs) phase = 1;
+        else if ((j -= cs) < nb) phase = 2;
+        else if ((j -= nb) < cs) phase = 3;
+        else { j -= cs; phase = 4; }
+        int r, chunk = 0;
+        if (phase == 2) {
+          r = bs->blist[j];
+        } else {
+          int lo = 0, hi = nf - 1;  // the listed replica whose chunk range holds j
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (bs->spref[mid] <= j) lo = mid;
+            else hi = mid - 1;
+          }
+          r = bs->list[lo];
+          chunk = j - bs->spref[lo];
+        }
+        RepState* S = a.st + r;
+        const unsigned C = (unsigned)a.rep[r].ntiles;
+        if (threadIdx.x == 0) {
+          s_ok = wait_ge_u32(&S->sort_items, split_sort_need(phase, C));
+          if (!s_ok) {
+            atomicExch(&c->err, 1);
+            s_step_tally += 1ull << kTallyRebuildShift;
+          }
+          s_max = __ldcg(&S->rbuf) | (__ldcg(&S->abuf) << 1);  // the parities before the sort
+        }
+        __syncthreads();
+        if (s_ok) {
+          split_sort_item(a, r, phase, chunk, s_max & 1, s_max >> 1, bs->scan);
+          __syncthreads();
+          if (threadIdx.x == 0) {
+            const unsigned done = atom_add_acq_rel(&S->sort_items, 1u) + 1u;
+            if (done == split_sort_items(C)) {
+              // the last item: flip the parities, reset the count, publish
+              S->rbuf = (s_max & 1) ^ 1;
+              S->abuf = (s_max >> 1) ^ 1;
+              S->actual_max_nbrs = 0;  // the per-build maximum (k_rb_clear)
+              S->sort_items = 0u;
+              __threadfence();
+              st_release_u32(&S->sort_done, epoch);
+            }
+          }
+        }
       } else if (tile_item) {
-        const int tile = it < (unsigned)(nf + q) ? (int)it - nf : (int)it - nf - t2;
+        const int tile = it < (unsigned)(so + q) ? (int)it - so : (int)it - so - t2;
         const int r = a.tile_rep[tile];
         if (!((bs->bits[r >> 5] >> (r & 31)) & 1u))
           force_tile<TP, true, false, FM_STREAMED, false, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, nullptr,
                                                                 0, nullptr, nullptr, nullptr, par ^ 1);
       } else {
-        const bool build = it < (unsigned)(nf + q + t2);
-        const int k = build ? (int)it - nf - q : (int)it - nf - ntiles - t2;
+        const bool build = it < (unsigned)(so + q + t2);
+        const int k = build ? (int)it - so - q : (int)it - so - ntiles - t2;
         int lo = 0, hi = nf - 1;  // the listed replica holding flagged tile k
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
@@ -3038,7 +3249,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
         const int tile = a.rep[r].tile0 + (k - bs->pref[lo]);
         RepState* S = a.st + r;
         if (threadIdx.x == 0) {
-          s_ok = build ? wait_eq_u32(&S->sort_done, s_gen * kBatchEpochSteps + (unsigned)step + 1u)
+          s_ok = build ? wait_eq_u32(&S->sort_done, epoch)
                        : wait_eq_u32(reinterpret_cast<const unsigned*>(&S->rebuild), 0u);
           if (!s_ok) {
             // recorded for the host and tallied with the barrier arrival, so
@@ -3063,7 +3274,7 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     }
     // step barrier: arrival + "steps left" and overflow tallies
     if (threadIdx.x == 0) {
-      s_base += (unsigned)(s_nf + s_ntiles + 2 * s_t2) + gridDim.x;
+      s_base += (unsigned)(s_ns + 4 * s_cs + s_nb + s_ntiles + 2 * s_t2) + gridDim.x;
       const int budget = --s_budget;
       const unsigned long long mine = 1ull + s_step_tally;
       const unsigned long long now = atom_add_acq_rel_u64(&c->word[par], mine) + mine;
@@ -3090,8 +3301,8 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       // list overflows and waits that gave up: the host repairs or reports
       const unsigned stop = (unsigned)((d >> kTallyRebuildShift) & kTallyField);
       // steps per launch: the epochs' and the tally fields' range, and the
-      // 32-bit ticket counter (at most nrep + 3 ntiles + grid tickets a step)
-      const unsigned per_step = (unsigned)s_nrep + 3u * (unsigned)s_ntiles + gridDim.x;
+      // 32-bit ticket counter (at most nrep + 7 ntiles + grid tickets a step)
+      const unsigned per_step = (unsigned)s_nrep + 7u * (unsigned)s_ntiles + gridDim.x;
       const int cap = min(min(kBatchEpochSteps - 2, (int)(kTallyField / (unsigned)(s_nrep + 1))),
                           (int)min(0x7fffffffu, 0xffffffffu / per_step));
       const int go = ok && stop == 0 && more > 0 && budget > 0 && step + 1 < cap;

@@ -108,14 +108,18 @@ def test_batch_kernel_mixed_sizes_types_and_methods(capi, ka_params, oracle):
     """k_batch on a mix it must handle: replicas of one and two types, a
     small box on the all-pairs list (no sort), sizes from 2 to 6000, uneven
     step queues, and an energy log; against one launch per step (itself
-    checked against the oracle elsewhere), bit for bit."""
+    checked against the oracle elsewhere), bit for bit.  k_batch runs with
+    every cell-method replica sorted in phases over many blocks (split
+    threshold 1 tile), with the default threshold (16 tiles: the 6000, 3000
+    and 1500-particle replicas) and with none split."""
     from rumd_b200 import initconf as I
     lj = oracle.lj_params(1, oracle.lj_table())
     specs = [("ka", 6000, 0.7, 90), ("lj", 3000, 1.2, 120), ("ka", 300, 2.0, 45), ("lj", 64, 1.0, 120),
              ("ka", 2, 1.0, 33), ("ka", 1500, 0.45, 120)]
     res = []
-    for persistent in (0, 2):
+    for persistent, split in ((0, 16), (2, 1), (2, 16), (2, 1 << 20)):
         e = engine(capi, persistent)
+        e.set_variant(capi.VARIANT_SPLIT_SORT_TILES, split)
         ids = []
         for kind, n, T, k in specs:
             c = (I.ka_config if kind == "ka" else I.lj_config)(n, T=T, seed=n)
@@ -132,13 +136,14 @@ def test_batch_kernel_mixed_sizes_types_and_methods(capi, ka_params, oracle):
             assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == 2
         res.append([(state(e, rid, n), e.stats(rid), e.energy_log(rid)) for rid, n, _, _ in ids])
         e.close()
-    for (sa, ta, la), (sb, tb, lb), spec in zip(res[0], res[1], specs):
-        assert ta["steps"] == tb["steps"] == spec[3]
-        assert ta["rebuilds"] == tb["rebuilds"]
-        assert ta["xi"] == tb["xi"]
-        assert np.array_equal(la, lb)
-        for a, b in zip(sa, sb):
-            assert np.array_equal(a, b)
+    for other in res[1:]:
+        for (sa, ta, la), (sb, tb, lb), spec in zip(res[0], other, specs):
+            assert ta["steps"] == tb["steps"] == spec[3]
+            assert ta["rebuilds"] == tb["rebuilds"]
+            assert ta["xi"] == tb["xi"]
+            assert np.array_equal(la, lb)
+            for a, b in zip(sa, sb):
+                assert np.array_equal(a, b)
 
 
 def test_overflow_repair_under_persistent_runs(capi, ka_params):
