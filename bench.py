@@ -394,7 +394,7 @@ def profile_batched(capi, device, args):
     tune = batch_tuning()
     e = batch_engine(capi, device, tune["pb"], tune["tp"], ns, Ts, confs, skin=tune["skin"])
     e.set_variant(capi.VARIANT_PERSISTENT, tune["persistent"])
-    e.run(300)
+    e.run_timed(300)  # warm-up with eager launches too (no graphs under the profiler)
     torch.cuda.synchronize(device)
     torch.cuda.profiler.start()
     ms, nl = e.run_timed(max(args.steps, 1))

@@ -3163,11 +3163,13 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
     }
     __syncthreads();
     // claim items until the step's are gone (each block overshoots once).
-    // Ticket order: [one-block sorts] [split sorts: phase 0 .. 4 items of
-    // every replica sorted in phases] [the first q tiles, other replicas]
-    // [builds] [the remaining tiles] [the listed replicas' force tiles]: the
-    // first tiles give the sorts time, the remaining ones the builds.  Every
-    // wait is on items with earlier tickets.
+    // Ticket order: [one-block sorts] [split sorts: phases 0, 1, 2]
+    // [a third of the first q tiles] [split phase 3] [a third] [split phase 4]
+    // [the last third] [builds] [the remaining tiles] [the listed replicas'
+    // force tiles]: force tiles of the other replicas between the split
+    // phases keep blocks busy while a phase's items complete, the first
+    // tiles give the sorts time, the remaining ones the builds.  Every wait
+    // is on items with earlier tickets.
     for (;;) {
       if (threadIdx.x == 0) s_item = (int)(atomicAdd(&c->ticket, 1u) - s_base);
       __syncthreads();
@@ -3178,18 +3180,39 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       const int q = batch_first_tiles(ntiles, t2);
       const unsigned epoch = s_gen * kBatchEpochSteps + (unsigned)step + 1u;
       if (it >= (unsigned)(so + ntiles + 2 * t2)) break;
-      const bool tile_item = it >= (unsigned)so && (it < (unsigned)(so + q) || (it >= (unsigned)(so + q + t2) &&
-                                                                             it < (unsigned)(so + ntiles + t2)));
+      // the sort segment [0, so + q): split phases 0-2 end at e2, then a
+      // third of the first tiles, phase 3 from b3, a third, phase 4 from b4,
+      // the last third from e4
+      const int f1 = q / 3, f2 = q / 3;
+      const int e2 = ns + 2 * cs + nb, b3 = e2 + f1, b4 = b3 + cs + f2, e4 = b4 + cs;
+      int phase = -1, j = 0, tile = -1;
       if (it < (unsigned)ns) {
-        block_sort(a, bs->slist[it], epoch, bs->scan);
-      } else if (it < (unsigned)so) {
-        // a split-sort item: its phase, replica and chunk
-        int j = (int)it - ns, phase;
+        phase = 5;  // a one-block sort
+      } else if (it < (unsigned)e2) {
+        j = (int)it - ns;
         if (j < cs) phase = 0;
         else if ((j -= cs) < cs) phase = 1;
-        else if ((j -= cs) < nb) phase = 2;
-        else if ((j -= nb) < cs) phase = 3;
-        else { j -= cs; phase = 4; }
+        else { j -= cs; phase = 2; }
+      } else if (it < (unsigned)b3) {
+        tile = (int)it - e2;
+      } else if (it < (unsigned)(b3 + cs)) {
+        j = (int)it - b3;
+        phase = 3;
+      } else if (it < (unsigned)b4) {
+        tile = f1 + ((int)it - b3 - cs);
+      } else if (it < (unsigned)e4) {
+        j = (int)it - b4;
+        phase = 4;
+      } else if (it < (unsigned)(so + q)) {
+        tile = f1 + f2 + ((int)it - e4);
+      } else if (it >= (unsigned)(so + q + t2) && it < (unsigned)(so + ntiles + t2)) {
+        tile = (int)it - so - t2;
+      }
+      const bool tile_item = tile >= 0;
+      if (phase == 5) {
+        block_sort(a, bs->slist[it], epoch, bs->scan);
+      } else if (phase >= 0) {
+        // a split-sort item: its replica and chunk
         int r, chunk = 0;
         if (phase == 2) {
           r = bs->blist[j];
@@ -3231,7 +3254,6 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
           }
         }
       } else if (tile_item) {
-        const int tile = it < (unsigned)(so + q) ? (int)it - so : (int)it - so - t2;
         const int r = a.tile_rep[tile];
         if (!((bs->bits[r >> 5] >> (r & 31)) & 1u))
           force_tile<TP, true, false, FM_STREAMED, false, true>(a, tile, s_dyn, s_blk, s_tot, s_bar, s_rows, nullptr,
