@@ -433,7 +433,8 @@ def batched(capi, device, pb, tp, steps, seed=0):
     rate_s = ps_seq / t_seq
     return {"value": rate_b, "unit": "particle-steps/s", "replicas": R, "particles": int(ns.sum()),
             "steps": steps, "ms_per_step": t_b / steps * 1e3, "tuning": tune,
-            "persistent_kernel": {0: "none (one launch per step)", 1: "k_steps", 2: "k_batch"}.get(kind, kind),
+            "persistent_kernel": {0: "none (one launch per step)", 1: "k_steps", 2: "k_batch",
+                                  3: "k_flow"}.get(kind, kind),
             "sequential_plain_value": rate_s,
             "sequential_sample": f"{len(sample)} of the {R} replicas run alone, one after another",
             "speedup_vs_sequential": rate_b / rate_s}
@@ -456,7 +457,7 @@ def served(capi, device, pb, tp, njobs, seed=0):
     # is rebuilt) while the stream runs; about 180 list entries per particle
     e = new_engine(capi, device=device, max_particles=total_n + 64 * njobs, max_replicas=min(njobs, 1024),
                    max_list_entries=180 * (total_n + 32 * njobs), pb=tune["pb"], tp=tune["tp"])
-    e.set_variant(capi.VARIANT_PERSISTENT, 2)
+    e.set_variant(capi.VARIANT_PERSISTENT, 3)  # k_flow: replicas step on their own
     srv = serving.MDServer(e, hbm_budget=150e9, chunk_steps="auto", dt=DT, skin=tune["skin"], tau=TAU,
                            workers=2, max_resident=1024)
     srv.serve(jobs)

@@ -195,15 +195,19 @@ B2MD_API int b2md_engine_set_graph_mode(b2md_engine* e, int conditional);
  *                              runs steps back to back, with a grid barrier
  *                              between them, until a list rebuild is due;
  *                              engines with more tiles than resident blocks
- *                              (batches) with the batched kernel (k_batch),
- *                              which runs whole steps, list rebuilds
- *                              included, with one grid barrier each;
- *                              2: k_batch whenever it applies (at most 1024
+ *                              (batches) with k_flow: whole steps, list
+ *                              rebuilds included, each replica stepping on
+ *                              its own through a queue of ready work items;
+ *                              (k_batch and k_flow apply to at most 1024
  *                              replicas of at most 65536 particles);
+ *                              3: k_flow whenever it applies (the limits
+ *                              of k_batch);  2: k_batch, the same items
+ *                              with one grid barrier per step for all
+ *                              replicas;
  *                              0: one kernel launch per step.
  *   B2MD_VARIANT_PERSISTENT_ACTIVE  read-only: the persistent kernel of the
  *                              current step graph (1 k_steps, 2 k_batch,
- *                              0 none).
+ *                              3 k_flow, 0 none).
  *   B2MD_VARIANT_GRAPH_BUILDS  read-only: step graphs instantiated so far
  *                              (admissions and removals do not rebuild a
  *                              k_batch graph).

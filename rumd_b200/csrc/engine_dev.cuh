@@ -103,6 +103,8 @@ struct RepState {
   int err;               // a bounded device wait gave up (reported to the host)
   unsigned sort_done;    // k_batch: epoch of the replica's last in-launch sort
   unsigned sort_items;   // k_batch: phase items of the replica's split sort completed (reset by the last)
+  int flow_left;         // k_flow: items of the replica's current phase not yet finished
+  int launch_steps;      // k_flow: steps the replica ran in the current launch
 };
 
 // Control block of the persistent step kernel (k_steps), one per engine.
@@ -121,6 +123,13 @@ struct PersistCtl {
   // so admissions and removals need no new graph
   int lay_ntiles;
   int lay_nrep;
+  // k_flow's item queue: tickets taken by consumers (head) and producers
+  // (tail), monotone across launches; replicas still stepping; the most
+  // steps a replica ran in the launch; blocks that left the launch
+  unsigned long long qhead, qtail;
+  int active;
+  int ran;
+  unsigned exited;
 };
 
 struct EngArgs {
@@ -174,6 +183,9 @@ struct EngArgs {
   int* flist;          // k_batch: rebuild lists, two halves by step parity (replica ids)
   int bshared_off;     // k_batch: offset of its per-block tables in dynamic shared memory
   int split_tiles;     // k_batch: replicas of at least this many tiles sort as phase items over many blocks
+  int2* fq;            // k_flow: item queue slots (replica, item code)
+  unsigned long long* fseq;  // k_flow: ticket + 1 of the item in each slot (release-published)
+  unsigned qcap;       // k_flow: queue slots
 };
 
 }  // namespace b2md

@@ -261,6 +261,10 @@ __device__ __forceinline__ void integrate_one(const RepDev& R, float xi_f, float
 // k_steps: what this block adds to its step-barrier arrival (its replica
 // still has steps, its tile asks for a rebuild); thread 0 only.
 __shared__ unsigned long long s_step_tally;
+// k_flow: the finalizing block's decision for its replica's next step
+// (-1: this block did not finalize; 0 stop, 1 force items, 2 rebuild items)
+__shared__ int s_fin;
+constexpr int kFlowPar = -2;  // finish_step's bpar in k_flow
 constexpr int kTallyMoreShift = 24, kTallyRebuildShift = 44;
 constexpr unsigned long long kTallyArriveMask = (1ull << kTallyMoreShift) - 1ull;
 constexpr unsigned long long kTallyField = (1ull << 20) - 1ull;
@@ -302,6 +306,13 @@ __device__ void finish_step(const EngArgs& a, int rep, const RepDev& R, RepState
   int ex = atomicExch(&S->exceed, 0);
   S->rebuild = ex > 0;
   if (ex > 0) atomicAdd(a.any_rebuild, 1);
+  if (bpar == kFlowPar) {
+    // k_flow: the replica's steps in this launch, and what comes next
+    const int ls = __ldcg(&S->launch_steps) + 1;
+    S->launch_steps = ls;
+    atomicMax(&a.pctl->ran, ls);
+    s_fin = (left > 1 && ls < __ldcg(&a.pctl->budget)) ? (ex > 0 ? 2 : 1) : 0;
+  }
   if (bpar >= 0 && left > 1) {
     s_step_tally += 1ull << kTallyMoreShift;
     if (ex > 0) {
@@ -2444,7 +2455,8 @@ __device__ __forceinline__ int run_store(unsigned bits, const int* __restrict__ 
 // and cell arrays were written earlier in the same launch (k_batch), so they
 // are read with coherent loads.
 template <bool COH>
-__device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
+__device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max,
+                                                int* s_last = nullptr) {
   constexpr unsigned FULL = 0xffffffffu;
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
@@ -2611,6 +2623,7 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
     }
     __threadfence();
     const unsigned cdone = atomicAdd(&a.rctr[rep], 1u);
+    if (s_last) *s_last = cdone == (unsigned)(R.ntiles - 1);
     if (cdone == (unsigned)(R.ntiles - 1)) {
       a.rctr[rep] = 0u;
       S->nrebuilds += 1;
@@ -2624,6 +2637,11 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
 // not add to those of k_batch's force path.
 __device__ __noinline__ void build_runs_tile_batch(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
   build_runs_tile<true>(a, tile, s_cs2, s_run, s_max);
+}
+// k_flow's: also reports whether this tile's build was the replica's last.
+__device__ __noinline__ void build_runs_tile_flow(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max,
+                                                  int* s_last) {
+  build_runs_tile<true>(a, tile, s_cs2, s_run, s_max, s_last);
 }
 
 __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
@@ -3335,6 +3353,260 @@ __global__ void __maxnreg__(64) k_batch(EngArgs a, cudaGraphConditionalHandle h_
       s_go = go;
     }
     __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k_flow: the same steps as k_batch, each replica stepping on its own.
+// Work items go through one queue (a ring of slots in global memory); an
+// item is queued only when everything it reads is complete, so no item
+// waits:
+//   * a replica's step: its force tiles (fused force + Nose-Hoover); the
+//     replica's finalizer (the last tile's block) queues the next step's
+//     items -- force tiles, or the sort when its list is due -- or, when the
+//     replica has no steps left or has run the launch's budget, retires it
+//     from the launch;
+//   * a rebuild: the sort (one item for replicas below the split threshold,
+//     else the five split phases, each phase's last item queueing the next),
+//     then one build item per tile; the last build queues the force tiles.
+// Items of one phase count down the replica's flow_left; the block that
+// finishes the last queues the next phase.  Replicas therefore advance at
+// their own pace: a large replica's rebuild no longer holds every other
+// replica at a step barrier.  The queue's tickets are 64-bit and monotone
+// across launches; a slot is published by a release store of its ticket + 1,
+// and a consumer polls (bounded) for it, or for no replica left stepping,
+// which ends the launch.  The arithmetic of a replica is that of k_batch and
+// the per-step path (the same items), so results agree bit for bit.
+// ---------------------------------------------------------------------------
+constexpr unsigned kFlowForce = 0u, kFlowSort1 = 1u, kFlowSplit = 2u, kFlowBuild = 3u;
+
+// Queues items idx = 0 .. n-1 of kind/phase for replica rep (all threads of
+// the block; the caller has published the replica's state with a fence).
+__device__ __forceinline__ void flow_push(const EngArgs& a, int rep, unsigned kind, unsigned phase, int n,
+                                          unsigned long long* s_t0) {
+  PersistCtl* c = a.pctl;
+  if (threadIdx.x == 0) *s_t0 = atomicAdd(&c->qtail, (unsigned long long)n);
+  __syncthreads();
+  const unsigned long long t0 = *s_t0;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    const unsigned long long t = t0 + (unsigned long long)k;
+    const unsigned slot = (unsigned)(t % a.qcap);
+    a.fq[slot] = make_int2(rep, (int)((kind << 28) | (phase << 20) | (unsigned)k));
+    st_release_u64(&a.fseq[slot], t + 1ull);
+  }
+  __syncthreads();
+}
+
+// A replica's next items: its force tiles, or (rebuild) the start of its sort.
+__device__ void flow_start_step(const EngArgs& a, int rep, bool rebuild, unsigned long long* s_t0) {
+  const RepDev& R = a.rep[rep];
+  RepState* S = a.st + rep;
+  unsigned kind = kFlowForce;
+  int n = R.ntiles;
+  if (rebuild) {
+    if (R.nb_method == NB_CELLS && R.ntiles >= a.split_tiles) {
+      kind = kFlowSplit;  // phase 0: one item per chunk
+    } else {
+      kind = kFlowSort1;
+      n = 1;
+    }
+  }
+  if (threadIdx.x == 0) {
+    S->flow_left = n;
+    __threadfence();
+  }
+  __syncthreads();
+  flow_push(a, rep, kind, 0u, n, s_t0);
+}
+
+// Counts one finished item of the replica's phase; true in every thread of
+// the block that finished the phase's last.
+__device__ __forceinline__ bool flow_item_done(RepState* S, int* s_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    *s_flag = atomicSub(&S->flow_left, 1) == 1;
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
+__device__ __forceinline__ void flow_retire(const EngArgs& a) {
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicSub(&a.pctl->active, 1);
+  }
+}
+
+template <int TP>
+__global__ void __maxnreg__(64) k_flow(EngArgs a, cudaGraphConditionalHandle h_loop) {
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  __shared__ double s_blk[kNPart], s_tot[kNPart];
+  __shared__ __align__(8) uint64_t s_bar;
+  __shared__ unsigned s_rows;
+  __shared__ int s_go, s_last, s_max, s_flag, s_rep, s_code;
+  __shared__ unsigned s_gen;
+  __shared__ unsigned long long s_t0;
+  __shared__ int s_scan[33];
+  PersistCtl* c = a.pctl;
+  if (threadIdx.x == 0) {
+    s_go = __ldcg(&c->err) == 0;
+    if (!s_go && blockIdx.x == 0) set_loop(h_loop, 0u);
+  }
+  __syncthreads();
+  if (!s_go) return;
+  // setup barrier; its last block aligns the queue's tickets, starts every
+  // replica that has steps left and releases the others
+  if (threadIdx.x == 0) {
+    s_gen = ld_acquire_u32(&c->gen);
+    const unsigned long long nnow = atom_add_acq_rel_u64(&c->arrive, 1ull) + 1ull;
+    s_last = (nnow & kTallyArriveMask) == gridDim.x;
+  }
+  __syncthreads();
+  if (s_last) {
+    const int nrep = __ldcg(&c->lay_nrep);
+    if (threadIdx.x == 0) {
+      const unsigned long long h = __ldcg(&c->qhead), t = __ldcg(&c->qtail);
+      c->qhead = c->qtail = h > t ? h : t;
+      c->active = 0;
+      c->ran = 0;
+      c->exited = 0u;
+      *a.any_rebuild = 0;
+    }
+    __syncthreads();
+    for (int r = 0; r < nrep; ++r) {
+      RepState* S = a.st + r;
+      if (threadIdx.x == 0)
+        s_flag = a.rep[r].active && !S->overflow && S->steps_left > 0 && a.rep[r].ntiles > 0;
+      __syncthreads();
+      if (s_flag) {
+        if (threadIdx.x == 0) {
+          S->launch_steps = 0;
+          c->active += 1;
+        }
+        flow_start_step(a, r, S->rebuild != 0, &s_t0);
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      c->arrive = 0ull;
+      __threadfence();
+      st_release_u32(&c->gen, s_gen + 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    s_go = barrier_wait(c, s_gen, h_loop);
+  }
+  __syncthreads();
+  while (s_go) {
+    // the next item, or the end of the launch
+    if (threadIdx.x == 0) {
+      const unsigned long long t = atomicAdd(&c->qhead, 1ull);
+      const unsigned slot = (unsigned)(t % a.qcap);
+      int got = 0;
+      for (unsigned it = 0;; ++it) {
+        if (ld_acquire_u64(&a.fseq[slot]) == t + 1ull) {
+          const int2 q = __ldcg(a.fq + slot);
+          s_rep = q.x;
+          s_code = q.y;
+          got = 1;
+          break;
+        }
+        if (ld_acquire_u32(reinterpret_cast<const unsigned*>(&c->active)) == 0u || __ldcg(&c->err)) break;
+        if (it >= kBarrierPolls) {
+          atomicExch(&c->err, 1);
+          break;
+        }
+        __nanosleep(32);
+      }
+      s_go = got;
+    }
+    __syncthreads();
+    if (!s_go) break;
+    const int rep = s_rep;
+    const unsigned code = (unsigned)s_code;
+    const unsigned kind = code >> 28, phase = (code >> 20) & 0xffu;
+    const int idx = (int)(code & 0xfffffu);
+    const RepDev& R = a.rep[rep];
+    RepState* S = a.st + rep;
+    if (kind == kFlowForce) {
+      if (threadIdx.x == 0) s_fin = -1;
+      __syncthreads();
+      force_tile<TP, true, false, FM_STREAMED, false, true>(a, R.tile0 + idx, s_dyn, s_blk, s_tot, s_bar, s_rows,
+                                                            nullptr, 0, nullptr, nullptr, nullptr, kFlowPar);
+      __syncthreads();
+      const int fin = s_fin;
+      if (fin == 0) flow_retire(a);
+      else if (fin > 0) flow_start_step(a, rep, fin == 2, &s_t0);
+    } else if (kind == kFlowSort1 || kind == kFlowSplit) {
+      if (kind == kFlowSort1) {
+        block_sort(a, rep, 0u, s_scan);
+      } else {
+        if (threadIdx.x == 0) s_max = __ldcg(&S->rbuf) | (__ldcg(&S->abuf) << 1);
+        __syncthreads();
+        split_sort_item(a, rep, (int)phase, idx, s_max & 1, s_max >> 1, s_scan);
+      }
+      if (flow_item_done(S, &s_flag)) {
+        unsigned nkind = kFlowBuild, nphase = 0u;
+        int n = R.ntiles;
+        if (kind == kFlowSplit && phase < 4u) {
+          nkind = kFlowSplit;
+          nphase = phase + 1u;
+          n = nphase == 2u ? 1 : R.ntiles;
+        }
+        if (threadIdx.x == 0) {
+          if (kind == kFlowSplit && phase == 4u) {
+            // the sort is complete: flip the parities (the per-build maximum
+            // starts again, as k_rb_clear does)
+            S->rbuf = (s_max & 1) ^ 1;
+            S->abuf = (s_max >> 1) ^ 1;
+            S->actual_max_nbrs = 0;
+          }
+          S->flow_left = n;
+          __threadfence();
+        }
+        __syncthreads();
+        flow_push(a, rep, nkind, nphase, n, &s_t0);
+      }
+    } else {
+      float* s_cs2 = reinterpret_cast<float*>(s_dyn);
+      int* s_run = reinterpret_cast<int*>(s_dyn + kCs2Floats * sizeof(float));
+      build_runs_tile_flow(a, R.tile0 + idx, s_cs2, s_run, &s_max, &s_last);
+      __syncthreads();
+      if (s_last) {
+        // the replica's lists are complete: its force tiles, unless a list
+        // overflowed (the replica leaves the launch; the host enlarges it)
+        if (threadIdx.x == 0) s_flag = __ldcg(&S->overflow) != 0;
+        __syncthreads();
+        if (s_flag) {
+          flow_retire(a);
+        } else {
+          if (threadIdx.x == 0) {
+            S->flow_left = R.ntiles;
+            __threadfence();
+          }
+          __syncthreads();
+          flow_push(a, rep, kFlowForce, 0u, R.ntiles, &s_t0);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // the last block out: the unspent budget and the graph's loop decision
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&c->exited, 1u) == gridDim.x - 1) {
+      const int budget = __ldcg(&c->budget) - __ldcg(&c->ran);
+      const int nrep = __ldcg(&c->lay_nrep);
+      int more = 0, ovf = 0;
+      for (int r = 0; r < nrep; ++r) {
+        const RepState* S = a.st + r;
+        if (!a.rep[r].active || __ldcg(&S->steps_left) <= 0) continue;
+        if (__ldcg(&S->overflow)) ovf = 1;
+        else more = 1;
+      }
+      c->budget = budget;
+      set_loop(h_loop, (more && !ovf && budget > 0 && __ldcg(&c->err) == 0) ? 1u : 0u);
+    }
   }
 }
 

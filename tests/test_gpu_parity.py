@@ -375,7 +375,7 @@ def test_conditional_and_plain_graphs_agree(capi, ka_params):
     assert res[0][1]["rebuilds"] == res[1][1]["rebuilds"]
 
 
-@pytest.mark.parametrize("persistent", [1, 2])
+@pytest.mark.parametrize("persistent", [1, 2, 3])
 def test_replica_in_batch_equals_alone(capi, ka_params, oracle, persistent):
     """A replica advanced in a batch -- by the step graphs with k_steps
     (persistent = 1) or by the batched kernel k_batch with its in-launch

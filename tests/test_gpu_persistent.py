@@ -5,6 +5,8 @@
   * k_batch (persistent = 2, or 1 when the tiles outnumber the resident
     blocks): whole steps, the list rebuilds included (block-local sorts and
     builds claimed as work items), one grid barrier per step.
+  * k_flow (persistent = 3): the same items, each replica stepping on its
+    own through a queue of items whose inputs are complete (no step barrier).
 They run the same per-replica arithmetic (sort, list, per-tile sums and
 reduction tree), so every result must agree bit for bit."""
 import numpy as np
@@ -86,8 +88,8 @@ def test_batch_uneven_queues_bit_identical(capi, ka_params):
 
 def test_more_tiles_than_resident_blocks(capi, ka_params):
     """A batch larger than the GPU holds at once: persistent = 1 then runs
-    k_batch (many tiles per block, rebuilds inside the launch), with the
-    results of one launch per step."""
+    k_flow (many tiles per block, rebuilds inside the launch, each replica
+    stepping on its own), with the results of one launch per step."""
     from rumd_b200 import initconf as I
     c = I.ka_config(4000, T=1.0, seed=9)
     res = []
@@ -96,7 +98,7 @@ def test_more_tiles_than_resident_blocks(capi, ka_params):
         ids = [e.add(c["pos4"], c["box"], ka_params, 2, cutoff="SF", dt=0.005, T=1.0 + 0.01 * k, vel4=c["vel4"])
                for k in range(48)]  # 48 x 125 tiles of 32
         e.run(60)
-        assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == (2 if persistent else 0)
+        assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == (3 if persistent else 0)
         res.append([e.get(rid, "pos", 4000) for rid in ids[::7]] + [e.stats(ids[-1])["xi"]] +
                    [e.stats(rid)["rebuilds"] for rid in ids])
         e.close()
@@ -117,7 +119,7 @@ def test_batch_kernel_mixed_sizes_types_and_methods(capi, ka_params, oracle):
     specs = [("ka", 6000, 0.7, 90), ("lj", 3000, 1.2, 120), ("ka", 300, 2.0, 45), ("lj", 64, 1.0, 120),
              ("ka", 2, 1.0, 33), ("ka", 1500, 0.45, 120)]
     res = []
-    for persistent, split in ((0, 16), (2, 1), (2, 16), (2, 1 << 20)):
+    for persistent, split in ((0, 16), (2, 1), (2, 16), (2, 1 << 20), (3, 1), (3, 16)):
         e = engine(capi, persistent)
         e.set_variant(capi.VARIANT_SPLIT_SORT_TILES, split)
         ids = []
@@ -133,7 +135,7 @@ def test_batch_kernel_mixed_sizes_types_and_methods(capi, ka_params, oracle):
             ids.append((rid, n, kind, box))
         assert e.run_queued() == 120
         if persistent:
-            assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == 2
+            assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == persistent
         res.append([(state(e, rid, n), e.stats(rid), e.energy_log(rid)) for rid, n, _, _ in ids])
         e.close()
     for other in res[1:]:
@@ -150,7 +152,7 @@ def test_overflow_repair_under_persistent_runs(capi, ka_params):
     n = 4000
     m = melted_ka(capi, ka_params, n, steps=50, seed=13)
     res = []
-    for persistent, cap in ((0, 0), (1, 40), (2, 40)):
+    for persistent, cap in ((0, 0), (1, 40), (2, 40), (3, 40)):
         e = engine(capi, persistent)
         rid = e.add(m["pos4"], m["box"], ka_params, 2, cutoff="SF", vel4=m["vel4"], max_nbrs=cap)
         e.run(120)
@@ -158,4 +160,5 @@ def test_overflow_repair_under_persistent_runs(capi, ka_params):
         assert st["overflow"] == 0 and st["steps"] == 120
         res.append(e.get(rid, "pos", n))
         e.close()
-    assert np.array_equal(res[0], res[1]) and np.array_equal(res[0], res[2])
+    for other in res[1:]:
+        assert np.array_equal(res[0], other)

@@ -18,7 +18,7 @@ def _stream():
     return serving.poisson_stream(14, rate=400.0, seed=7, n_range=(256, 4096), steps_range=(200, 3000))
 
 
-@pytest.mark.parametrize("persistent", [1, 2])
+@pytest.mark.parametrize("persistent", [1, 2, 3])
 def test_served_results_equal_results_alone(persistent):
     from rumd_b200 import capi, serving
     eng = capi.Engine(device=0, max_replicas=16, max_particles=1 << 16, pb=64, tp=4)
@@ -58,13 +58,14 @@ def _alone(capi, c, params, steps):
     return st, pos
 
 
-def test_admission_and_removal_under_a_running_chunk():
-    """k_batch engine: replicas A, B run; while a chunk holds A, A is removed
-    and C admitted into A's id and memory; C and B must equal themselves
-    alone, and the batched graph is built once."""
+@pytest.mark.parametrize("persistent", [2, 3])
+def test_admission_and_removal_under_a_running_chunk(persistent):
+    """k_batch (k_flow) engine: replicas A, B run; while a chunk holds A, A is
+    removed and C admitted into A's id and memory; C and B must equal
+    themselves alone, and the batched graph is built once."""
     from rumd_b200 import capi, initconf
     e = capi.Engine(device=0, max_replicas=8, max_particles=1 << 15, pb=128, tp=2)
-    e.set_variant(capi.VARIANT_PERSISTENT, 2)
+    e.set_variant(capi.VARIANT_PERSISTENT, persistent)
     ca, p = _ka(initconf, 2048, 1)
     cb, _ = _ka(initconf, 3000, 2)
     cc, _ = _ka(initconf, 2048, 3)
@@ -73,7 +74,7 @@ def test_admission_and_removal_under_a_running_chunk():
     e.queue(a, 5000)
     e.queue(b, 1500)
     t1 = e.run_queued_async(400)
-    assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == 2
+    assert e.get_variant(capi.VARIANT_PERSISTENT_ACTIVE) == persistent
     builds = e.get_variant(capi.VARIANT_GRAPH_BUILDS)
     e.remove(a)  # A is still being advanced by chunk t1
     c = e.add(cc["pos4"], cc["box"], p, 2, vel4=cc["vel4"])
