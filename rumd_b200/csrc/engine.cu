@@ -492,6 +492,7 @@ EngArgs make_args(b2md_engine* e) {
   a.fq = e->fq;
   a.fseq = e->fseq;
   a.qcap = e->fqcap;
+  a.rb_steps_only = 0;
   return a;
 }
 
@@ -985,6 +986,7 @@ void check_launch() { CK(cudaGetLastError()); }
 // Builds the step graphs: [gate] -> K x { IF(rebuild) {rebuild kernels} ; fused step }.
 void build_graph(b2md_engine* e, int which, int K) {
   EngArgs a = make_args(e);
+  a.rb_steps_only = 1;
   cudaGraph_t g;
   CK(cudaGraphCreate(&g, 0));
   const size_t smem = force_smem(e, a);
@@ -1147,6 +1149,7 @@ int steps_grid(const b2md_engine* e, StepsFn fn, size_t smem) {
 // barrier each instead of a conditional node and a kernel launch.
 void build_persist_graph(b2md_engine* e) {
   EngArgs a = make_args(e);
+  a.rb_steps_only = 1;
   const size_t smem = persist_smem(e, a);
   force_fn(e, true, false, a);  // checks the shared-memory need
   StepsFn fs = steps_fn(e->tp);
@@ -2285,6 +2288,7 @@ int b2md_run_timed(b2md_engine* e, long long nsteps, double* step_kernel_ms, lon
     ensure_layout(e);
     if (e->ntiles == 0) return;
     EngArgs a = make_args(e);
+    a.rb_steps_only = 1;
     int R = (int)e->reps.size();
     k_set_steps<<<(R + 127) / 128, 128, 0, e->stream>>>(a, nsteps, 1);
     launch_momentum(e);

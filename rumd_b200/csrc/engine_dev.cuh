@@ -186,6 +186,7 @@ struct EngArgs {
   int2* fq;            // k_flow: item queue slots (replica, item code)
   unsigned long long* fseq;  // k_flow: ticket + 1 of the item in each slot (release-published)
   unsigned qcap;       // k_flow: queue slots
+  int rb_steps_only;   // rebuild kernels of a run: only replicas with queued steps (CalcF: every flagged one)
 };
 
 }  // namespace b2md

@@ -1480,13 +1480,21 @@ __global__ void k_set_steps(EngArgs a, long long nsteps, int reset_run_step) {
 // before it).
 __global__ void k_queue_steps(RepState* s, long long nsteps) { s->steps_left += nsteps; }
 
+// Within a run only replicas that step again are rebuilt (a replica whose
+// queue is empty keeps its flag until it steps or CalcF runs), as the
+// batched kernels do.
+__device__ __forceinline__ bool rb_active(const EngArgs& a, int rep) {
+  const RepState* S = a.st + rep;
+  return a.rep[rep].active && S->rebuild && !S->overflow && (!a.rb_steps_only || S->steps_left > 0);
+}
+
 // Gate: publishes "any replica flagged for rebuild" to the first conditional node.
 __global__ void k_gate(EngArgs a, cudaGraphConditionalHandle h) {
   __shared__ int s_any;
   if (threadIdx.x == 0) s_any = 0;
   __syncthreads();
   for (int r = threadIdx.x; r < a.nrep; r += blockDim.x)
-    if (a.rep[r].active && a.st[r].rebuild && !a.st[r].overflow) s_any = 1;
+    if (rb_active(a, r)) s_any = 1;
   __syncthreads();
   if (threadIdx.x == 0) cudaGraphSetConditional(h, s_any ? 1u : 0u);
 }
@@ -1498,7 +1506,7 @@ __global__ void k_gate_flag(EngArgs a, int* out) {
   if (threadIdx.x == 0) s_any = 0;
   __syncthreads();
   for (int r = threadIdx.x; r < a.nrep; r += blockDim.x)
-    if (a.rep[r].active && a.st[r].rebuild && !a.st[r].overflow) s_any = 1;
+    if (rb_active(a, r)) s_any = 1;
   __syncthreads();
   if (threadIdx.x == 0) *out = s_any;
 }
@@ -1508,10 +1516,6 @@ __global__ void k_gate_flag(EngArgs a, int* out) {
 // Grid = tiles, block = pb (one thread per slot).  Every kernel returns at once
 // for replicas that are not flagged, so the same sequence serves batches.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool rb_active(const EngArgs& a, int rep) {
-  const RepState* S = a.st + rep;
-  return a.rep[rep].active && S->rebuild && !S->overflow;
-}
 
 __device__ __forceinline__ int cell_chunk(const RepDev& R) { return (R.ncell + R.ntiles - 1) / R.ntiles; }
 

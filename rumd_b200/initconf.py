@@ -132,7 +132,12 @@ def ipl_n_params(ntypes, n, table):
 
 
 def fcc_positions(n, density):
-    """First n sites of the smallest FCC lattice with >= n sites, box scaled to density."""
+    """n sites of the smallest FCC lattice with >= n sites, box scaled to
+    density.  When n is not 4 m^3 the sites taken are spread evenly over the
+    lattice (every (4 m^3 / n)-th in lattice order), so that the start has the
+    box's density everywhere; the first n sites would pack the particles into
+    part of the box at up to twice the density, and overflow neighbour lists
+    sized for the mean density."""
     m = 1
     while 4 * m ** 3 < n:
         m += 1
@@ -140,7 +145,8 @@ def fcc_positions(n, density):
     a = L / m
     basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
     g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
-    sites = (g[:, None, :] + basis[None, :, :]).reshape(-1, 3)[:n]
+    sites = (g[:, None, :] + basis[None, :, :]).reshape(-1, 3)
+    sites = sites[(np.arange(n) * len(sites)) // n]
     pos = (sites + 0.25) * a - L / 2.0
     return pos, np.array([L, L, L])
 
