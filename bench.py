@@ -476,18 +476,18 @@ def served(capi, device, pb, tp, njobs, seed=0):
     offered = tl.get("offered_particle_steps_per_s") or 0.0
     thr = summ["throughput"]
     if offered > thr:
-        verdict = (f"not sustainable: 50 jobs/s offers {offered:.3g} particle-steps/s, {offered / thr:.1f}x the "
+        statement = (f"not sustainable: 50 jobs/s offers {offered:.3g} particle-steps/s, {offered / thr:.1f}x the "
                    f"measured capacity of {thr:.3g}; the backlog grows while jobs arrive and drains only after "
                    f"the arrivals stop (rows of load_over_time). The sustainable rate for this job mix is about "
                    f"{50.0 * thr / offered:.1f} jobs/s.")
     else:
-        verdict = (f"sustainable: 50 jobs/s offers {offered:.3g} particle-steps/s, below the measured capacity "
+        statement = (f"sustainable: 50 jobs/s offers {offered:.3g} particle-steps/s, below the measured capacity "
                    f"of {thr:.3g}")
     return {"value": thr, "unit": "particle-steps/s", "jobs": summ["jobs"],
             "p50_latency_s": summ["p50_s"], "p99_latency_s": summ["p99_s"], "makespan_s": summ["makespan_s"],
             "particle_steps": summ["particle_steps"], "hbm_max_used_bytes": srv.max_used,
             "hbm_reserved_bytes": reserved, "engine_counters": counters, "tuning": tune,
-            "sustainability": verdict, "load_over_time": tl,
+            "sustainability": statement, "load_over_time": tl,
             "one_at_a_time_value": one_rate,
             "one_at_a_time_sample": f"{len(sample)} of the {njobs} jobs run alone back to back (wall clock)",
             "speedup_vs_one_at_a_time": thr / one_rate,

@@ -305,19 +305,21 @@ void stage_commit(b2md_engine* e) {
   e->ring_open.clear();
 }
 
+// A ring of at least `cap` bytes (grown while nothing may still read it).
+void ring_reserve(b2md_engine* e, size_t cap) {
+  if (cap <= e->ring_cap) return;
+  CK(cudaStreamSynchronize(e->stream));
+  ring_reset(e);
+  if (e->ring) CK(cudaFreeHost(e->ring));
+  e->ring = nullptr;
+  e->ring_cap = 0;
+  CK(cudaMallocHost(&e->ring, cap));
+  e->ring_cap = cap;
+}
+
 char* stage_alloc(b2md_engine* e, size_t bytes) {
   const size_t n = (std::max<size_t>(bytes, 1) + 255) & ~(size_t)255;
-  if (2 * n > e->ring_cap) {
-    // grow: nothing may still read the old ring
-    CK(cudaStreamSynchronize(e->stream));
-    ring_reset(e);
-    if (e->ring) CK(cudaFreeHost(e->ring));
-    e->ring = nullptr;
-    e->ring_cap = 0;
-    const size_t cap = std::max<size_t>(4 * n, (size_t)16 << 20);
-    CK(cudaMallocHost(&e->ring, cap));
-    e->ring_cap = cap;
-  }
+  if (2 * n > e->ring_cap) ring_reserve(e, std::max<size_t>(4 * n, (size_t)4 << 20));
   size_t lo = e->ring_head;
   if (lo + n > e->ring_cap) lo = 0;
   const size_t hi = lo + n;
@@ -1574,7 +1576,11 @@ int b2md_engine_create(int device, long long max_particles, int max_replicas, lo
     }
     // pinned staging for the expected particles, so that admissions and
     // read-backs do not allocate it later
-    if (max_particles > 0) host_stage(e, (size_t)max_particles * kStagePerParticle);
+    if (max_particles > 0) {
+      host_stage(e, (size_t)max_particles * kStagePerParticle);
+      ring_reserve(e, std::min<size_t>(std::max<size_t>((size_t)max_particles * 64, (size_t)4 << 20),
+                                       (size_t)64 << 20));
+    }
     init_func_attrs(device);
     CK(cudaMalloc(&e->fctr, sizeof(unsigned)));
     CK(cudaDeviceGetAttribute(&e->nsm, cudaDevAttrMultiProcessorCount, device));
