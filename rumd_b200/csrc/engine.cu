@@ -168,9 +168,9 @@ struct b2md_engine {
   int build_lanes = 0;         // list build: 0 contiguous candidate runs per lane, else lanes per particle (32: one warp per cell)
   bool build_smem = false;     // list build: tile assembled in shared memory
   int persist = 1;             // runs: 0 one launch per step; 1 persistent (k_steps when every tile has a
-                               // resident block, else k_batch); 2 k_batch whenever it applies
+                               // resident block, else k_flow); 2 k_batch, 3 k_flow whenever they apply
   bool persist_on = false;     // the current graphs are persistent ones (kind below)
-  int persist_kind = 0;        // 1 k_steps, 2 k_batch
+  int persist_kind = 0;        // 1 k_steps, 2 k_batch, 3 k_flow
   int* flist = nullptr;        // k_batch rebuild lists (2 x rcap)
   int split_tiles = 16;        // k_batch: replicas of at least this many tiles sort in phases over many blocks
   int2* fq = nullptr;          // k_flow: item queue slots

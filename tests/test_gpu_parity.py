@@ -378,8 +378,9 @@ def test_conditional_and_plain_graphs_agree(capi, ka_params):
 @pytest.mark.parametrize("persistent", [1, 2, 3])
 def test_replica_in_batch_equals_alone(capi, ka_params, oracle, persistent):
     """A replica advanced in a batch -- by the step graphs with k_steps
-    (persistent = 1) or by the batched kernel k_batch with its in-launch
-    rebuilds (persistent = 2) -- ends bit for bit where it ends alone."""
+    (persistent = 1), by the batched kernel k_batch with its in-launch
+    rebuilds (persistent = 2) or by k_flow, each replica stepping on its own
+    (persistent = 3) -- ends bit for bit where it ends alone."""
     from rumd_b200 import initconf as I
     sizes = [600, 2048, 777, 5000]
     temps = [0.5, 1.0, 1.5, 2.0]

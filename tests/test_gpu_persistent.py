@@ -2,11 +2,11 @@
   * k_steps (persistent = 1 when every tile has a resident block): fused
     steps back to back in one cooperative launch, a grid barrier between
     them, leaving the launch for each list rebuild;
-  * k_batch (persistent = 2, or 1 when the tiles outnumber the resident
-    blocks): whole steps, the list rebuilds included (block-local sorts and
-    builds claimed as work items), one grid barrier per step.
-  * k_flow (persistent = 3): the same items, each replica stepping on its
-    own through a queue of items whose inputs are complete (no step barrier).
+  * k_batch (persistent = 2): whole steps, the list rebuilds included
+    (sorts and builds claimed as work items), one grid barrier per step.
+  * k_flow (persistent = 3, or 1 when the tiles outnumber the resident
+    blocks): the same items, each replica stepping on its own through a
+    queue of items whose inputs are complete (no step barrier).
 They run the same per-replica arithmetic (sort, list, per-tile sums and
 reduction tree), so every result must agree bit for bit."""
 import numpy as np
