@@ -2398,14 +2398,16 @@ struct Cs2Table {
   __device__ __forceinline__ float operator()(int tj) const { return row[tj]; }
 };
 
-// Accept bits of a lane's run for up to four of the cell's particles (a
+// Accept bits of a lane's run for G (4 or 2) of the cell's particles (a
 // missing one repeats the last; its bits are unused): each candidate's
-// position is read once and tested against all four.
-template <bool WRAP, bool COH, class CS2>
-__device__ __forceinline__ void run_tests4(const int* __restrict__ run, int nrun, const float4* rc,
-                                           const float4 (&rp)[4], const int (&ip)[4], const CS2 (&cs)[4],
-                                           float Lx, float Ly, float Lz, float iLx, float iLy, float iLz,
-                                           unsigned (&bits)[4]) {
+// position is read once and tested against all G.  G = 2 serves the last
+// one or two particles of a cell, so that cells of 1, 2, 5 or 6 particles do
+// not test padding copies.
+template <bool WRAP, bool COH, int G, class CS2>
+__device__ __forceinline__ void run_tests(const int* __restrict__ run, int nrun, const float4* rc,
+                                          const float4 (&rp)[4], const int (&ip)[4], const CS2 (&cs)[4],
+                                          float Lx, float Ly, float Lz, float iLx, float iLy, float iLz,
+                                          unsigned (&bits)[4]) {
 #pragma unroll
   for (int q = 0; q < 4; ++q) bits[q] = 0u;
 #pragma unroll 2
@@ -2415,7 +2417,7 @@ __device__ __forceinline__ void run_tests4(const int* __restrict__ run, int nrun
       const float4 rj = COH ? ld_ca_f4(rc + j) : __ldg(rc + j);
       const int tj = __float_as_int(rj.w);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
+      for (int q = 0; q < G; ++q) {
         float dx = rp[q].x - rj.x, dy = rp[q].y - rj.y, dz = rp[q].z - rj.z;
         if (WRAP) {
           dx = mi_comp(dx, Lx, iLx);
@@ -2581,7 +2583,10 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
 #define RUNS(W, T, MK)                                                                                    \
   {                                                                                                       \
     const T cs[4] = {MK(crow[0]), MK(crow[1]), MK(crow[2]), MK(crow[3])};                                 \
-    run_tests4<W, COH>(run, nrun, rc, rp, ip, cs, R.L[0], R.L[1], R.L[2], R.invL[0], R.invL[1], R.invL[2], bits); \
+    if (pe - p <= 2)                                                                                      \
+      run_tests<W, COH, 2>(run, nrun, rc, rp, ip, cs, R.L[0], R.L[1], R.L[2], R.invL[0], R.invL[1], R.invL[2], bits); \
+    else                                                                                                  \
+      run_tests<W, COH, 4>(run, nrun, rc, rp, ip, cs, R.L[0], R.L[1], R.L[2], R.invL[0], R.invL[1], R.invL[2], bits); \
   }
 #define ONE(c) Cs2One{(c)[0]}
 #define TWO(c) Cs2Two{(c)[0], (c)[1]}
