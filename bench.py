@@ -47,7 +47,7 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--pb", type=int, default=64)
     p.add_argument("--tp", type=int, default=2)
-    p.add_argument("--batch-steps", type=int, default=2000)
+    p.add_argument("--batch-steps", type=int, default=10000)
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--served-jobs", type=int, default=400, help="jobs in the served stream (0: skip)")
     p.add_argument("--served-only", action="store_true",
@@ -533,6 +533,7 @@ def lj_hbm_scale(capi, device, args):
     bytes_alg = n * (168.0 + 4.0 * st["mean_nbrs"])
     peak, peak_kind = measured_peaks()
     achieved = bytes_alg / per_launch_s / 1e9
+    accuracy = fp64_comparison(capi, device, e, rid, n, c["box"], params)
     print(json.dumps({"workload": "single-component LJ, N=1048576, rho=0.8442, T=0.722, NVT tau=0.2, dt=0.004, "
                                   "skin 0.3, SF rc=2.5 (plain method, HBM scale)",
                       "value": n * steps / t, "unit": "particle-steps/s", "steps": steps,
@@ -540,8 +541,49 @@ def lj_hbm_scale(capi, device, args):
                       "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                                    "frac": achieved / peak, "peak_source": peak_kind,
                                    "kernel_ms": per_launch_s * 1e3, "bytes_per_launch_alg": bytes_alg,
-                                   "mean_list_length": st["mean_nbrs"]}}), flush=True)
+                                   "mean_list_length": st["mean_nbrs"]},
+                      "fp64_oracle": accuracy}), flush=True)
     e.close()
+
+
+def fp64_comparison(capi, device, e, rid, n, box, params, steps=5000):
+    """The same state in the pure-FP64 GPU engine (b2md_f64_*): energy per
+    particle and the configurational pressure W/V at that configuration, then
+    `steps` NVT steps of each from it (FP32 engine and FP64 engine) with the
+    run-averaged energy per particle over the second half (the trajectories
+    decorrelate; the averages should not) and the FP64 run's own speed."""
+    import torch
+    pos4, vel4, im3 = e.read(rid, n)
+    e.calc_f()
+    s32 = e.stats(rid)
+    V = float(np.prod(np.asarray(box, np.float64)))
+    e64 = capi.F64Engine(pos4, box, params, 1, cutoff="SF", skin=SKIN, dt=0.004, T=0.722, tau=TAU, vel4=vel4,
+                         im3=im3, device=device)
+    e64.set_xi(s32["xi"])
+    e64.calc_f()
+    s64 = e64.stats()
+    out = {"pe_per_particle_f32": s32["pe"] / n, "pe_per_particle_f64": s64["pe"] / n,
+           "d_pe_per_particle": (s32["pe"] - s64["pe"]) / n,
+           "W_over_V_f32": s32["virial"] / V, "W_over_V_f64": s64["virial"] / V,
+           "d_pressure_configurational": (s32["virial"] - s64["virial"]) / V}
+    e.set_energy_log(rid, 1, steps)
+    e.run(steps)
+    log = e.energy_log(rid)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    en = e64.run(steps, energies=True)
+    torch.cuda.synchronize(device)
+    t64 = time.perf_counter() - t0
+    e64.close()
+    half = steps // 2
+    out.update({"nvt_steps": steps,
+                "mean_pe_per_particle_f32": float(log[half:, 1].mean() / n),
+                "mean_pe_per_particle_f64": float(en[half:, 0].mean() / n),
+                "mean_W_over_V_f32": float(log[half:, 2].mean() / V),
+                "mean_W_over_V_f64": float(en[half:, 1].mean() / V),
+                "f64_value": n * steps / t64, "f64_unit": "particle-steps/s (wall clock)"})
+    out["d_mean_pe_per_particle"] = out["mean_pe_per_particle_f32"] - out["mean_pe_per_particle_f64"]
+    return out
 
 
 def kernel_variants(engine):
