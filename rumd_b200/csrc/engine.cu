@@ -111,6 +111,8 @@ struct HostRep {
   std::vector<float> params;   // RUMD layout
   int nb_method_req = -1;      // -1 default
   long long bytes = 0;         // device bytes held in the engine's pools (b2md_engine_usage)
+  long long admit_seq = 0;     // chunks launched before this replica was admitted
+  long long repair_seq = -1;   // chunks launched when its list was last enlarged
   // a second pair potential (b2md_replica_add_potential): RUMD layout table,
   // pair function, cut-off method, its packed table's place
   std::vector<float> params1;
@@ -1341,7 +1343,11 @@ bool repair_overflow(b2md_engine* e) {
     any = true;
     ++e->list_repairs;
   }
-  if (any) invalidate_graphs(e, INV_REPAIR);
+  // The graphs read each replica's list place and capacity from the replica
+  // table, and a pool growth has dropped them already; only the variants that
+  // size shared memory by the longest list (staged list tiles, position
+  // windows, a build assembling its tile in shared memory) must be rebuilt.
+  if (any && (e->force_mode != FM_STREAMED || e->build_smem)) invalidate_graphs(e, INV_REPAIR);
   return any;
 }
 
@@ -1420,6 +1426,7 @@ int guarded(F&& fn) {
 // Waits for a chunk of b2md_run_queued_async and checks what it left: a
 // step-barrier wait that gave up is reported; overflowed lists are enlarged
 // and flagged for a rebuild (their replicas continue in the next chunk).
+long long replica_bytes(const b2md_engine* e, const HostRep& h);
 void finish_chunk(b2md_engine* e, ChunkRec& c) {
   CK(cudaEventSynchronize(c.done));
   c.waited = true;
@@ -1428,10 +1435,36 @@ void finish_chunk(b2md_engine* e, ChunkRec& c) {
     check_persist(e);  // clears the flag and reports
   }
   c.ran = c.persistent ? c.budget - c.h_ctl->budget : c.budget;
-  bool fix = false;
-  for (size_t r = 0; r < c.active.size(); ++r)
-    if (c.active[r] && (c.h_st[r].overflow || c.h_st[r].err)) fix = true;
-  if (fix) repair_overflow(e);
+  // overflowed lists, from the snapshot and without waiting for the chunk
+  // in flight (it skips replicas flagged as overflowed): the list is placed
+  // anew, the replica's descriptor uploaded through the staging ring and its
+  // flags reset in stream order; a later snapshot still showing the flag
+  // (taken before the reset) is not repaired twice
+  bool any = false;
+  for (size_t r = 0; r < c.active.size() && r < e->reps.size(); ++r) {
+    HostRep& h = e->reps[r];
+    if (!c.active[r] || !h.active || h.admit_seq >= c.ticket) continue;  // not the replica the chunk ran
+    const RepState& st = c.h_st[r];
+    if (st.err)
+      api_fail(B2MD_ERR_CUDA, "a bounded device wait for the neighbour-list copy gave up (replica " +
+                                  std::to_string(r) + ")");
+    if (!st.overflow || h.repair_seq >= c.ticket) continue;
+    int want = std::max(h.d.max_nbrs * 2, st.actual_max_nbrs + 8);
+    want = std::min(want, std::max(h.n - 1, 1));
+    if (want <= h.d.max_nbrs) api_fail(B2MD_ERR_OVERFLOW, "neighbour list cannot grow further");
+    place_list(e, h, want);
+    h.bytes = replica_bytes(e, h);
+    RepDev* d = reinterpret_cast<RepDev*>(stage_alloc(e, sizeof(RepDev)));
+    *d = h.d;
+    CK(cudaMemcpyAsync(e->rep + r, d, sizeof(RepDev), cudaMemcpyHostToDevice, e->stream));
+    stage_commit(e);
+    k_clear_overflow<<<1, 1, 0, e->stream>>>(e->st + r);
+    check_launch();
+    h.repair_seq = e->chunk_seq;
+    ++e->list_repairs;
+    any = true;
+  }
+  if (any && (e->force_mode != FM_STREAMED || e->build_smem)) invalidate_graphs(e, INV_REPAIR);
 }
 
 ChunkRec* find_chunk(b2md_engine* e, long long ticket) {
@@ -1847,6 +1880,7 @@ int b2md_replica_add(b2md_engine* e, const b2md_replica_desc* d, const float* po
     s->rebuild = 1;
     CK(cudaMemcpyAsync(e->st + id, s, sizeof(RepState), cudaMemcpyHostToDevice, e->stream));
     stage_commit(e);
+    h.admit_seq = e->chunk_seq;
     e->reps[id] = h;
     // tiles, the replica table and the momentum follow before the next launch
     e->layout_dirty = true;

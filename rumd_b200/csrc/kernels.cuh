@@ -1480,6 +1480,13 @@ __global__ void k_set_steps(EngArgs a, long long nsteps, int reset_run_step) {
 // before it).
 __global__ void k_queue_steps(RepState* s, long long nsteps) { s->steps_left += nsteps; }
 
+// An enlarged list is in place: the replica's overflow flag is cleared and
+// its list is due (in stream order).
+__global__ void k_clear_overflow(RepState* s) {
+  s->overflow = 0;
+  s->rebuild = 1;
+}
+
 // Within a run only replicas that step again are rebuilt (a replica whose
 // queue is empty keeps its flag until it steps or CalcF runs), as the
 // batched kernels do.

@@ -132,12 +132,12 @@ def ipl_n_params(ntypes, n, table):
 
 
 def fcc_positions(n, density):
-    """n sites of the smallest FCC lattice with >= n sites, box scaled to
-    density.  When n is not 4 m^3 the sites taken are spread evenly over the
-    lattice (every (4 m^3 / n)-th in lattice order), so that the start has the
-    box's density everywhere; the first n sites would pack the particles into
-    part of the box at up to twice the density, and overflow neighbour lists
-    sized for the mean density."""
+    """The first n sites of the smallest FCC lattice with >= n sites, box
+    scaled to density, as RUMD's rumd_init_conf drops the trailing sites
+    (Tools/rumd_init_conf.cc:460-467).  When n is not 4 m^3 the particles fill
+    part of the box at up to twice the density at the start; neighbour lists
+    sized for the mean density may overflow in the first steps, and the
+    engine enlarges them (NeighborList.cu:657-676)."""
     m = 1
     while 4 * m ** 3 < n:
         m += 1
@@ -145,8 +145,7 @@ def fcc_positions(n, density):
     a = L / m
     basis = np.array([[0, 0, 0], [0.5, 0.5, 0], [0.5, 0, 0.5], [0, 0.5, 0.5]])
     g = np.stack(np.meshgrid(np.arange(m), np.arange(m), np.arange(m), indexing="ij"), -1).reshape(-1, 3)
-    sites = (g[:, None, :] + basis[None, :, :]).reshape(-1, 3)
-    sites = sites[(np.arange(n) * len(sites)) // n]
+    sites = (g[:, None, :] + basis[None, :, :]).reshape(-1, 3)[:n]
     pos = (sites + 0.25) * a - L / 2.0
     return pos, np.array([L, L, L])
 

@@ -113,3 +113,40 @@ def test_footprint_matches_usage():
     e.remove(rid)
     assert e.usage()[0] == 0
     e.close()
+
+
+def test_list_repair_between_chunks_keeps_results_and_graph():
+    """A replica whose list is too small overflows at its first build; the
+    chunk's wait enlarges the list from the snapshot, without waiting for the
+    chunk in flight and without rebuilding the step graph, and the replica
+    then catches up: its result equals the same replica's queued steps run
+    with b2md_run_queued (synchronous repair), bit for bit."""
+    from rumd_b200 import capi, initconf
+    c, p = _ka(initconf, 3000, 11)
+    d, _ = _ka(initconf, 2000, 12)
+    e = capi.Engine(device=0, max_replicas=4, max_particles=1 << 14, pb=128, tp=2)
+    e.set_variant(capi.VARIANT_PERSISTENT, 3)
+    a = e.add(c["pos4"], c["box"], p, 2, vel4=c["vel4"], max_nbrs=40)
+    b = e.add(d["pos4"], d["box"], p, 2, vel4=d["vel4"])
+    e.queue(a, 600)
+    e.queue(b, 600)
+    left = 1
+    while left > 0:
+        t1 = e.run_queued_async(150)
+        t2 = e.run_queued_async(150)
+        e.wait(t1)
+        _, snap = e.wait(t2)
+        left = max(snap[a, 2], snap[b, 2])
+    cnt = e.counters()
+    assert cnt["list_repairs"] >= 1 and cnt["graphs_dropped_by_list_repair"] == 0
+    sa = e.stats(a)
+    pa = e.get(a, "pos", 3000)
+    e.close()
+    ref = capi.Engine(device=0, pb=128, tp=2)
+    r = ref.add(c["pos4"], c["box"], p, 2, vel4=c["vel4"], max_nbrs=40)
+    ref.queue(r, 600)
+    ref.run_queued(0)
+    assert sa["steps"] == ref.stats(r)["steps"] == 600
+    assert sa["pe"] == ref.stats(r)["pe"] and sa["xi"] == ref.stats(r)["xi"]
+    assert np.array_equal(pa, ref.get(r, "pos", 3000))
+    ref.close()
