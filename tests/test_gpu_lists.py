@@ -203,3 +203,49 @@ def test_kob_andersen_n1000_run(capi, oracle, ka_params, seed):
     fref, u, w = oracle.forces_f64(pos4[:, :3].astype(np.float64), types, c["box"], 2, ka_params, oracle.SF)
     assert rms_rel(f[:, :3].astype(np.float64), fref) <= 1e-5
     identity_build(capi, oracle, pos4, c["box"], ka_params, 2)
+
+
+def test_lists_asymmetric_cutoff_table(capi, oracle, ka_params):
+    """A pair table whose (A, B) and (B, A) cut-offs differ (RUMD stores the
+    table per ordered type pair): each particle's list uses its own row of the
+    table, as the oracle's does."""
+    from rumd_b200 import initconf as I
+    n = 4096
+    params = ka_params.copy().reshape(4, -1)
+    params[2, 0] = params[1, 0] * 0.9  # rc of (1, 0) below that of (0, 1)
+    params = params.reshape(-1)
+    c = I.ka_config(n, T=1.0, seed=21)
+    identity_build(capi, oracle, c["pos4"], c["box"], params, 2)
+
+
+def test_lists_over_full_cell(capi, oracle, lj_params):
+    """LJ at density 0.8442 with 70 particles moved into a cube of side 1.2 --
+    one cell holds them all and the rows through it have over a hundred
+    candidates; then the particles are spread again and the same engine
+    rebuilds.  Both lists are the oracle's."""
+    from rumd_b200 import initconf as I
+    n, k = 32000, 70
+    c = I.lj_config(n, density=0.8442, T=1.0, seed=5)
+    pos_blob = c["pos4"].copy()
+    rng = np.random.default_rng(5)
+    centre = np.asarray(c["box"], np.float32) * 0.3
+    pos_blob[:k, :3] = centre + rng.uniform(-0.6, 0.6, (k, 3)).astype(np.float32)
+    box = c["box"]
+    identity_build(capi, oracle, pos_blob, box, lj_params, 1, max_nbrs=400)
+    spread = I.lj_config(n, density=0.8442, T=1.0, seed=6)["pos4"]
+    e = capi.Engine(device=0, pb=64, tp=4, max_particles=n)
+    rid = e.add(pos_blob, box, lj_params, 1, cutoff="SF", skin=0.3, max_nbrs=400)
+    e.calc_f()
+    assert e.stats(rid)["rebuilds"] == 1
+    e.set(rid, "pos", spread)
+    e.calc_f()
+    assert e.stats(rid)["rebuilds"] == 2
+    L = np.asarray(box, np.float32)
+    nc = oracle.cell_grid(L, oracle.max_cutoff(lj_params, 1), 0.3)
+    uidx = e.sort_index(rid, n)
+    pos_slot = e.get(rid, "pos", n)[uidx]
+    counts, nbl, ov = oracle.nbl_cells(pos_slot, L, nc, 1, lj_params, 0.3, 400)
+    assert not ov
+    gc, gl = e.nbl(rid, n, 400)
+    compare_lists(gc, gl, uidx, counts, nbl)
+    e.close()
