@@ -2469,7 +2469,7 @@ __device__ __forceinline__ int run_store(unsigned bits, const int* __restrict__ 
 // are read with coherent loads.
 template <bool COH>
 __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max,
-                                                int* s_last = nullptr) {
+                                                int* s_last = nullptr, int* s_next = nullptr) {
   constexpr unsigned FULL = 0xffffffffu;
   const int rep = a.tile_rep[tile];
   const RepDev& R = a.rep[rep];
@@ -2477,7 +2477,10 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
   const int nt = R.ntypes;
   const int nwarps = blockDim.x >> 5;
   for (int k = threadIdx.x; k < nt * nt; k += blockDim.x) s_cs2[k] = a.par[R.par0 + k * kParStride + 6];
-  if (threadIdx.x == 0) *s_max = 0;
+  if (threadIdx.x == 0) {
+    *s_max = 0;
+    if (s_next) *s_next = nwarps;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int first = a.tile_first[tile];
@@ -2502,7 +2505,15 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
     k1 = cell_coord(rl.x, iLx, nx) + cell_coord(rl.y, iLy, ny) * nx + cell_coord(rl.z, iLz, nz) * nx * ny;
   }
   int wmax = 0;
-  for (int c = k0 + warp; c <= k1; c += nwarps) {
+  // cells in order, each warp taking the next unclaimed one (s_next: the
+  // warps' cells even out within the block), or every nwarps-th
+  auto next_cell = [&](int c) -> int {
+    if (!s_next) return c + nwarps;
+    int v = 0;
+    if (lane == 0) v = atomicAdd(s_next, 1);
+    return k0 + __shfl_sync(FULL, v, 0);
+  };
+  for (int c = k0 + warp; c <= k1; c = next_cell(c)) {
     const int p0 = cells ? max(cbeg[c], first) : first;
     const int p1 = cells ? min(cbeg[c] + ccnt[c], last) : last;
     if (p0 >= p1) continue;  // no particle of this tile in the cell
@@ -2654,18 +2665,19 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
 __device__ __noinline__ void build_runs_tile_batch(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
   build_runs_tile<true>(a, tile, s_cs2, s_run, s_max);
 }
-// k_flow's: also reports whether this tile's build was the replica's last.
+// k_flow's: also reports whether this tile's build was the replica's last
+// (s_next: the block's cell-claim counter).
 __device__ __noinline__ void build_runs_tile_flow(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max,
-                                                  int* s_last) {
-  build_runs_tile<true>(a, tile, s_cs2, s_run, s_max, s_last);
+                                                  int* s_last, int* s_next) {
+  build_runs_tile<true>(a, tile, s_cs2, s_run, s_max, s_last, s_next);
 }
 
 __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
   __shared__ float s_cs2[kCs2Floats];
   __shared__ int s_run[kRunWarps * 32 * kRunStride];
-  __shared__ int s_max;
+  __shared__ int s_max, s_next;
   if (!rb_active(a, a.tile_rep[blockIdx.x])) return;
-  build_runs_tile<false>(a, blockIdx.x, s_cs2, s_run, &s_max);
+  build_runs_tile<false>(a, blockIdx.x, s_cs2, s_run, &s_max, nullptr, &s_next);
 }
 
 // ---------------------------------------------------------------------------
@@ -3586,7 +3598,7 @@ __global__ void __maxnreg__(64) k_flow(EngArgs a, cudaGraphConditionalHandle h_l
     } else {
       float* s_cs2 = reinterpret_cast<float*>(s_dyn);
       int* s_run = reinterpret_cast<int*>(s_dyn + kCs2Floats * sizeof(float));
-      build_runs_tile_flow(a, R.tile0 + idx, s_cs2, s_run, &s_max, &s_last);
+      build_runs_tile_flow(a, R.tile0 + idx, s_cs2, s_run, &s_max, &s_last, &s_flag);  // s_flag: cell claims
       __syncthreads();
       if (s_last) {
         // the replica's lists are complete: its force tiles, unless a list
