@@ -105,6 +105,7 @@ struct RepState {
   unsigned sort_items;   // k_batch: phase items of the replica's split sort completed (reset by the last)
   int flow_left;         // k_flow: items of the replica's current phase not yet finished
   int launch_steps;      // k_flow: steps the replica ran in the current launch
+  int build_next;        // k_rb_build_runs: the replica's next unclaimed cell (0 between builds)
 };
 
 // Control block of the persistent step kernel (k_steps), one per engine.

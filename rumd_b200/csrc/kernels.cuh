@@ -2467,7 +2467,11 @@ __device__ __forceinline__ int run_store(unsigned bits, const int* __restrict__ 
 // s_run: 32 * kRunStride ints per warp, s_max: one int.  COH: the positions
 // and cell arrays were written earlier in the same launch (k_batch), so they
 // are read with coherent loads.
-template <bool COH>
+// GRID: the block's warps claim cells of the whole replica from its counter
+// (S->build_next) and list every particle of a claimed cell, so the work of
+// all the replica's blocks evens out (cell method only); the tile's range
+// then serves only the bookkeeping.
+template <bool COH, bool GRID = false>
 __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max,
                                                 int* s_last = nullptr, int* s_next = nullptr) {
   constexpr unsigned FULL = 0xffffffffu;
@@ -2498,7 +2502,9 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
   // units of work: the cells from the first to the last particle's (keys
   // ascend along the slots), or one unit for all pairs
   int k0 = 0, k1 = 0;
-  if (cells && last > first) {
+  if (GRID) {
+    k1 = R.ncell - 1;
+  } else if (cells && last > first) {
     const float4 rf = rc[first], rl = rc[last - 1];
     const float iLx = R.invL[0], iLy = R.invL[1], iLz = R.invL[2];
     k0 = cell_coord(rf.x, iLx, nx) + cell_coord(rf.y, iLy, ny) * nx + cell_coord(rf.z, iLz, nz) * nx * ny;
@@ -2508,14 +2514,19 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
   // cells in order, each warp taking the next unclaimed one (s_next: the
   // warps' cells even out within the block), or every nwarps-th
   auto next_cell = [&](int c) -> int {
+    if (GRID) {
+      int v = 0;
+      if (lane == 0) v = atomicAdd(&S->build_next, 1);
+      return __shfl_sync(FULL, v, 0);
+    }
     if (!s_next) return c + nwarps;
     int v = 0;
     if (lane == 0) v = atomicAdd(s_next, 1);
     return k0 + __shfl_sync(FULL, v, 0);
   };
-  for (int c = k0 + warp; c <= k1; c = next_cell(c)) {
-    const int p0 = cells ? max(cbeg[c], first) : first;
-    const int p1 = cells ? min(cbeg[c] + ccnt[c], last) : last;
+  for (int c = GRID ? next_cell(0) : k0 + warp; c <= k1; c = next_cell(c)) {
+    const int p0 = GRID ? cbeg[c] : cells ? max(cbeg[c], first) : first;
+    const int p1 = GRID ? cbeg[c] + ccnt[c] : cells ? min(cbeg[c] + ccnt[c], last) : last;
     if (p0 >= p1) continue;  // no particle of this tile in the cell
     // lane r < 25: row (dz, dy) = (r/5 - 2, r%5 - 2) as one or two slot parts
     int b0 = 0, e0 = 0, b1 = 0, e1 = 0;
@@ -2653,6 +2664,7 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
     if (s_last) *s_last = cdone == (unsigned)(R.ntiles - 1);
     if (cdone == (unsigned)(R.ntiles - 1)) {
       a.rctr[rep] = 0u;
+      if (GRID) S->build_next = 0;
       S->nrebuilds += 1;
       // the replica's lists are complete: released to k_batch's force items
       st_release_u32(reinterpret_cast<unsigned*>(&S->rebuild), 0u);
@@ -2676,8 +2688,10 @@ __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
   __shared__ float s_cs2[kCs2Floats];
   __shared__ int s_run[kRunWarps * 32 * kRunStride];
   __shared__ int s_max, s_next;
-  if (!rb_active(a, a.tile_rep[blockIdx.x])) return;
-  build_runs_tile<false>(a, blockIdx.x, s_cs2, s_run, &s_max, nullptr, &s_next);
+  const int rep = a.tile_rep[blockIdx.x];
+  if (!rb_active(a, rep)) return;
+  if (a.rep[rep].nb_method == NB_CELLS) build_runs_tile<false, true>(a, blockIdx.x, s_cs2, s_run, &s_max);
+  else build_runs_tile<false>(a, blockIdx.x, s_cs2, s_run, &s_max, nullptr, &s_next);
 }
 
 // ---------------------------------------------------------------------------
