@@ -2677,11 +2677,13 @@ __device__ __forceinline__ void build_runs_tile(const EngArgs& a, int tile, floa
 __device__ __noinline__ void build_runs_tile_batch(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max) {
   build_runs_tile<true>(a, tile, s_cs2, s_run, s_max);
 }
-// k_flow's: also reports whether this tile's build was the replica's last
-// (s_next: the block's cell-claim counter).
+// k_flow's: also reports whether this item's build was the replica's last;
+// cell-method replicas claim cells replica-wide (an item queued late finds
+// the cells taken and ends at once), others by the block's counter s_next.
 __device__ __noinline__ void build_runs_tile_flow(const EngArgs& a, int tile, float* s_cs2, int* s_run, int* s_max,
                                                   int* s_last, int* s_next) {
-  build_runs_tile<true>(a, tile, s_cs2, s_run, s_max, s_last, s_next);
+  if (a.rep[a.tile_rep[tile]].nb_method == NB_CELLS) build_runs_tile<true, true>(a, tile, s_cs2, s_run, s_max, s_last);
+  else build_runs_tile<true>(a, tile, s_cs2, s_run, s_max, s_last, s_next);
 }
 
 __global__ void __launch_bounds__(kRunWarps * 32) k_rb_build_runs(EngArgs a) {
